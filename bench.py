@@ -1,0 +1,355 @@
+"""Benchmark of the epoch-kernel hot path: BFS, SSSP and PageRank on one
+synthetic Kronecker graph, reported as GTEPS with the HBM roofline.
+
+Workload (one step): Kronecker scale 22, edge factor 16, symmetrized, int32
+weights in [1,255] (seeded synthetic; no dataset); BFS from 64 sources, SSSP
+from the same 64 sources (SourcePicker seed 37525), PageRank d=0.85 with an L1
+tolerance of 1e-4 and at most 50 iterations.  GTEPS follows the reference's
+benchmark formula: every run (one source, or one PageRank solve) counts M/2
+edges (src/benchmarks/gpu_benchmark.cuh:259), value = runs * M/2 / time.
+
+  python bench.py [--gpus N --steps K --warmup W]          this engine
+  python bench.py --impl reference [...]                   the reference's own
+        OpenMP CPU code (oracle/_ref), host cores, bounded sample per step
+
+Under torchrun (N > 1) each rank holds a replica of the graph and runs its own
+64 sources (weak scaling, no data-path collective); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "hetero-compute_b200"))
+
+METRIC = "GTEPS & %HBM roofline, BFS/SSSP/PR: batched+adjoint vs plain, 1 B200"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--edge-factor", type=int, default=16)
+    p.add_argument("--sources", type=int, default=64)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-budget-s", type=float, default=20.0)
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload(a):
+    return {"workload": f"kronecker-s{a.scale}-ef{a.edge_factor}: bfs x{a.sources} + sssp x{a.sources} + pagerank",
+            "scale": a.scale, "edge_factor": a.edge_factor, "sources_per_gpu": a.sources,
+            "weights": "int32 uniform [1,255]", "pagerank": "d=0.85, L1 tol 1e-4, max 50 iters",
+            "l2": "CSR (>= 0.5 GB) larger than L2; L2 flushed between timed steps"}
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------- CPU legs
+
+def reference_sample(host, a, budget_s: float, threads: int):
+    """Times the reference's own CPU code (oracle/_ref) on a bounded sample of the step; returns
+    (gteps_estimate, detail).  The step time is extrapolated from per-run means: 64 x BFS + 64 x SSSP + 1 PR."""
+    import hc
+    import oracle
+    m = host.num_edges
+    with tempfile.TemporaryDirectory() as tmp:
+        sg, wsg = os.path.join(tmp, "g.sg"), os.path.join(tmp, "g.wsg")
+        hc.write_graph(sg, hc.HostCSR(host.index, host.neighbors))
+        hc.write_graph(wsg, host)
+        if os.path.exists(oracle.REF_DRIVER):
+            kind = "reference"
+            t0 = time.time()
+            bfs = oracle.run_reference("bfs", sg, 4, "-", threads=threads)
+            left = budget_s - (time.time() - t0)
+            sssp = oracle.run_reference("sssp", wsg, 1, "-", threads=threads)
+            pr = oracle.run_reference("pr", wsg, 0, "-", threads=threads)
+            t_bfs = float(np.mean(bfs["ms"])) / 1e3
+            t_sssp = float(np.mean(sssp["ms"])) / 1e3
+            t_pr = float(pr["ms"][0]) / 1e3
+            sample = (f"reference bfs_do_cpu x{len(bfs['ms'])}, sssp_pull_cpu x{len(sssp['ms'])}, "
+                      f"pr_pull_cpu x1 on {threads} OpenMP threads; step = 64 bfs + 64 sssp + 1 pr "
+                      f"extrapolated from per-run means")
+            del left
+        else:
+            kind = "port"
+            src = hc.pick_sources(host, 2)
+            t0 = time.time()
+            oracle.bfs_depth(host.index, host.neighbors, src[0])
+            t_bfs = time.time() - t0
+            t0 = time.time()
+            oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, src[0])
+            t_sssp = time.time() - t0
+            t0 = time.time()
+            oracle.pr_pull(host.index, host.neighbors, max_iters=5)
+            t_pr = (time.time() - t0) * 10
+            threads = 1
+            sample = "oracle port (1 thread): bfs x1, dijkstra x1, pagerank 5 sweeps scaled to 50"
+    runs = 2 * a.sources + 1
+    t_step = a.sources * t_bfs + a.sources * t_sssp + t_pr
+    gteps = runs * (m / 2) / t_step / 1e9
+    return gteps, {"kind": kind, "cores": threads, "sample": sample,
+                   "per_run_s": {"bfs": t_bfs, "sssp": t_sssp, "pagerank": t_pr}}
+
+
+def run_reference_arm(a):
+    import hc
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    host = hc.gen_kronecker(a.scale, a.edge_factor, a.seed, hc.W_I32)
+    threads = os.cpu_count() or 1
+    vals = []
+    detail = None
+    for i in range(a.warmup + a.steps):
+        v, detail = reference_sample(host, a, a.cpu_budget_s, threads)
+        if i >= a.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    ms_step = (2 * a.sources + 1) * (host.num_edges / 2) / (value * 1e9) * 1e3
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32", "data": "synthetic",
+        "config": workload(a),
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": detail["cores"], "kind": detail["kind"],
+                         "sample": detail["sample"]},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "detail": detail}))
+
+
+# ----------------------------------------------------------- GPU arm
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference_arm(a)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import hc
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+
+    t0 = time.time()
+    host = hc.gen_kronecker(a.scale, a.edge_factor, a.seed, hc.W_I32)
+    gen_s = time.time() - t0
+    n, m = host.num_nodes, host.num_edges
+    g = hc.Graph.from_host(host, device=local)
+    # One side stream for the library and the timing events.
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    g.set_stream(stream.cuda_stream)
+    k = a.sources
+    src_all = hc.pick_sources(host, k * (rank + 1))
+    src = src_all[k * rank:]
+    src_dev = torch.from_numpy(src).to(dev)
+
+    depth = torch.empty((k, n), dtype=torch.int32, device=dev)
+    parent = torch.empty((k, n), dtype=torch.int32, device=dev)
+    dist_o = torch.empty((k, n), dtype=torch.int32, device=dev)
+    scores = torch.empty(n, dtype=torch.float32, device=dev)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
+
+    def step(times):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        _, _, sb = g.bfs(src_dev, depth, parent)
+        ev[1].record(stream)
+        _, _, ss = g.sssp(src_dev, dist_o)
+        ev[2].record(stream)
+        _, sp = g.pagerank(None, scores, tol_l1=1e-4, max_iters=50)
+        ev[3].record(stream)
+        torch.cuda.synchronize(dev)
+        times.append([ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3])])
+        return sb, ss, sp
+
+    # Instrumented pass (not timed): algorithmic byte counts and kernel times.
+    _, _, bst = g.bfs(src_dev, depth, parent, stats=True)
+    _, _, sst = g.sssp(src_dev, dist_o, stats=True)
+    _, pst = g.pagerank(None, scores, tol_l1=1e-4, max_iters=50)
+    for _ in range(a.warmup):
+        step([])
+    # Timed region: K steps, L2 flushed (untimed) between steps.
+    times = []
+    pr_iters = []
+    with ClockSampler(local) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1)
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize(dev)
+            sb, ss, sp = step(times)
+            pr_iters.append(sp.iterations)
+    t = np.array(times)  # ms per algorithm per step
+    step_ms = t.sum(axis=1)
+    total_ms = float(step_ms.sum())
+    if world > 1:
+        tt = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    runs = 2 * k + 1
+    value = world * a.steps * runs * (m / 2) / (total_ms / 1e3) / 1e9
+
+    # End to end through the public API with host buffers: sources from pinned
+    # host memory in, depth/parent/distances/scores back to pinned host memory.
+    src_pin = torch.from_numpy(src.copy()).pin_memory()
+    h_depth = torch.empty((k, n), dtype=torch.int32).pin_memory().numpy()
+    h_parent = torch.empty((k, n), dtype=torch.int32).pin_memory().numpy()
+    h_dist = torch.empty((k, n), dtype=torch.int32).pin_memory().numpy()
+    h_scores = torch.empty(n, dtype=torch.float32).pin_memory().numpy()
+    e2e_ms = []
+    for _ in range(max(1, a.steps)):
+        flush.fill_(1)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        s_np = src_pin.numpy()
+        g.bfs(s_np, h_depth, h_parent)
+        g.sssp(s_np, h_dist)
+        g.pagerank(None, h_scores, tol_l1=1e-4, max_iters=50)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = float(np.sum(e2e_ms))
+    if world > 1:
+        tt = torch.tensor([e2e_total], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+    e2e_value = world * len(e2e_ms) * runs * (m / 2) / (e2e_total / 1e3) / 1e9
+
+    # Roofline of the dominant kernel (largest share of the step).
+    hbm, peak_kind = peaks()
+    per_algo = {}
+    share = t.sum(axis=0) / t.sum()
+    for i, (name, st) in enumerate([("bfs", bst), ("sssp", sst), ("pagerank", pst)]):
+        ms_kernel = st.ms  # device time of the launches themselves (library events)
+        runs_a = k if name != "pagerank" else 1
+        per_algo[name] = {
+            "gteps": runs_a * (m / 2) / (float(t[:, i].mean()) / 1e3) / 1e9,
+            "ms_per_step": float(t[:, i].mean()),
+            "share": float(share[i]),
+            "kernel_ms": ms_kernel,
+            "bytes_model": st.bytes_model,
+            "achieved_gbs": st.bytes_model / (ms_kernel / 1e3) / 1e9 if ms_kernel > 0 else None,
+        }
+    per_algo["pagerank"]["iterations"] = int(pst.iterations)
+    per_algo["bfs"]["levels"] = int(bst.levels)
+    per_algo["sssp"]["epochs"] = int(sst.epochs)
+    dom = max(per_algo, key=lambda x: per_algo[x]["share"])
+    achieved = per_algo[dom]["achieved_gbs"]
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"s{a.scale}", {}).get(dom)
+        except Exception:
+            traffic = None
+    roof = {"bound": "hbm", "kernel": {"bfs": "bfs_persistent", "sssp": "sssp_persistent",
+                                       "pagerank": "pr_sweep"}[dom],
+            "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm if achieved else None, "peak_kind": peak_kind, "traffic": traffic}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            v, d = reference_sample(host, a, a.cpu_budget_s, os.cpu_count() or 1)
+            cpu = {"value": v, "unit": "GTEPS", "cores": d["cores"], "kind": d["kind"], "sample": d["sample"]}
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": "GTEPS", "cores": None, "kind": "unavailable", "sample": str(ex)}
+
+    # Launches per step: one persistent BFS kernel per source; one SSSP kernel
+    # per source plus the weight check; PageRank init + sweeps queued in rounds
+    # of four (sweeps queued after convergence exit at once).
+    launches = a.steps * (k + (k + 1) + (1 + 4 * int(np.ceil(max(pr_iters) / 4.0))))
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": float(step_ms.mean()), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32", "data": "synthetic",
+            "config": workload(a) | {"num_nodes": n, "num_edges": m, "parallelism": f"replicas x{world}"},
+            "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": int(src.nbytes),
+                    "d2h_bytes_per_step": int(3 * k * n * 4 + n * 4)},
+            "gpu_launches": launches, "clocks": clk.summary(), "per_algo": per_algo,
+            "graph_gen_s": gen_s}), flush=True)
+    g.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,418 @@
+// Direction-optimising BFS as one persistent cooperative launch per source.
+//
+// Reference path: bfs_gpu (src/kernels/gpu/bfs.cuh:21-95) runs bottom-up
+// epochs only, one launch + blocking 4-byte D2H + cudaMemset per level; the
+// direction heuristic lives in the CPU bfs_do_cpu (src/kernels/cpu/bfs.cuh:48-114,
+// alpha = 15, beta = 18).  Here the whole level loop runs on the device: every
+// block evaluates the same alpha/beta state machine from counters read after a
+// grid barrier, so the per-level selector costs no host round trip.
+//
+// HBM layout of the working set (W = ceil(N/32) words):
+//   depth, parent  int32[N]      outputs (caller's device buffer or ours)
+//   visited        uint32[W]     claimed vertices
+//   fb[3]          uint32[W]     frontier bitmaps: level L reads fb[L%3],
+//                                writes fb[(L+1)%3], zeroes fb[(L+2)%3]
+//   q[2]           int32[N]      frontier queues (top-down levels)
+//   tasks          int2[]        (vertex, chunk) pieces of long rows
+#include <algorithm>
+#include <vector>
+
+#include "hc_expand.cuh"
+#include "hc_graph.cuh"
+
+namespace hc {
+namespace {
+
+constexpr int kBfsThreads = 512;
+
+struct LevelCnt {
+    int nf;                 // vertices in this frontier
+    int tasks;              // long-row tasks queued while expanding it
+    unsigned long long mf;  // sum of their degrees (top-down only)
+};
+
+struct BfsCtl {
+    GridSync gs;
+    LevelCnt cnt[3];
+    int conv;               // bitmap -> queue conversion counter
+    int levels, td_levels, bu_levels;
+    unsigned long long vscan, escan, reached;
+};
+
+struct BfsArgs {
+    const int64_t *index;
+    const int32_t *nbr;
+    int32_t n, n_active, n_warp_rows;
+    int64_t m;
+    int32_t *depth, *parent;
+    uint32_t *visited, *fb0, *fb1, *fb2;
+    int32_t *q0, *q1;
+    int2 *tasks;
+    BfsCtl *ctl;
+    int32_t src;
+    int alpha, beta, direction, bu_variant, max_levels;
+};
+
+__device__ __forceinline__ uint32_t *fb_sel(const BfsArgs &a, int i) {
+    return i == 0 ? a.fb0 : (i == 1 ? a.fb1 : a.fb2);
+}
+
+template <bool kStats>
+__global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
+    __shared__ unsigned long long s_red[32];
+    BfsCtl *ctl = a.ctl;
+    const int lane = threadIdx.x & 31;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthreads = gridDim.x * blockDim.x;
+    const int gwarp = gtid >> 5, nwarps = nthreads >> 5;
+    const int W = (a.n + 31) >> 5;
+    const int W_act = (a.n_active + 31) >> 5;
+
+    for (int i = gtid; i < a.n; i += nthreads) {
+        a.depth[i] = -1;
+        a.parent[i] = -1;
+    }
+    for (int i = gtid; i < W; i += nthreads) {
+        a.visited[i] = 0;
+        a.fb0[i] = 0;
+        a.fb1[i] = 0;
+        a.fb2[i] = 0;
+    }
+    const unsigned long long t_start = globaltimer_ns();
+    if (!grid_barrier(&ctl->gs)) return;
+    if (gtid == 0) {
+        const int32_t s = a.src;
+        a.depth[s] = 0;
+        a.parent[s] = s;
+        a.visited[s >> 5] = 1u << (s & 31);
+        a.fb0[s >> 5] = 1u << (s & 31);
+        a.q0[0] = s;
+        ctl->cnt[0].nf = 1;
+        ctl->cnt[0].mf = (unsigned long long)(a.index[s + 1] - a.index[s]);
+    }
+    if (!grid_barrier(&ctl->gs)) return;
+
+    // Direction state (identical in every block).
+    bool push = a.direction != 2;
+    bool have_queue = true;
+    long long edges_to_check = a.m;
+    long long num_edges = (long long)(a.index[a.src + 1] - a.index[a.src]);
+    unsigned long long my_vscan = 0, my_escan = 0, my_found = 0;
+    int L = 0, td_levels = 0, bu_levels = 0;
+
+    for (;;) {
+        const int cur = L % 3, nxt = (L + 1) % 3, old = (L + 2) % 3;
+        int nf = __ldcg(&ctl->cnt[cur].nf);
+        if (nf == 0) break;
+        if (L >= a.max_levels) {
+            if (gtid == 0) atomicExch(&ctl->gs.err, (int)HC_ERR_NOT_CONVERGED);
+            break;
+        }
+        if (gtid == 0) {
+            if (globaltimer_ns() - t_start > kRunLimitNs) atomicExch(&ctl->gs.err, (int)HC_ERR_TIMEOUT);
+            ctl->cnt[old].nf = 0;
+            ctl->cnt[old].tasks = 0;
+            ctl->cnt[old].mf = 0;
+        }
+        uint32_t *fcur = fb_sel(a, cur), *fnext = fb_sel(a, nxt), *fold = fb_sel(a, old);
+        for (int i = gtid; i < W_act; i += nthreads) fold[i] = 0;
+        int32_t *qcur = (L & 1) ? a.q1 : a.q0;
+        int32_t *qnext = (L & 1) ? a.q0 : a.q1;
+
+        if (a.direction == 0 && push && num_edges > edges_to_check / a.alpha) push = false;
+
+        if (push) {
+            if (!have_queue) {
+                // Frontier came from a bottom-up level: compact its bitmap.
+                for (int w0 = gwarp * 32; w0 < W_act; w0 += nwarps * 32) {
+                    const int w = w0 + lane;
+                    uint32_t bits = w < W_act ? __ldcg(fcur + w) : 0u;
+                    int total;
+                    int pos = warp_exclusive_scan(__popc(bits), &total);
+                    int base = 0;
+                    if (lane == 0 && total) base = atomicAdd(&ctl->conv, total);
+                    pos += __shfl_sync(kFull, base, 0);
+                    while (bits) {
+                        const int b = __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        qcur[pos++] = w * 32 + b;
+                    }
+                }
+                if (!grid_barrier(&ctl->gs)) return;
+                nf = __ldcg(&ctl->conv);
+                have_queue = true;
+            }
+            edges_to_check -= num_edges;
+            td_levels++;
+            const int next_depth = L + 1;
+            unsigned long long mf_local = 0;
+            auto visit = [&](bool act, int32_t u, int64_t e) {
+                bool take = false;
+                int32_t v = 0;
+                if (act) {
+                    v = a.nbr[e];
+                    const uint32_t bit = 1u << (v & 31);
+                    if (!(__ldcg(a.visited + (v >> 5)) & bit) && atomicCAS(a.parent + v, -1, u) == -1) {
+                        a.depth[v] = next_depth;
+                        atomicOr(a.visited + (v >> 5), bit);
+                        atomicOr(fnext + (v >> 5), bit);
+                        mf_local += (unsigned long long)(a.index[v + 1] - a.index[v]);
+                        take = true;
+                    }
+                }
+                warp_append(take, v, qnext, &ctl->cnt[nxt].nf);
+            };
+            if (kStats) {
+                for (int i = gtid; i < nf; i += nthreads) {
+                    const int32_t u = __ldcg(qcur + i);
+                    my_escan += (unsigned long long)(a.index[u + 1] - a.index[u]);
+                }
+                if (gtid == 0) my_vscan += nf;
+            }
+            expand_small(a.index, qcur, nf, a.tasks, &ctl->cnt[cur].tasks, gwarp, nwarps, visit);
+            if (!grid_barrier(&ctl->gs)) return;
+            const int nt = __ldcg(&ctl->cnt[cur].tasks);
+            if (nt > 0) {
+                expand_tasks(a.index, a.tasks, nt, gwarp, nwarps, visit);
+            }
+            unsigned long long mf_blk = block_sum(mf_local, s_red);
+            if (threadIdx.x == 0 && mf_blk) atomicAdd(&ctl->cnt[nxt].mf, mf_blk);
+            if (!grid_barrier(&ctl->gs)) return;
+            num_edges = (long long)__ldcg(&ctl->cnt[nxt].mf);
+            have_queue = true;
+        } else {
+            bu_levels++;
+            const int next_depth = L + 1;
+            int found_local = 0;
+            // Rows of degree >= 32: warp per vertex, 32 probes per step.
+            const int n_warp = a.bu_variant == HC_VARIANT_WARP
+                                   ? a.n_active
+                                   : (a.bu_variant == HC_VARIANT_THREAD ? 0 : a.n_warp_rows);
+            const int n_warp_al = min(((n_warp + 31) >> 5) << 5, W_act << 5);
+            for (int v = gwarp; v < n_warp_al; v += nwarps) {
+                if (v >= a.n_active) break;
+                const uint32_t bit = 1u << (v & 31);
+                if (__ldcg(a.visited + (v >> 5)) & bit) continue;
+                const int64_t b = a.index[v], e = a.index[v + 1];
+                int32_t par = -1;
+                int64_t probes = 0;
+                for (int64_t e0 = b; e0 < e; e0 += 32) {
+                    const int64_t i = e0 + lane;
+                    bool hit = false;
+                    int32_t u = 0;
+                    if (i < e) {
+                        u = a.nbr[i];
+                        hit = (__ldcg(fcur + (u >> 5)) >> (u & 31)) & 1u;
+                    }
+                    const unsigned bal = __ballot_sync(kFull, hit);
+                    if (kStats) probes += bal ? (int64_t)__ffs(bal) : ((e - e0) < 32 ? (e - e0) : (int64_t)32);
+                    if (bal) {
+                        par = __shfl_sync(kFull, u, __ffs(bal) - 1);
+                        break;
+                    }
+                }
+                if (kStats && lane == 0) {
+                    my_vscan++;
+                    my_escan += probes;
+                }
+                if (par >= 0 && lane == 0) {
+                    a.parent[v] = par;
+                    a.depth[v] = next_depth;
+                    atomicOr(a.visited + (v >> 5), bit);
+                    atomicOr(fnext + (v >> 5), bit);
+                    found_local++;
+                }
+            }
+            // Remaining rows: thread per vertex, warp owns one bitmap word.
+            for (int w = (n_warp_al >> 5) + gwarp; w < W_act; w += nwarps) {
+                const uint32_t vis = __ldcg(a.visited + w);
+                const int v = w * 32 + lane;
+                int32_t par = -1;
+                if (v < a.n_active && !((vis >> lane) & 1u)) {
+                    const int64_t b = a.index[v], e = a.index[v + 1];
+                    for (int64_t i = b; i < e; i++) {
+                        const int32_t u = a.nbr[i];
+                        if ((__ldcg(fcur + (u >> 5)) >> (u & 31)) & 1u) {
+                            par = u;
+                            if (kStats) my_escan += (unsigned long long)(i - b + 1);
+                            break;
+                        }
+                    }
+                    if (kStats) {
+                        my_vscan++;
+                        if (par < 0) my_escan += (unsigned long long)(e - b);
+                    }
+                }
+                const unsigned bal = __ballot_sync(kFull, par >= 0);
+                if (par >= 0) {
+                    a.parent[v] = par;
+                    a.depth[v] = next_depth;
+                }
+                if (lane == 0) {
+                    fnext[w] = bal;
+                    if (bal) a.visited[w] = vis | bal;
+                    found_local += __popc(bal);
+                }
+            }
+            unsigned long long f_blk = block_sum((unsigned long long)found_local, s_red);
+            if (threadIdx.x == 0 && f_blk) atomicAdd((unsigned long long *)&ctl->reached, f_blk);
+            if (threadIdx.x == 0 && f_blk) atomicAdd(&ctl->cnt[nxt].nf, (int)f_blk);
+            if (gtid == 0) ctl->conv = 0;
+            if (!grid_barrier(&ctl->gs)) return;
+            const int nf_next = __ldcg(&ctl->cnt[nxt].nf);
+            if (a.direction == 0 && !(nf_next > nf || nf_next > a.n / a.beta)) {
+                push = true;
+                num_edges = 1;
+            }
+            have_queue = false;
+        }
+        (void)my_found;
+        L++;
+    }
+
+    if (kStats) {
+        unsigned long long v = block_sum(my_vscan, s_red);
+        if (threadIdx.x == 0 && v) atomicAdd(&ctl->vscan, v);
+        unsigned long long e = block_sum(my_escan, s_red);
+        if (threadIdx.x == 0 && e) atomicAdd(&ctl->escan, e);
+    }
+    if (gtid == 0) {
+        ctl->levels = L;
+        ctl->td_levels = td_levels;
+        ctl->bu_levels = bu_levels;
+    }
+}
+
+// Discovered count for top-down levels is the queue length; add it up after
+// the run from the per-level counters is not possible (they rotate), so the
+// reached total is recounted from the depth array.
+__global__ void count_reached(const int32_t *depth, int32_t n, unsigned long long *out) {
+    __shared__ unsigned long long s_red[32];
+    unsigned long long c = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        c += depth[i] >= 0;
+    c = block_sum(c, s_red);
+    if (threadIdx.x == 0 && c) atomicAdd(out, c);
+}
+
+template <bool kStats>
+hc_status launch_bfs(hc_graph *g, const BfsArgs &args) {
+    static int blocks_per_sm[2] = {0, 0};
+    int &bps = blocks_per_sm[kStats ? 1 : 0];
+    if (bps == 0) {
+        HC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, bfs_persistent<kStats>, kBfsThreads, 0));
+        if (bps < 1) return fail(HC_ERR_CUDA, "BFS kernel cannot be resident");
+    }
+    dim3 grid(g->sm_count * bps), block(kBfsThreads);
+    BfsArgs a = args;
+    void *params[] = {&a};
+    HC_CUDA_TRY(cudaLaunchCooperativeKernel((void *)bfs_persistent<kStats>, grid, block, params, 0, g->stream));
+    return HC_OK;
+}
+
+}  // namespace
+}  // namespace hc
+
+using namespace hc;
+
+extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sources, int32_t *depth_out,
+                            int32_t *parent_out, const hc_bfs_opts *opts, hc_bfs_stats *stats) {
+    clear_error();
+    HC_TRY(activate(g));
+    if (!sources || num_sources < 0) return fail(HC_ERR_INVALID_ARG, "hc_bfs: bad source list");
+    hc_bfs_opts o{};
+    if (opts) o = *opts;
+    if (o.alpha <= 0) o.alpha = 15;
+    if (o.beta <= 0) o.beta = 18;
+    if (o.direction < 0 || o.direction > 2) return fail(HC_ERR_INVALID_ARG, "hc_bfs: direction must be 0, 1 or 2");
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+
+    std::vector<int32_t> src(num_sources);
+    HC_CUDA_TRY(cudaMemcpy(src.data(), sources, sizeof(int32_t) * num_sources, cudaMemcpyDefault));
+    for (int32_t s : src)
+        if (s < 0 || s >= g->N) return fail(HC_ERR_INVALID_ARG, "hc_bfs: source %d outside [0, %d)", s, g->N);
+
+    const int64_t n = g->N;
+    const int64_t W = (n + 31) / 32;
+    const int64_t ntasks = max_expand_tasks(g->M, n);
+    const size_t bytes = sizeof(uint32_t) * 4 * W + sizeof(int32_t) * 2 * n + sizeof(int2) * ntasks + 1024;
+    HC_TRY(g->ws_bfs.ensure(bytes));
+    HC_TRY(g->ws_ctl.ensure(4096));
+    char *p = g->ws_bfs.as<char>();
+    auto take = [&](size_t b) {
+        char *r = p;
+        p += (b + 255) / 256 * 256;
+        return r;
+    };
+    BfsArgs a{};
+    a.index = g->index.as<int64_t>();
+    a.nbr = g->nbr.as<int32_t>();
+    a.n = g->N;
+    a.n_active = g->n_active;
+    a.n_warp_rows = g->n_warp_rows;
+    a.m = g->M;
+    a.visited = (uint32_t *)take(4 * W);
+    a.fb0 = (uint32_t *)take(4 * W);
+    a.fb1 = (uint32_t *)take(4 * W);
+    a.fb2 = (uint32_t *)take(4 * W);
+    a.q0 = (int32_t *)take(4 * n);
+    a.q1 = (int32_t *)take(4 * n);
+    a.tasks = (int2 *)take(sizeof(int2) * ntasks);
+    a.ctl = g->ws_ctl.as<BfsCtl>();
+    a.alpha = o.alpha;
+    a.beta = o.beta;
+    a.direction = o.direction;
+    a.bu_variant = (int)o.bu_variant;
+    a.max_levels = g->N + 1;
+
+    const bool dev_depth = is_device_pointer(depth_out);
+    const bool dev_parent = is_device_pointer(parent_out);
+    if (!dev_depth) HC_TRY(g->ws_out0.ensure(4 * n));
+    if (!dev_parent) HC_TRY(g->ws_out1.ensure(4 * n));
+
+    double total_ms = 0;
+    for (int32_t i = 0; i < num_sources; i++) {
+        a.src = src[i];
+        a.depth = dev_depth ? depth_out + (size_t)i * n : g->ws_out0.as<int32_t>();
+        a.parent = dev_parent ? parent_out + (size_t)i * n : g->ws_out1.as<int32_t>();
+        HC_CUDA_TRY(cudaMemsetAsync(a.ctl, 0, sizeof(BfsCtl), g->stream));
+        HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
+        HC_TRY(o.collect_stats ? launch_bfs<true>(g, a) : launch_bfs<false>(g, a));
+        HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
+        if (depth_out && !dev_depth) HC_TRY(copy_out(depth_out + (size_t)i * n, a.depth, 4 * n, g->stream));
+        if (parent_out && !dev_parent) HC_TRY(copy_out(parent_out + (size_t)i * n, a.parent, 4 * n, g->stream));
+        BfsCtl c;
+        HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
+        if (stats) {
+            unsigned long long *cnt = (unsigned long long *)((char *)a.ctl + 2048);
+            HC_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, g->stream));
+            count_reached<<<g->sm_count * 4, 256, 0, g->stream>>>(a.depth, g->N, cnt);
+            unsigned long long reached = 0;
+            HC_CUDA_TRY(cudaMemcpyAsync(&reached, cnt, 8, cudaMemcpyDeviceToHost, g->stream));
+            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            stats->reached += (int32_t)reached;
+        }
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (c.gs.err) return fail((hc_status)c.gs.err, "hc_bfs: device run from source %d ended with status %d",
+                                  src[i], c.gs.err);
+        float ms = 0;
+        HC_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_start, g->ev_stop));
+        total_ms += ms;
+        if (stats) {
+            stats->levels = std::max(stats->levels, c.levels);
+            stats->td_levels += c.td_levels;
+            stats->bu_levels += c.bu_levels;
+            stats->vertices_scanned += (int64_t)c.vscan;
+            stats->edges_scanned += (int64_t)c.escan;
+        }
+    }
+    if (stats) {
+        stats->ms = total_ms;
+        // Streamed bytes: 16 B offsets per scanned vertex, 4 B per scanned edge,
+        // 4 B per discovered vertex, and for bottom-up levels two bitmap sweeps.
+        stats->bytes_model = 16.0 * (double)stats->vertices_scanned + 4.0 * (double)stats->edges_scanned +
+                             4.0 * (double)stats->reached +
+                             2.0 * ((double)g->N / 8.0) * (double)stats->bu_levels;
+    }
+    return HC_OK;
+}

@@ -1,0 +1,180 @@
+// Device-side building blocks shared by the BFS / SSSP / PageRank kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "hc_common.h"
+
+#define HC_CUDA_TRY(expr)                                                        \
+    do {                                                                         \
+        cudaError_t _e = (expr);                                                 \
+        if (_e != cudaSuccess)                                                   \
+            return ::hc::fail(_e == cudaErrorMemoryAllocation ? HC_ERR_OOM      \
+                                                               : HC_ERR_CUDA,   \
+                              "%s failed: %s (%s:%d)", #expr,                    \
+                              cudaGetErrorString(_e), __FILE__, __LINE__);       \
+    } while (0)
+
+#define HC_TRY(expr)                        \
+    do {                                    \
+        hc_status _s = (expr);              \
+        if (_s != HC_OK) return _s;         \
+    } while (0)
+
+namespace hc {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int32_t kInfDist = 0x7fffffff;
+
+// Bound on every device-side spin: a wait that lasts longer than this gives
+// up, records HC_ERR_TIMEOUT and lets the kernel return.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+// Bound on one persistent run (all its epochs): past it the run records
+// HC_ERR_TIMEOUT and every block leaves at the next barrier.
+constexpr unsigned long long kRunLimitNs = 20000000000ull;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier for cooperative (co-resident) launches.  Arrival is an
+// atomic on `count`; the last block to arrive resets it and bumps `gen`.
+// Waiters poll `gen` with an acquire load and give up after kWaitLimitNs,
+// setting *err.  Once *err is set every later barrier returns at once, so a
+// failed run drains in bounded time.  Returns false when the run must stop.
+struct GridSync {
+    unsigned count;
+    unsigned gen;
+    int err;
+    int pad;
+};
+
+__device__ __forceinline__ bool grid_barrier(GridSync *gs) {
+    __syncthreads();
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        if (*(volatile int *)&gs->err) {
+            ok = 0;
+        } else {
+            unsigned my_gen = ld_acquire_u32(&gs->gen);
+            __threadfence();
+            unsigned arrived = atomicAdd(&gs->count, 1u);
+            if (arrived == gridDim.x - 1) {
+                gs->count = 0;
+                __threadfence();
+                st_release_u32(&gs->gen, my_gen + 1);
+            } else {
+                unsigned long long t0 = globaltimer_ns();
+                while (ld_acquire_u32(&gs->gen) == my_gen) {
+                    if (*(volatile int *)&gs->err) { ok = 0; break; }
+                    if (globaltimer_ns() - t0 > kWaitLimitNs) {
+                        atomicExch(&gs->err, (int)HC_ERR_TIMEOUT);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Warp-level helpers (full mask; the reference's ALLWARP mask at
+// src/cuda.cuh:24 evaluates to 0x80000000, which is not a full warp).
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+template <class T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+// Exclusive prefix sum across the warp; *total receives the warp total.
+template <class T>
+__device__ __forceinline__ T warp_exclusive_scan(T v, T *total) {
+    const int lane = threadIdx.x & 31;
+    T x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    *total = __shfl_sync(kFull, x, 31);
+    return x - v;
+}
+
+// Block-wide sum of a per-thread value (blockDim.x a multiple of 32, <= 1024).
+template <class T>
+__device__ __forceinline__ T block_sum(T v, T *smem32) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) smem32[w] = v;
+    __syncthreads();
+    T r = 0;
+    if (w == 0) {
+        r = lane < (int)(blockDim.x >> 5) ? smem32[lane] : T(0);
+        r = warp_sum(r);
+    }
+    return r;  // valid in thread 0
+}
+
+// L2-coherent loads for state that other blocks write during a launch.
+__device__ __forceinline__ int32_t ld_cg(const int32_t *p) { return __ldcg(p); }
+__device__ __forceinline__ uint32_t ld_cg(const uint32_t *p) { return __ldcg(p); }
+
+// ------------------------------------------------------------- host helpers
+
+// True when `p` is device (or managed) memory of the current context.
+bool is_device_pointer(const void *p);
+
+// Device buffer that grows on demand and is freed with its owner.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    hc_status ensure(size_t want);
+    void release();
+    template <class T>
+    T *as() const { return reinterpret_cast<T *>(ptr); }
+};
+
+// Pinned host buffer that grows on demand.
+struct PinnedBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    hc_status ensure(size_t want);
+    void release();
+    template <class T>
+    T *as() const { return reinterpret_cast<T *>(ptr); }
+};
+
+// Copies between user memory (host or device) and HBM on `s`.
+hc_status copy_in(void *dst_dev, const void *src_any, size_t bytes, cudaStream_t s);
+hc_status copy_out(void *dst_any, const void *src_dev, size_t bytes, cudaStream_t s);
+
+}  // namespace hc

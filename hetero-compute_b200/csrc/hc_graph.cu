@@ -1,0 +1,361 @@
+// Device graph handle: upload, validation, degree analysis and the derived
+// arrays PageRank needs.  Replaces the per-call cudaMalloc + H2D of the
+// reference drivers (src/kernels/gpu/sssp.cuh:51-61, src/graph.cuh:250-286).
+#include <algorithm>
+#include <cstring>
+
+#include "hc_graph.cuh"
+
+namespace hc {
+
+constexpr int64_t kNbrPad = 64;
+
+bool is_device_pointer(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes attr;
+    cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+hc_status DevBuf::ensure(size_t want) {
+    if (want <= bytes && ptr) return HC_OK;
+    release();
+    size_t b = std::max<size_t>(want, 256);
+    cudaError_t e = cudaMalloc(&ptr, b);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ptr = nullptr;
+        return fail(HC_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", b, cudaGetErrorString(e));
+    }
+    bytes = b;
+    return HC_OK;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+hc_status PinnedBuf::ensure(size_t want) {
+    if (want <= bytes && ptr) return HC_OK;
+    release();
+    size_t b = std::max<size_t>(want, 4096);
+    cudaError_t e = cudaMallocHost(&ptr, b);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ptr = nullptr;
+        return fail(HC_ERR_OOM, "cudaMallocHost of %zu bytes failed: %s", b, cudaGetErrorString(e));
+    }
+    bytes = b;
+    return HC_OK;
+}
+
+void PinnedBuf::release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+hc_status copy_in(void *dst_dev, const void *src_any, size_t bytes, cudaStream_t s) {
+    if (!bytes) return HC_OK;
+    HC_CUDA_TRY(cudaMemcpyAsync(dst_dev, src_any, bytes, cudaMemcpyDefault, s));
+    return HC_OK;
+}
+
+hc_status copy_out(void *dst_any, const void *src_dev, size_t bytes, cudaStream_t s) {
+    if (!bytes) return HC_OK;
+    HC_CUDA_TRY(cudaMemcpyAsync(dst_any, src_dev, bytes, cudaMemcpyDefault, s));
+    return HC_OK;
+}
+
+hc_status activate(hc_graph *g) {
+    if (!g) return fail(HC_ERR_INVALID_ARG, "null graph handle");
+    HC_CUDA_TRY(cudaSetDevice(g->device));
+    return HC_OK;
+}
+
+namespace {
+
+struct Analysis {
+    int unsorted;      // degrees increase somewhere
+    int first_zero;    // first vertex of degree 0 (N if none)
+    int max_degree;
+    int first_small;   // first vertex of degree < 32 (N if none)
+    int bad_index;     // offsets decrease or exceed [0, M]
+    int bad_nbr;       // neighbour outside [0, N)
+    int rows_unsorted; // some row not strictly increasing
+    int pad;
+};
+
+__global__ void analyze_index(const int64_t *index, int32_t n, int64_t m, Analysis *out) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        int64_t b = index[v], e = index[v + 1];
+        if (b < 0 || e < b || e > m) {
+            out->bad_index = 1;
+            continue;
+        }
+        int64_t d = e - b;
+        if (v + 1 < n) {
+            int64_t d2 = index[v + 2] - e;
+            if (d2 > d) out->unsorted = 1;
+        }
+        if (d == 0) atomicMin(&out->first_zero, v);
+        if (d < 32) atomicMin(&out->first_small, v);
+        atomicMax(&out->max_degree, (int)(d > 0x7fffffffll ? 0x7fffffffll : d));
+    }
+}
+
+// Neighbour range and row order; only run once the index checked out.
+__global__ void analyze_rows(const int64_t *index, const int32_t *nbr, int32_t n, Analysis *out) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        int64_t b = index[v], e = index[v + 1];
+        for (int64_t i = b + lane; i < e; i += 32) {
+            int32_t x = nbr[i];
+            if (x < 0 || x >= n) out->bad_nbr = 1;
+            if (i + 1 < e && nbr[i + 1] <= x) out->rows_unsorted = 1;
+        }
+    }
+}
+
+__global__ void build_inv_deg(const int64_t *index, int32_t n, float *inv_deg) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        int64_t d = index[v + 1] - index[v];
+        inv_deg[v] = d ? 1.0f / (float)d : 0.0f;
+    }
+}
+
+// Row sums of the raw weights (warp per row), stored as reciprocals.
+__global__ void build_inv_wsum(const int64_t *index, const float *w, int32_t n, float *inv_wsum) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        int64_t b = index[v], e = index[v + 1];
+        double s = 0.0;
+        for (int64_t i = b + lane; i < e; i += 32) s += (double)w[i];
+        s = warp_sum(s);
+        if (lane == 0) inv_wsum[v] = s > 0.0 ? (float)(1.0 / s) : 0.0f;
+    }
+}
+
+// wtn[slot (v,i)] = w[u -> v] / sum_k w[u -> k] with u = nbr[v][i]: the weight
+// the forward pull at v needs, stored in v's own row so the pull streams it.
+// Rows are sorted, so the reverse slot is found by binary search in row u.
+__global__ void build_wtn(const int64_t *index, const int32_t *nbr, const float *w,
+                          const float *inv_wsum, int32_t n, float *wtn, int *missing) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        int64_t b = index[v], e = index[v + 1];
+        for (int64_t i = b + lane; i < e; i += 32) {
+            int32_t u = nbr[i];
+            int64_t lo = index[u], hi = index[u + 1];
+            while (lo < hi) {
+                int64_t mid = (lo + hi) >> 1;
+                if (nbr[mid] < v) lo = mid + 1; else hi = mid;
+            }
+            if (lo < index[u + 1] && nbr[lo] == v) {
+                wtn[i] = w[lo] * inv_wsum[u];
+            } else {
+                wtn[i] = 0.0f;
+                *missing = 1;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+hc_status ensure_pr_derived(hc_graph *g, bool weighted) {
+    const int grid = g->sm_count * 8, block = 256;
+    if (!g->inv_deg.ptr) {
+        HC_TRY(g->inv_deg.ensure(sizeof(float) * std::max<int32_t>(g->N, 1)));
+        build_inv_deg<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->N, g->inv_deg.as<float>());
+        HC_CUDA_TRY(cudaGetLastError());
+    }
+    if (weighted && !g->wtn.ptr) {
+        if (g->wtype != HC_W_F32)
+            return fail(HC_ERR_UNSUPPORTED, "weighted PageRank needs fp32 edge weights");
+        HC_TRY(g->inv_wsum.ensure(sizeof(float) * std::max<int32_t>(g->N, 1)));
+        HC_TRY(g->wtn.ensure(sizeof(float) * (size_t)(g->M + kNbrPad)));
+        build_inv_wsum<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->wgt.as<float>(), g->N,
+                                                        g->inv_wsum.as<float>());
+        HC_CUDA_TRY(cudaGetLastError());
+        DevBuf flag;
+        HC_TRY(flag.ensure(sizeof(int)));
+        HC_CUDA_TRY(cudaMemsetAsync(flag.ptr, 0, sizeof(int), g->stream));
+        build_wtn<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
+                                                   g->wgt.as<float>(), g->inv_wsum.as<float>(), g->N,
+                                                   g->wtn.as<float>(), flag.as<int>());
+        HC_CUDA_TRY(cudaGetLastError());
+        int missing = 0;
+        HC_CUDA_TRY(cudaMemcpyAsync(&missing, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        flag.release();
+        if (missing) {
+            g->wtn.release();
+            return fail(HC_ERR_INVALID_ARG,
+                        "weighted PageRank needs a symmetric structure with sorted rows "
+                        "(an edge u->v has no v->u slot)");
+        }
+    }
+    return HC_OK;
+}
+
+}  // namespace hc
+
+int64_t hc_graph::bytes_held() const {
+    const hc::DevBuf *bufs[] = {&index, &nbr, &wgt, &inv_deg, &inv_wsum, &wtn, &pr_plan,
+                                &pr_plan_huge_rows, &ws_bfs, &ws_sssp, &ws_pr, &ws_batch,
+                                &ws_out0, &ws_out1, &ws_ctl};
+    int64_t t = 0;
+    for (auto *b : bufs) t += (int64_t)b->bytes;
+    return t;
+}
+
+using namespace hc;
+
+extern "C" {
+
+hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const void *weights,
+                          hc_wtype wtype, int32_t num_nodes, int64_t num_edges, int32_t device,
+                          hc_graph **out) {
+    clear_error();
+    if (!out) return fail(HC_ERR_INVALID_ARG, "hc_graph_create: null output handle");
+    *out = nullptr;
+    if (!index || num_nodes < 1 || num_edges < 0 || (num_edges > 0 && !neighbors))
+        return fail(HC_ERR_INVALID_ARG, "hc_graph_create: bad CSR (N=%d, M=%lld)", num_nodes,
+                    (long long)num_edges);
+    if (wtype != HC_W_NONE && !weights)
+        return fail(HC_ERR_INVALID_ARG, "hc_graph_create: weight type given without weights");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(HC_ERR_NO_DEVICE, "hc_graph_create: no CUDA device visible");
+    }
+    if (device < 0 || device >= ndev)
+        return fail(HC_ERR_INVALID_ARG, "hc_graph_create: device %d out of range (%d)", device, ndev);
+    HC_CUDA_TRY(cudaSetDevice(device));
+
+    hc_graph *g = new hc_graph();
+    g->device = device;
+    g->N = num_nodes;
+    g->M = num_edges;
+    g->wtype = wtype;
+    auto bail = [&](hc_status s) {
+        hc_graph_destroy(g);
+        return s;
+    };
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return bail(fail(HC_ERR_CUDA, "cudaGetDeviceProperties failed"));
+    g->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(HC_ERR_CUDA, "cudaStreamCreate failed"));
+    g->stream = g->own_stream;
+    if (cudaEventCreate(&g->ev_start) != cudaSuccess || cudaEventCreate(&g->ev_stop) != cudaSuccess)
+        return bail(fail(HC_ERR_CUDA, "cudaEventCreate failed"));
+
+    hc_status st;
+    if ((st = g->index.ensure(sizeof(int64_t) * ((size_t)num_nodes + 1))) != HC_OK) return bail(st);
+    if ((st = g->nbr.ensure(sizeof(int32_t) * (size_t)(num_edges + kNbrPad))) != HC_OK) return bail(st);
+    if (cudaMemsetAsync(g->nbr.ptr, 0, g->nbr.bytes, g->stream) != cudaSuccess)
+        return bail(fail(HC_ERR_CUDA, "memset failed"));
+    if ((st = copy_in(g->index.ptr, index, sizeof(int64_t) * ((size_t)num_nodes + 1), g->stream)) != HC_OK)
+        return bail(st);
+    if ((st = copy_in(g->nbr.ptr, neighbors, sizeof(int32_t) * (size_t)num_edges, g->stream)) != HC_OK)
+        return bail(st);
+    if (wtype != HC_W_NONE) {
+        if ((st = g->wgt.ensure(4 * (size_t)(num_edges + kNbrPad))) != HC_OK) return bail(st);
+        if (cudaMemsetAsync(g->wgt.ptr, 0, g->wgt.bytes, g->stream) != cudaSuccess)
+            return bail(fail(HC_ERR_CUDA, "memset failed"));
+        if ((st = copy_in(g->wgt.ptr, weights, 4 * (size_t)num_edges, g->stream)) != HC_OK) return bail(st);
+    }
+
+    // Validate and analyse on the device (works for host or device inputs).
+    DevBuf abuf;
+    if ((st = abuf.ensure(sizeof(Analysis))) != HC_OK) return bail(st);
+    Analysis init;
+    std::memset(&init, 0, sizeof(init));
+    init.first_zero = num_nodes;
+    init.first_small = num_nodes;
+    int64_t ends[2] = {0, 0};
+    if (cudaMemcpyAsync(abuf.ptr, &init, sizeof(init), cudaMemcpyHostToDevice, g->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&ends[0], g->index.as<int64_t>(), 8, cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&ends[1], g->index.as<int64_t>() + num_nodes, 8, cudaMemcpyDeviceToHost, g->stream) != cudaSuccess)
+        return bail(fail(HC_ERR_CUDA, "analysis setup failed"));
+    const int grid = g->sm_count * 8;
+    analyze_index<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), num_nodes, num_edges, abuf.as<Analysis>());
+    Analysis res;
+    if (cudaMemcpyAsync(&res, abuf.ptr, sizeof(res), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
+        cudaStreamSynchronize(g->stream) != cudaSuccess)
+        return bail(fail(HC_ERR_CUDA, "graph analysis failed: %s", cudaGetErrorString(cudaGetLastError())));
+    if (ends[0] != 0 || ends[1] != num_edges || res.bad_index)
+        return bail(fail(HC_ERR_INVALID_ARG,
+                         "hc_graph_create: index must be non-decreasing from 0 to num_edges"));
+    analyze_rows<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), num_nodes,
+                                                abuf.as<Analysis>());
+    if (cudaMemcpyAsync(&res, abuf.ptr, sizeof(res), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
+        cudaStreamSynchronize(g->stream) != cudaSuccess)
+        return bail(fail(HC_ERR_CUDA, "graph analysis failed: %s", cudaGetErrorString(cudaGetLastError())));
+    if (res.bad_nbr) return bail(fail(HC_ERR_INVALID_ARG, "hc_graph_create: neighbour id outside [0, N)"));
+
+    g->degree_sorted = !res.unsorted;
+    g->max_degree = res.max_degree;
+    g->n_active = g->degree_sorted ? res.first_zero : num_nodes;
+    if (g->degree_sorted) {
+        int32_t r = (int32_t)std::min<int64_t>(((int64_t)res.first_small + 31) / 32 * 32, num_nodes);
+        g->n_warp_rows = r;
+    } else {
+        g->n_warp_rows = 0;
+    }
+    *out = g;
+    return HC_OK;
+}
+
+hc_status hc_graph_destroy(hc_graph *g) {
+    if (!g) return HC_OK;
+    cudaSetDevice(g->device);
+    if (g->own_stream) cudaStreamSynchronize(g->own_stream);
+    if (g->stream && g->stream != g->own_stream) cudaStreamSynchronize(g->stream);
+    DevBuf *bufs[] = {&g->index, &g->nbr, &g->wgt, &g->inv_deg, &g->inv_wsum, &g->wtn, &g->pr_plan,
+                      &g->pr_plan_huge_rows, &g->ws_bfs, &g->ws_sssp, &g->ws_pr, &g->ws_batch,
+                      &g->ws_out0, &g->ws_out1, &g->ws_ctl};
+    for (auto *b : bufs) b->release();
+    g->pinned.release();
+    if (g->ev_start) cudaEventDestroy(g->ev_start);
+    if (g->ev_stop) cudaEventDestroy(g->ev_stop);
+    if (g->own_stream) cudaStreamDestroy(g->own_stream);
+    delete g;
+    return HC_OK;
+}
+
+hc_status hc_graph_set_stream(hc_graph *g, void *stream) {
+    clear_error();
+    if (!g) return fail(HC_ERR_INVALID_ARG, "null graph handle");
+    g->stream = stream ? (cudaStream_t)stream : g->own_stream;
+    return HC_OK;
+}
+
+hc_status hc_graph_get_info(const hc_graph *g, hc_graph_info *info) {
+    clear_error();
+    if (!g || !info) return fail(HC_ERR_INVALID_ARG, "null argument");
+    info->num_nodes = g->N;
+    info->num_edges = g->M;
+    info->num_active = g->n_active;
+    info->degree_sorted = g->degree_sorted;
+    info->max_degree = g->max_degree;
+    info->device = g->device;
+    info->wtype = g->wtype;
+    info->device_bytes = g->bytes_held();
+    return HC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,364 @@
+// Single-source shortest paths as one persistent cooperative launch per source.
+//
+// Reference path: sssp_pull_gpu (src/kernels/gpu/sssp.cuh:42-100) sweeps every
+// vertex each epoch with an in-place Bellman-Ford pull over float weights and
+// round-trips a counter to the host per epoch.  Here only vertices whose
+// distance dropped are expanded (push relaxation with int32 atomicMin), split
+// near/far by a moving threshold (Davidson et al., "Work-efficient parallel GPU
+// methods for single-source shortest paths", IPDPS 2014), and the epoch loop
+// stays on the device.  Distances are exact integers; unreachable = INT32_MAX.
+//
+// Working set (N vertices): dist int32[N]; near queues q[2] int32[N];
+// far piles far[2] int32[N]; stamp / fstamp int32[N] (queue dedup without
+// clearing: a vertex joins the epoch-E queue by raising stamp[v] to E);
+// tasks int2[] for long rows.
+#include <algorithm>
+#include <climits>
+#include <vector>
+
+#include "hc_expand.cuh"
+#include "hc_graph.cuh"
+
+namespace hc {
+namespace {
+
+constexpr int kSsspThreads = 512;
+
+struct SsspCtl {
+    GridSync gs;
+    int qlen[3];
+    int tasks[3];
+    int far_len[2];
+    int min_far;
+    int epochs, phases;
+    unsigned long long vproc, erelax;
+};
+
+struct SsspArgs {
+    const int64_t *index;
+    const int32_t *nbr;
+    const int32_t *w;
+    int32_t n;
+    int32_t *dist;
+    int32_t *q0, *q1, *far0, *far1, *stamp, *fstamp;
+    int2 *tasks;
+    SsspCtl *ctl;
+    int32_t src;
+    int32_t delta;  // <= 0: no far pile (plain frontier Bellman-Ford)
+    int max_epochs;
+};
+
+template <bool kStats>
+__global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
+    __shared__ unsigned long long s_red[32];
+    __shared__ int s_min[32];
+    SsspCtl *ctl = a.ctl;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthreads = gridDim.x * blockDim.x;
+    const int gwarp = gtid >> 5, nwarps = nthreads >> 5;
+    const int lane = threadIdx.x & 31;
+
+    for (int i = gtid; i < a.n; i += nthreads) {
+        a.dist[i] = kInfDist;
+        a.stamp[i] = -1;
+        a.fstamp[i] = -1;
+    }
+    const unsigned long long t_start = globaltimer_ns();
+    if (!grid_barrier(&ctl->gs)) return;
+    if (gtid == 0) {
+        a.dist[a.src] = 0;
+        a.stamp[a.src] = 0;
+        a.q0[0] = a.src;
+        ctl->qlen[0] = 1;
+        ctl->min_far = kInfDist;
+    }
+    if (!grid_barrier(&ctl->gs)) return;
+
+    const bool use_far = a.delta > 0;
+    int32_t T = use_far ? a.delta : kInfDist;
+    int E = 0, phase = 0;
+    unsigned long long my_v = 0, my_e = 0;
+
+    for (;;) {
+        const int cur = E % 3, nxt = (E + 1) % 3, old = (E + 2) % 3;
+        int32_t *qcur = (E & 1) ? a.q1 : a.q0;
+        int32_t *qnext = (E & 1) ? a.q0 : a.q1;
+        if (gtid == 0 && globaltimer_ns() - t_start > kRunLimitNs) atomicExch(&ctl->gs.err, (int)HC_ERR_TIMEOUT);
+        int nq = __ldcg(&ctl->qlen[cur]);
+        if (nq == 0) {
+            if (!use_far) break;
+            int32_t *fcur = (phase & 1) ? a.far1 : a.far0;
+            int32_t *fnew = (phase & 1) ? a.far0 : a.far1;
+            const int fl = __ldcg(&ctl->far_len[phase & 1]);
+            if (fl == 0) break;
+            // Smallest live distance in the far pile picks the next bucket.
+            int mn = kInfDist;
+            for (int i = gtid; i < fl; i += nthreads) {
+                const int32_t d = __ldcg(a.dist + __ldcg(fcur + i));
+                if (d >= T) mn = min(mn, d);
+            }
+            mn = warp_min(mn);
+            if (lane == 0) s_min[threadIdx.x >> 5] = mn;
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                int x = threadIdx.x < (blockDim.x >> 5) ? s_min[threadIdx.x] : kInfDist;
+                x = warp_min(x);
+                if (threadIdx.x == 0 && x < kInfDist) atomicMin(&ctl->min_far, x);
+            }
+            if (!grid_barrier(&ctl->gs)) return;
+            const int32_t mf = __ldcg(&ctl->min_far);
+            if (mf == kInfDist) break;
+            const int32_t T_old = T;
+            const long long tn = ((long long)mf / a.delta + 1) * (long long)a.delta;
+            T = (int32_t)(tn < (long long)kInfDist ? tn : (long long)kInfDist);
+            // Split: [T_old, T) joins the epoch-E queue, >= T stays far.
+            for (int i0 = gwarp * 32; i0 < fl; i0 += nwarps * 32) {
+                const int i = i0 + lane;
+                bool to_near = false, to_far = false;
+                int32_t v = 0;
+                if (i < fl) {
+                    v = __ldcg(fcur + i);
+                    const int32_t d = __ldcg(a.dist + v);
+                    if (d >= T_old && d < T) to_near = atomicMax(a.stamp + v, E) < E;
+                    else if (d >= T) to_far = atomicMax(a.fstamp + v, phase + 2) < phase + 2;
+                }
+                warp_append(to_near, v, qcur, &ctl->qlen[cur]);
+                warp_append(to_far, v, fnew, &ctl->far_len[(phase + 1) & 1]);
+            }
+            if (!grid_barrier(&ctl->gs)) return;
+            if (gtid == 0) {
+                ctl->far_len[phase & 1] = 0;
+                ctl->min_far = kInfDist;
+            }
+            phase++;
+            nq = __ldcg(&ctl->qlen[cur]);
+            if (nq == 0) continue;
+        }
+        if (E >= a.max_epochs) {
+            if (gtid == 0) atomicExch(&ctl->gs.err, (int)HC_ERR_NOT_CONVERGED);
+            break;
+        }
+        if (gtid == 0) {
+            ctl->qlen[old] = 0;
+            ctl->tasks[old] = 0;
+        }
+        int32_t *fpile = (phase & 1) ? a.far1 : a.far0;
+        int *fpile_len = &ctl->far_len[phase & 1];
+        const int next_e = E + 1;
+        auto relax = [&](bool act, int32_t u, int64_t e) {
+            bool near = false, far = false;
+            int32_t v = 0;
+            if (act) {
+                v = a.nbr[e];
+                const int32_t nd = __ldcg(a.dist + u) + a.w[e];
+                if (kStats) my_e++;
+                if (nd < __ldcg(a.dist + v)) {
+                    const int32_t prev = atomicMin(a.dist + v, nd);
+                    if (nd < prev) {
+                        if (nd < T) near = atomicMax(a.stamp + v, next_e) < next_e;
+                        else far = atomicMax(a.fstamp + v, phase + 1) < phase + 1;
+                    }
+                }
+            }
+            warp_append(near, v, qnext, &ctl->qlen[nxt]);
+            if (use_far) warp_append(far, v, fpile, fpile_len);
+        };
+        if (kStats && gtid == 0) my_v += nq;
+        expand_small(a.index, qcur, nq, a.tasks, &ctl->tasks[cur], gwarp, nwarps, relax);
+        if (!grid_barrier(&ctl->gs)) return;
+        const int nt = __ldcg(&ctl->tasks[cur]);
+        if (nt > 0) {
+            expand_tasks(a.index, a.tasks, nt, gwarp, nwarps, relax);
+            if (!grid_barrier(&ctl->gs)) return;
+        }
+        E++;
+    }
+    if (kStats) {
+        unsigned long long v = block_sum(my_v, s_red);
+        if (threadIdx.x == 0 && v) atomicAdd(&ctl->vproc, v);
+        unsigned long long e = block_sum(my_e, s_red);
+        if (threadIdx.x == 0 && e) atomicAdd(&ctl->erelax, e);
+    }
+    if (gtid == 0) {
+        ctl->epochs = E;
+        ctl->phases = phase;
+    }
+}
+
+// Shortest-path tree: any u with dist[u] + w(u->v) == dist[v] is a valid
+// parent (weights are non-negative integers).  Warp per source row, push
+// direction, so directed weights are read from the row that owns them.
+__global__ void sssp_parent_init(int32_t *parent, int32_t n, int32_t src) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        parent[v] = v == src ? src : -1;
+}
+
+__global__ void sssp_parents_fill(const int64_t *index, const int32_t *nbr, const int32_t *w, const int32_t *dist,
+                                  int32_t n, int32_t src, int32_t *parent) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += nw) {
+        const int32_t du = dist[u];
+        if (du == kInfDist) continue;
+        const int64_t b = index[u], e = index[u + 1];
+        for (int64_t i = b + lane; i < e; i += 32) {
+            const int32_t v = nbr[i];
+            if (v != src && du + w[i] == dist[v]) parent[v] = u;
+        }
+    }
+}
+
+__global__ void count_finite(const int32_t *dist, int32_t n, unsigned long long *out) {
+    __shared__ unsigned long long s_red[32];
+    unsigned long long c = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        c += dist[i] != kInfDist;
+    c = block_sum(c, s_red);
+    if (threadIdx.x == 0 && c) atomicAdd(out, c);
+}
+
+__global__ void weight_stats(const int32_t *w, int64_t m, int *neg, unsigned long long *sum) {
+    __shared__ unsigned long long s_red[32];
+    unsigned long long s = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t x = w[i];
+        if (x < 0) *neg = 1;
+        s += (unsigned long long)max(x, 0);
+    }
+    s = block_sum(s, s_red);
+    if (threadIdx.x == 0 && s) atomicAdd(sum, s);
+}
+
+template <bool kStats>
+hc_status launch_sssp(hc_graph *g, const SsspArgs &args) {
+    static int blocks_per_sm[2] = {0, 0};
+    int &bps = blocks_per_sm[kStats ? 1 : 0];
+    if (bps == 0) {
+        HC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sssp_persistent<kStats>, kSsspThreads, 0));
+        if (bps < 1) return fail(HC_ERR_CUDA, "SSSP kernel cannot be resident");
+    }
+    dim3 grid(g->sm_count * bps), block(kSsspThreads);
+    SsspArgs a = args;
+    void *params[] = {&a};
+    HC_CUDA_TRY(cudaLaunchCooperativeKernel((void *)sssp_persistent<kStats>, grid, block, params, 0, g->stream));
+    return HC_OK;
+}
+
+}  // namespace
+}  // namespace hc
+
+using namespace hc;
+
+extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_sources, int32_t *dist_out,
+                             int32_t *parent_out, const hc_sssp_opts *opts, hc_sssp_stats *stats) {
+    clear_error();
+    HC_TRY(activate(g));
+    if (!sources || num_sources < 0) return fail(HC_ERR_INVALID_ARG, "hc_sssp: bad source list");
+    if (g->wtype != HC_W_I32) return fail(HC_ERR_UNSUPPORTED, "hc_sssp: graph needs int32 edge weights");
+    hc_sssp_opts o{};
+    if (opts) o = *opts;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    std::vector<int32_t> src(num_sources);
+    HC_CUDA_TRY(cudaMemcpy(src.data(), sources, sizeof(int32_t) * num_sources, cudaMemcpyDefault));
+    for (int32_t s : src)
+        if (s < 0 || s >= g->N) return fail(HC_ERR_INVALID_ARG, "hc_sssp: source %d outside [0, %d)", s, g->N);
+
+    const int64_t n = g->N;
+    const int64_t ntasks = max_expand_tasks(g->M, n);
+    HC_TRY(g->ws_sssp.ensure(sizeof(int32_t) * 6 * n + sizeof(int2) * ntasks + 2048));
+    HC_TRY(g->ws_ctl.ensure(4096));
+    char *p = g->ws_sssp.as<char>();
+    auto take = [&](size_t b) {
+        char *r = p;
+        p += (b + 255) / 256 * 256;
+        return r;
+    };
+    SsspArgs a{};
+    a.index = g->index.as<int64_t>();
+    a.nbr = g->nbr.as<int32_t>();
+    a.w = g->wgt.as<int32_t>();
+    a.n = g->N;
+    a.q0 = (int32_t *)take(4 * n);
+    a.q1 = (int32_t *)take(4 * n);
+    a.far0 = (int32_t *)take(4 * n);
+    a.far1 = (int32_t *)take(4 * n);
+    a.stamp = (int32_t *)take(4 * n);
+    a.fstamp = (int32_t *)take(4 * n);
+    a.tasks = (int2 *)take(sizeof(int2) * ntasks);
+    a.ctl = g->ws_ctl.as<SsspCtl>();
+    a.max_epochs = o.max_epochs > 0 ? o.max_epochs : 0x7fffffff;
+
+    // Weights must be non-negative; the mean weight sets the default delta.
+    {
+        int *neg = (int *)((char *)a.ctl + 2048);
+        unsigned long long *sum = (unsigned long long *)((char *)a.ctl + 2056);
+        HC_CUDA_TRY(cudaMemsetAsync(neg, 0, 16, g->stream));
+        weight_stats<<<g->sm_count * 4, 256, 0, g->stream>>>(a.w, g->M, neg, sum);
+        int hneg = 0;
+        unsigned long long hsum = 0;
+        HC_CUDA_TRY(cudaMemcpyAsync(&hneg, neg, 4, cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaMemcpyAsync(&hsum, sum, 8, cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (hneg) return fail(HC_ERR_INVALID_ARG, "hc_sssp: negative edge weight");
+        if (o.delta == 0) {
+            const double wavg = g->M ? (double)hsum / (double)g->M : 1.0;
+            const double davg = g->n_active ? (double)g->M / (double)g->n_active : 1.0;
+            a.delta = (int32_t)std::max(1.0, std::min(1e9, wavg * 32.0 / std::max(davg, 1.0)));
+        } else {
+            a.delta = o.delta;
+        }
+    }
+
+    const bool dev_dist = is_device_pointer(dist_out);
+    const bool dev_parent = is_device_pointer(parent_out);
+    if (!dev_dist) HC_TRY(g->ws_out0.ensure(4 * n));
+    if (parent_out && !dev_parent) HC_TRY(g->ws_out1.ensure(4 * n));
+
+    double total_ms = 0;
+    for (int32_t i = 0; i < num_sources; i++) {
+        a.src = src[i];
+        a.dist = dev_dist ? dist_out + (size_t)i * n : g->ws_out0.as<int32_t>();
+        HC_CUDA_TRY(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), g->stream));
+        HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
+        HC_TRY(o.collect_stats ? launch_sssp<true>(g, a) : launch_sssp<false>(g, a));
+        HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
+        if (parent_out) {
+            int32_t *par = dev_parent ? parent_out + (size_t)i * n : g->ws_out1.as<int32_t>();
+            sssp_parent_init<<<g->sm_count * 4, 256, 0, g->stream>>>(par, g->N, a.src);
+            sssp_parents_fill<<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, a.w, a.dist, g->N, a.src, par);
+            HC_CUDA_TRY(cudaGetLastError());
+            if (!dev_parent) HC_TRY(copy_out(parent_out + (size_t)i * n, par, 4 * n, g->stream));
+        }
+        if (dist_out && !dev_dist) HC_TRY(copy_out(dist_out + (size_t)i * n, a.dist, 4 * n, g->stream));
+        SsspCtl c;
+        HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
+        if (stats) {
+            unsigned long long *cnt = (unsigned long long *)((char *)a.ctl + 2048);
+            HC_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, g->stream));
+            count_finite<<<g->sm_count * 4, 256, 0, g->stream>>>(a.dist, g->N, cnt);
+            unsigned long long reached = 0;
+            HC_CUDA_TRY(cudaMemcpyAsync(&reached, cnt, 8, cudaMemcpyDeviceToHost, g->stream));
+            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            stats->reached += (int32_t)reached;
+        }
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (c.gs.err) return fail((hc_status)c.gs.err, "hc_sssp: device run from source %d ended with status %d",
+                                  src[i], c.gs.err);
+        float ms = 0;
+        HC_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_start, g->ev_stop));
+        total_ms += ms;
+        if (stats) {
+            stats->epochs = std::max(stats->epochs, c.epochs);
+            stats->vertices_processed += (int64_t)c.vproc;
+            stats->edges_relaxed += (int64_t)c.erelax;
+        }
+    }
+    if (stats) {
+        stats->ms = total_ms;
+        // 16 B offsets per processed vertex, 8 B (neighbour + weight) per
+        // relaxed edge, 4 B distance write per reached vertex.
+        stats->bytes_model = 16.0 * (double)stats->vertices_processed + 8.0 * (double)stats->edges_relaxed +
+                             4.0 * (double)stats->reached;
+    }
+    return HC_OK;
+}

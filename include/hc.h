@@ -1,0 +1,297 @@
+/*
+ * hc.h -- C ABI of the B200-native epoch-kernel engine (BFS, SSSP, PageRank).
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, never
+ * exits the process and reports failure through an hc_status code plus a
+ * thread-local message (hc_last_error).  Array arguments may be host or device
+ * pointers unless stated otherwise: the library inspects each pointer and
+ * copies through HBM as needed.
+ *
+ * Reference interfaces replaced (paths inside chrisliu/hetero-compute):
+ *   graph container / loader ........ src/graph.cuh:43-100, :207-239
+ *   SourcePicker .................... src/graph.cuh:106-141
+ *   epoch-kernel typedefs ........... src/kernels/kernel_types.cuh:29-63
+ *   bfs_gpu driver .................. src/kernels/gpu/bfs.cuh:21-95
+ *   sssp_pull_gpu driver ............ src/kernels/gpu/sssp.cuh:42-100
+ *   pr_pull_gpu driver .............. src/kernels/gpu/pr.cuh:42-118
+ *   CUDA_ERRCHK / CONDCHK (abort) ... src/cuda.cuh:14-21, src/util.h:16-22
+ */
+#ifndef HC_H
+#define HC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Replaces the reference's print-and-exit error macros
+ * (src/cuda.cuh:14-21, src/util.h:16-22). */
+typedef enum hc_status {
+    HC_OK = 0,
+    HC_ERR_INVALID_ARG = 1,
+    HC_ERR_OOM = 2,
+    HC_ERR_CUDA = 3,
+    HC_ERR_NOT_CONVERGED = 4, /* iteration / epoch cap reached */
+    HC_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up */
+    HC_ERR_NO_DEVICE = 6,
+    HC_ERR_UNSUPPORTED = 7,
+    HC_ERR_IO = 8
+} hc_status;
+
+/* Edge-weight storage.  The reference keeps weights interleaved with the
+ * neighbour id as float (wnode_t, src/graph.cuh:37-41); here they are a
+ * separate array (SoA) of int32 (SSSP) or fp32 (weighted PageRank). */
+typedef enum hc_wtype { HC_W_NONE = 0, HC_W_I32 = 1, HC_W_F32 = 2 } hc_wtype;
+
+/* Epoch-kernel granularity.  Reference registries: BFSGPU
+ * (src/kernels/gpu/bfs.cuh:295-298), SSSPGPU (src/kernels/gpu/sssp.cuh:287-289),
+ * PRGPU (src/kernels/gpu/pr.cuh:324-326): one_to_one = THREAD,
+ * warp / warp_red = WARP, block_red = BLOCK.  AUTO lets the per-epoch
+ * selector choose. */
+typedef enum hc_variant {
+    HC_VARIANT_AUTO = 0,
+    HC_VARIANT_THREAD = 1,
+    HC_VARIANT_WARP = 2,
+    HC_VARIANT_BLOCK = 3
+} hc_variant;
+
+/* Host CSR graph: int64 offsets, int32 neighbours (GenericCSRGraph,
+ * src/graph.cuh:43-86).  Arrays owned by the library when produced by
+ * hc_gen_* / hc_csr_read and released with hc_csr_free. */
+typedef struct hc_csr {
+    int32_t num_nodes;
+    int64_t num_edges;  /* directed edges = length of neighbors */
+    int64_t *index;     /* num_nodes + 1 */
+    int32_t *neighbors; /* num_edges */
+    void *weights;      /* num_edges int32 or float, or NULL */
+    hc_wtype wtype;
+} hc_csr;
+
+const char *hc_last_error(void);
+const char *hc_status_string(hc_status s);
+int32_t hc_abi_version(void);
+
+/* ---------------------------------------------------------------- graphs */
+
+/* Kronecker / R-MAT (A=.57, B=.19, C=.19), 2^scale vertices,
+ * edge_factor * 2^scale generated pairs, random id permutation,
+ * symmetrized, self-loops and duplicates removed (the lightest weight of a
+ * duplicate set is kept), relabelled by descending degree, rows sorted.
+ * Semantics of the reference's gapbs adapters: src/gapbs/generator.h:82-115,
+ * src/gapbs/builder.h:141-186, :366-406.  Weights: HC_W_I32 uniform [1,255]
+ * (src/gapbs/generator.h:133-147), HC_W_F32 uniform (0,1]. */
+hc_status hc_gen_kronecker(int32_t scale, int32_t edge_factor, uint64_t seed,
+                           hc_wtype wtype, hc_csr *out);
+/* Erdos-Renyi: uniform endpoints (src/gapbs/generator.h:65-80), same build. */
+hc_status hc_gen_uniform(int32_t scale, int32_t degree, uint64_t seed,
+                         hc_wtype wtype, hc_csr *out);
+/* rows x cols 4-neighbour grid, id = r * cols + c, symmetric weights. */
+hc_status hc_gen_grid(int32_t rows, int32_t cols, uint64_t seed, hc_wtype wtype,
+                      hc_csr *out);
+void hc_csr_free(hc_csr *g);
+/* .sg / .wsg binary format (src/graph.cuh:207-224):
+ * [int32 N][int64 M][int64 index[N+1]][M x (int32 v) or M x (int32 v, float w)]. */
+hc_status hc_csr_read(const char *path, int32_t weighted, hc_csr *out);
+hc_status hc_csr_write(const char *path, const hc_csr *g);
+/* SourcePicker (src/graph.cuh:106-141): mt19937 seeded 37525, uniform over
+ * [0, N-1], rejecting degree-0 and self-loop-only vertices.  const_source >= 0
+ * repeats that vertex.  Host arrays only. */
+hc_status hc_pick_sources(const int64_t *index, const int32_t *neighbors,
+                          int32_t num_nodes, int32_t count, int32_t const_source,
+                          int32_t *out);
+
+/* ---------------------------------------------------------- device graph */
+
+typedef struct hc_graph hc_graph;
+
+typedef struct hc_graph_info {
+    int32_t num_nodes;
+    int64_t num_edges;
+    int32_t num_active;     /* vertices with degree > 0 (prefix when degree-sorted) */
+    int32_t degree_sorted;  /* 1 if degrees are non-increasing in vertex id */
+    int32_t max_degree;
+    int32_t device;
+    hc_wtype wtype;
+    int64_t device_bytes;   /* HBM held by the handle */
+} hc_graph_info;
+
+/* Upload a CSR graph once (the reference re-uploads per driver call,
+ * src/kernels/gpu/sssp.cuh:51-61).  Inputs may be host or device pointers. */
+hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors,
+                          const void *weights, hc_wtype wtype, int32_t num_nodes,
+                          int64_t num_edges, int32_t device, hc_graph **out);
+hc_status hc_graph_destroy(hc_graph *g);
+/* Work of this handle goes to `stream` (a cudaStream_t); NULL restores the
+ * handle's own stream. */
+hc_status hc_graph_set_stream(hc_graph *g, void *stream);
+hc_status hc_graph_get_info(const hc_graph *g, hc_graph_info *info);
+
+/* ------------------------------------------------------------------- BFS */
+
+typedef struct hc_bfs_opts {
+    int32_t alpha;        /* top-down -> bottom-up when m_f > m_u / alpha (0: 15) */
+    int32_t beta;         /* bottom-up -> top-down when n_f < N / beta (0: 18) */
+    int32_t direction;    /* 0 auto (direction-optimising), 1 top-down only, 2 bottom-up only */
+    hc_variant bu_variant;/* bottom-up granularity (AUTO / THREAD / WARP) */
+    int32_t collect_stats;/* count scanned vertices / edges (slower) */
+} hc_bfs_opts;
+
+typedef struct hc_bfs_stats {
+    int32_t levels;
+    int32_t td_levels;
+    int32_t bu_levels;
+    int32_t reached;
+    int64_t vertices_scanned;
+    int64_t edges_scanned;
+    double bytes_model;   /* algorithmic bytes, summed over sources */
+    double ms;            /* device time, summed over sources */
+} hc_bfs_stats;
+
+/* BFS from each source in turn (one persistent launch per source).
+ * depth_out / parent_out: [num_sources][num_nodes] int32, -1 = unreached;
+ * parent[src] = src.  Either may be NULL.  Replaces bfs_gpu
+ * (src/kernels/gpu/bfs.cuh:21-95), which is bottom-up only and returns
+ * parents alone. */
+hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sources,
+                 int32_t *depth_out, int32_t *parent_out,
+                 const hc_bfs_opts *opts, hc_bfs_stats *stats);
+
+/* ------------------------------------------------------------------ SSSP */
+
+typedef struct hc_sssp_opts {
+    int32_t delta;        /* near/far split width; 0 = auto, < 0 = plain frontier Bellman-Ford */
+    int32_t max_epochs;   /* 0 = unlimited */
+    int32_t collect_stats;
+} hc_sssp_opts;
+
+typedef struct hc_sssp_stats {
+    int32_t epochs;
+    int32_t reached;
+    int64_t vertices_processed;
+    int64_t edges_relaxed;
+    double bytes_model;
+    double ms;
+} hc_sssp_stats;
+
+/* Single-source shortest paths over int32 weights (graph wtype HC_W_I32).
+ * dist_out: [num_sources][num_nodes] int32, INT32_MAX = unreachable.
+ * parent_out (optional): a shortest-path tree, parent[src] = src.
+ * Replaces sssp_pull_gpu (src/kernels/gpu/sssp.cuh:42-100). */
+hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_sources,
+                  int32_t *dist_out, int32_t *parent_out,
+                  const hc_sssp_opts *opts, hc_sssp_stats *stats);
+
+/* -------------------------------------------------------------- PageRank */
+
+typedef struct hc_pr_opts {
+    float damping;        /* 0 -> 0.85 (src/kernels/gpu/pr.cuh:149) */
+    float tol_l1;         /* stop when sum |x_new - x_old| < tol_l1 (0 -> off) */
+    float eps_vertex;     /* stop when no |x_new - x_old| > eps_vertex (0 -> off) */
+    int32_t max_iters;    /* 0 -> 50 */
+    int32_t weighted;     /* 1: transition weight w_uv / sum_k w_uk; 0: 1/deg(u) */
+    hc_variant variant;
+} hc_pr_opts;
+
+typedef struct hc_pr_stats {
+    int32_t iterations;
+    int32_t converged;
+    float residual_l1;
+    int32_t changed;      /* vertices with |delta| > eps_vertex in the last iteration */
+    double bytes_model;
+    double ms;
+} hc_pr_stats;
+
+/* Pull PageRank, x = (1-d) t + d A x with A[v,u] = transition weight u->v,
+ * no dangling redistribution (src/kernels/gpu/pr.cuh:140-174).  teleport:
+ * [num_nodes][ncols] fp32 or NULL for uniform 1/N (ncols must be 1 then).
+ * scores_out: [num_nodes][ncols] fp32.  ncols > 1 runs personalised
+ * PageRank for all columns in one SpMM-form launch per iteration. */
+hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t ncols,
+                        float *scores_out, const hc_pr_opts *opts,
+                        hc_pr_stats *stats);
+
+/* Adjoint of hc_pr_forward for ncols == 1.  Given the converged scores x and
+ * dL/dx, solves lambda = dL/dx + d A^T lambda and returns
+ * dL/dteleport = (1-d) lambda and, if dL_dweights != NULL, the gradient
+ * with respect to the raw edge weights (CSR slot order; unit weights when the
+ * graph is unweighted), chained through the row normalisation.
+ * No counterpart in the reference. */
+hc_status hc_pr_backward(hc_graph *g, const float *scores, const float *dL_dscores,
+                         float *dL_dteleport, float *dL_dweights,
+                         const hc_pr_opts *opts, hc_pr_stats *stats);
+
+/* Personalised PageRank for ncols teleport vectors at once (SpMM form):
+ * column c teleports uniformly to seeds[seed_offsets[c] .. seed_offsets[c+1]).
+ * scores_out: [num_nodes][ncols] fp32, 1 <= ncols <= 256.  Iterates until
+ * every column's L1 change is below tol_l1 or max_iters.
+ * No counterpart in the reference (it runs one uniform PageRank per call). */
+hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, const int32_t *seeds,
+                         int32_t ncols, float *scores_out, const hc_pr_opts *opts,
+                         hc_pr_stats *stats);
+
+/* --------------------------------------------------------------- batched */
+
+typedef struct hc_batch_opts {
+    int32_t group;        /* sources per group (0 = autotuned) */
+    int32_t max_epochs;   /* 0 = unlimited */
+    int32_t use_graph;    /* capture the epoch loop in a CUDA graph */
+} hc_batch_opts;
+
+typedef struct hc_batch_stats {
+    int32_t epochs;
+    int32_t groups;
+    double bytes_model;
+    double ms;
+} hc_batch_stats;
+
+/* Multi-source BFS: bit-sliced frontiers, all sources of a group advance in
+ * one launch per level.  depth_out: [num_sources][num_nodes] int32.
+ * The reference runs sources one after another (src/benchmarks/gpu_benchmark.cuh:577-586). */
+hc_status hc_bfs_batched(hc_graph *g, const int32_t *sources, int32_t num_sources,
+                         int32_t *depth_out, const hc_batch_opts *opts,
+                         hc_batch_stats *stats);
+
+/* Multi-source SSSP, one lane per source over vertex-major distances.
+ * dist_out: [num_sources][num_nodes] int32. */
+hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_t num_sources,
+                          int32_t *dist_out, const hc_batch_opts *opts,
+                          hc_batch_stats *stats);
+
+/* ------------------------------------------------ reference epoch kernels */
+/* One epoch of the reference's in-place pull kernels over [start_id, end_id),
+ * device pointers only, launched on `stream` with the given shape and
+ * granularity, adding to *updated (device int32).  These keep the epoch-kernel
+ * contract of src/kernels/kernel_types.cuh:36-63 for callers that drive their
+ * own epoch loop. */
+
+/* sssp_gpu_epoch_func (src/kernels/kernel_types.cuh:36-37): wnodes is the
+ * reference's interleaved {int32 v; float w} edge array. */
+hc_status hc_epoch_sssp_pull(const int64_t *index, const void *wnodes,
+                             int32_t start_id, int32_t end_id, float *dist,
+                             int32_t *updated, hc_variant variant,
+                             int32_t block_count, int32_t thread_count,
+                             void *stream);
+
+/* pr_gpu_epoch_func (src/kernels/kernel_types.cuh:46-47). */
+hc_status hc_epoch_pr_pull(const int64_t *index, const void *wnodes,
+                           int32_t start_id, int32_t end_id, float *score,
+                           int32_t *updated, int32_t num_nodes,
+                           const int64_t *degrees, hc_variant variant,
+                           int32_t block_count, int32_t thread_count,
+                           void *stream);
+
+/* bfs_gpu_epoch_func (src/kernels/kernel_types.cuh:60-63): the Bitmap
+ * structs become their 32-bit word buffers. */
+hc_status hc_epoch_bfs_pull(const int64_t *index, const int32_t *neighbors,
+                            int32_t *parents, int32_t start_id, int32_t end_id,
+                            const uint32_t *frontier, uint32_t *next_frontier,
+                            int32_t *num_nodes, hc_variant variant,
+                            int32_t block_count, int32_t thread_count,
+                            void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HC_H */

@@ -1,0 +1,226 @@
+"""GPU parity of the plain hot path (BFS, SSSP, PageRank) through the C ABI
+against the oracle and the reference's golden outputs."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import hc
+import oracle
+from conftest import make_graph
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["kron10", "kron12_ef8", "er10", "grid32", "kron16"]
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.fixture(scope="module")
+def graphs(golden):
+    out = {}
+    for name in CASES:
+        rec, arr = golden[name]
+        host = make_graph(rec)
+        out[name] = (rec, arr, host, hc.Graph.from_host(host))
+    return out
+
+
+# ------------------------------------------------------------------- BFS
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("direction,bu", [(0, hc.VARIANT_AUTO), (1, hc.VARIANT_AUTO), (2, hc.VARIANT_THREAD),
+                                          (2, hc.VARIANT_WARP), (0, hc.VARIANT_WARP)])
+def test_bfs_depths_bit_exact(graphs, name, direction, bu):
+    rec, arr, host, g = graphs[name]
+    src = rec["bfs_sources"]
+    depth, parent, st = g.bfs(src, direction=direction, bu_variant=bu)
+    for i, s in enumerate(src):
+        assert digest(depth[i]) == rec["bfs_depth_sha256"][i], (name, i)
+        bad, counts = oracle.verify_bfs_parents(host.index, host.neighbors, depth[i], parent[i], s)
+        assert bad == 0, counts
+
+
+def test_bfs_larger_graph_against_oracle():
+    host = hc.gen_kronecker(19, 16, 9)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, 6)
+    depth, parent, st = g.bfs(src, stats=True)
+    assert st.td_levels > 0 and st.bu_levels > 0
+    for i, s in enumerate(src):
+        d = oracle.bfs_depth(host.index, host.neighbors, s)
+        assert np.array_equal(depth[i], d)
+        assert oracle.verify_bfs_parents(host.index, host.neighbors, d, parent[i], s)[0] == 0
+
+
+def _handmade(edges, n):
+    """CSR from an edge list, kept as given (duplicates, self-loops, unsorted rows allowed)."""
+    edges = np.array(edges, dtype=np.int64).reshape(-1, 2)
+    order = np.argsort(edges[:, 0], kind="stable")
+    e = edges[order]
+    idx = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(idx, e[:, 0] + 1, 1)
+    return np.cumsum(idx), e[:, 1].astype(np.int32)
+
+
+def test_bfs_edge_cases():
+    # path 0-1-...-299 (high diameter), a star around 300, isolated 400, self-loops, duplicates
+    n = 401
+    edges = []
+    for i in range(299):
+        edges += [(i, i + 1), (i + 1, i)]
+    for j in range(301, 340):
+        edges += [(300, j), (j, 300), (300, j)]
+    edges += [(5, 5), (300, 300)]
+    idx, nbr = _handmade(edges, n)
+    g = hc.Graph(idx, nbr)
+    for s in [0, 150, 300, 320, 400, 5]:
+        for direction in (0, 1, 2):
+            depth, parent, _ = g.bfs([s], direction=direction)
+            d = oracle.bfs_depth(idx, nbr, s)
+            assert np.array_equal(depth[0], d), (s, direction)
+            assert oracle.verify_bfs_parents(idx, nbr, d, parent[0], s)[0] == 0
+    # empty graph (no edges) and a single vertex
+    g1 = hc.Graph(np.zeros(2, dtype=np.int64), np.zeros(0, dtype=np.int32))
+    depth, parent, _ = g1.bfs([0])
+    assert depth[0, 0] == 0 and parent[0, 0] == 0
+
+
+def test_bfs_unsorted_degrees():
+    host = hc.gen_kronecker(12, 8, 4)
+    n = host.num_nodes
+    perm = np.random.default_rng(1).permutation(n).astype(np.int32)  # old -> new
+    inv = np.argsort(perm)
+    deg = host.degrees()[inv]
+    idx = np.concatenate([[0], np.cumsum(deg)]).astype(np.int64)
+    nbr = np.concatenate([np.sort(perm[host.neighbors[host.index[o]:host.index[o + 1]]]) for o in inv]).astype(np.int32)
+    g = hc.Graph(idx, nbr)
+    assert g.info().degree_sorted == 0
+    for s in hc.pick_sources(hc.HostCSR(idx, nbr), 3):
+        depth, parent, _ = g.bfs([s])
+        assert np.array_equal(depth[0], oracle.bfs_depth(idx, nbr, s))
+
+
+def test_bfs_device_outputs():
+    torch = pytest.importorskip("torch")
+    host = hc.gen_kronecker(12, 16, 2)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, 3)
+    depth = torch.empty((3, host.num_nodes), dtype=torch.int32, device="cuda")
+    parent = torch.empty((3, host.num_nodes), dtype=torch.int32, device="cuda")
+    g.bfs(torch.from_numpy(src).cuda(), depth, parent)
+    torch.cuda.synchronize()
+    for i, s in enumerate(src):
+        assert np.array_equal(depth[i].cpu().numpy(), oracle.bfs_depth(host.index, host.neighbors, s))
+
+
+def test_bfs_rejects_bad_sources(graphs):
+    g = graphs["kron10"][3]
+    with pytest.raises(hc.HCError) as e:
+        g.bfs([5000])
+    assert e.value.status == hc.INVALID_ARG
+
+
+# ------------------------------------------------------------------ SSSP
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("delta", [0, -1, 1, 64, 100000])
+def test_sssp_distances_bit_exact(graphs, name, delta):
+    rec, arr, host, g = graphs[name]
+    src = rec["sssp_sources"]
+    dist, parent, _ = g.sssp(src, delta=delta, want_parent=True)
+    for i, s in enumerate(src):
+        assert digest(dist[i]) == rec["sssp_dist_sha256"][i], (name, i, delta)
+        assert oracle.verify_sp_tree(host.index, host.neighbors, host.weights, dist[i], parent[i], s) == 0
+
+
+def test_sssp_grid_against_dijkstra():
+    host = hc.gen_grid(200, 300, 3, wtype=hc.W_I32)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, 3)
+    dist, _, st = g.sssp(src, stats=True)
+    assert st.epochs > 200
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s))
+
+
+def test_sssp_larger_graph_against_dijkstra():
+    host = hc.gen_kronecker(18, 16, 5, wtype=hc.W_I32)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, 4)
+    for delta in (0, -1):
+        dist, _, _ = g.sssp(src, delta=delta)
+        for i, s in enumerate(src):
+            assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s))
+
+
+def test_sssp_errors():
+    host = hc.gen_kronecker(8, 4, 1)
+    g = hc.Graph.from_host(host)  # unweighted
+    with pytest.raises(hc.HCError) as e:
+        g.sssp([0])
+    assert e.value.status == hc.UNSUPPORTED
+    w = np.ones(host.num_edges, dtype=np.int32)
+    w[3] = -2
+    g2 = hc.Graph(host.index, host.neighbors, w)
+    with pytest.raises(hc.HCError) as e:
+        g2.sssp([int(hc.pick_sources(host, 1)[0])])
+    assert e.value.status == hc.INVALID_ARG
+    # epoch cap reached -> NOT_CONVERGED, and the handle stays usable
+    hg = hc.gen_grid(50, 50, 1, wtype=hc.W_I32)
+    g3 = hc.Graph.from_host(hg)
+    with pytest.raises(hc.HCError) as e:
+        g3.sssp([0], max_epochs=5)
+    assert e.value.status == hc.NOT_CONVERGED
+    dist, _, _ = g3.sssp([0])
+    assert np.array_equal(dist[0], oracle.sssp_dijkstra(hg.index, hg.neighbors, hg.weights, 0))
+
+
+# -------------------------------------------------------------- PageRank
+
+@pytest.mark.parametrize("name", CASES)
+def test_pagerank_matches_reference(graphs, name):
+    rec, arr, host, g = graphs[name]
+    ref = arr["pr_scores"]
+    s = hc.pr_pull_gpu(g)  # the reference stopping rule: no vertex moves by > 5e-8
+    err_ref = np.abs(s - ref).max()
+    assert err_ref <= 1e-5, err_ref
+    x, _ = oracle.pr_jacobi_f64(host.index, host.neighbors)
+    err64 = np.abs(s - x).max()
+    assert err64 <= 1e-5, err64
+
+
+def test_pagerank_l1_tolerance_mode():
+    host = hc.gen_kronecker(16, 16, 2)
+    g = hc.Graph.from_host(host)
+    s, st = g.pagerank(tol_l1=1e-4, max_iters=50)
+    assert st.converged and st.iterations <= 50 and st.residual_l1 < 1e-4
+    x, _ = oracle.pr_jacobi_f64(host.index, host.neighbors)
+    assert np.abs(s - x).max() < 1e-5
+    assert abs(s.sum() - x.sum()) < 1e-3
+
+
+def test_pagerank_weighted_and_teleport():
+    host = hc.gen_kronecker(11, 8, 3, wtype=hc.W_F32)
+    g = hc.Graph.from_host(host)
+    rng = np.random.default_rng(3)
+    t = rng.random(host.num_nodes).astype(np.float32)
+    t /= t.sum()
+    s, st = g.pagerank(t, weighted=True, tol_l1=1e-9, max_iters=300)
+    x = oracle.pr_dense(host.index, host.neighbors, host.weights.astype(np.float64), t.astype(np.float64))
+    assert np.abs(s - x).max() < 1e-6
+    s2, _ = g.pagerank(t, weighted=False, tol_l1=1e-9, max_iters=300)
+    x2 = oracle.pr_dense(host.index, host.neighbors, None, t.astype(np.float64))
+    assert np.abs(s2 - x2).max() < 1e-6
+
+
+def test_pagerank_hub_rows_chunked():
+    # scale 18 has rows above the hub threshold (16384 edges): exercises the chunked path
+    host = hc.gen_kronecker(18, 16, 1)
+    assert host.degrees().max() > 16384
+    g = hc.Graph.from_host(host)
+    s, st = g.pagerank(tol_l1=1e-7, max_iters=200)
+    x, _ = oracle.pr_jacobi_f64(host.index, host.neighbors, tol=1e-12)
+    assert np.abs(s - x).max() < 1e-6
