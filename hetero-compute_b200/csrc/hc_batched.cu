@@ -266,10 +266,10 @@ hc_status run_msbfs(hc_graph *g, const int32_t *d_src, int nsrc, int32_t *depth,
     uint32_t *act[2] = {(uint32_t *)take((size_t)W * 4), (uint32_t *)take((size_t)W * 4)};
     unsigned long long *found = (unsigned long long *)take(64);
     const int grid = g->sm_count * 8;
-    msbfs_init<K64><<<grid, 256, 0, g->stream>>>(g->N, nsrc, d_src, seen[0], fr[0], act[0], W);
+    { msbfs_init<K64><<<grid, 256, 0, g->stream>>>(g->N, nsrc, d_src, seen[0], fr[0], act[0], W); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaMemsetAsync(act[1], 0, (size_t)W * 4, g->stream));
     if (depth) HC_CUDA_TRY(cudaMemsetAsync(depth, 0xff, sizeof(int32_t) * (size_t)nsrc * n, g->stream));
-    msbfs_seed<K64><<<(nsrc + 255) / 256, 256, 0, g->stream>>>(nsrc, d_src, seen[0], fr[0], act[0], depth, n);
+    { msbfs_seed<K64><<<(nsrc + 255) / 256, 256, 0, g->stream>>>(nsrc, d_src, seen[0], fr[0], act[0], depth, n); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     const int max_levels = o.max_epochs > 0 ? o.max_epochs : g->N + 1;
     int level = 0;
@@ -278,9 +278,9 @@ hc_status run_msbfs(hc_graph *g, const int32_t *d_src, int nsrc, int32_t *depth,
         const int c = level & 1;
         HC_CUDA_TRY(cudaMemsetAsync(found, 0, 8, g->stream));
         HC_CUDA_TRY(cudaMemsetAsync(act[c ^ 1], 0, (size_t)W * 4, g->stream));
-        msbfs_level<K64><<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->n_active, nsrc,
+        { msbfs_level<K64><<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->n_active, nsrc,
                                                       seen[c], seen[c ^ 1], fr[c], fr[c ^ 1], act[c], act[c ^ 1],
-                                                      depth, n, level, found);
+                                                      depth, n, level, found); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         unsigned long long h = 0;
         HC_CUDA_TRY(cudaMemcpyAsync(&h, found, 8, cudaMemcpyDeviceToHost, g->stream));
@@ -398,8 +398,8 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
     for (int s0 = 0; s0 < num_sources; s0 += 32, groups++) {
         const int k = std::min(32, num_sources - s0);
         HC_CUDA_TRY(cudaMemcpyAsync(d_src, src.data() + s0, sizeof(int32_t) * k, cudaMemcpyHostToDevice, g->stream));
-        mssp_init<<<grid, 256, 0, g->stream>>>(g->N, dist, act[0], act[1]);
-        mssp_seed<<<1, 32, 0, g->stream>>>(k, d_src, dist, act[0], q[0], &ctr[0]);
+        { mssp_init<<<grid, 256, 0, g->stream>>>(g->N, dist, act[0], act[1]); ::hc::count_launch(); }
+        { mssp_seed<<<1, 32, 0, g->stream>>>(k, d_src, dist, act[0], q[0], &ctr[0]); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         int nq = 0;
         HC_CUDA_TRY(cudaMemcpyAsync(&nq, &ctr[0], 4, cudaMemcpyDeviceToHost, g->stream));
@@ -410,13 +410,13 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
             const int c = ep & 1;
             HC_CUDA_TRY(cudaMemsetAsync(&ctr[c ^ 1], 0, 4, g->stream));
             HC_CUDA_TRY(cudaMemsetAsync(&ctr[2], 0, 4, g->stream));
-            mssp_epoch<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->wgt.as<int32_t>(),
+            { mssp_epoch<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->wgt.as<int32_t>(),
                                                     dist, q[c], nq, act[c], act[c ^ 1], q[c ^ 1], &ctr[c ^ 1], tasks,
-                                                    &ctr[2], relaxed);
-            mssp_tasks<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->wgt.as<int32_t>(),
+                                                    &ctr[2], relaxed); ::hc::count_launch(); }
+            { mssp_tasks<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->wgt.as<int32_t>(),
                                                     dist, tasks, &ctr[2], act[c], act[c ^ 1], q[c ^ 1], &ctr[c ^ 1],
-                                                    relaxed);
-            mssp_clear<<<(nq + 255) / 256, 256, 0, g->stream>>>(q[c], nq, act[c]);
+                                                    relaxed); ::hc::count_launch(); }
+            { mssp_clear<<<(nq + 255) / 256, 256, 0, g->stream>>>(q[c], nq, act[c]); ::hc::count_launch(); }
             HC_CUDA_TRY(cudaGetLastError());
             HC_CUDA_TRY(cudaMemcpyAsync(&nq, &ctr[c ^ 1], 4, cudaMemcpyDeviceToHost, g->stream));
             HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
@@ -424,7 +424,7 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
         epochs_max = std::max(epochs_max, ep);
         if (dist_out) {
             int32_t *dst = dev_out ? dist_out + (size_t)s0 * n : g->ws_out0.as<int32_t>();
-            mssp_transpose<<<grid, 256, 0, g->stream>>>(dist, g->N, k, dst);
+            { mssp_transpose<<<grid, 256, 0, g->stream>>>(dist, g->N, k, dst); ::hc::count_launch(); }
             HC_CUDA_TRY(cudaGetLastError());
             if (!dev_out) HC_TRY(copy_out(dist_out + (size_t)s0 * n, dst, sizeof(int32_t) * (size_t)k * n, g->stream));
         }

@@ -306,6 +306,7 @@ hc_status launch_bfs(hc_graph *g, const BfsArgs &args) {
     dim3 grid(g->sm_count * bps), block(kBfsThreads);
     BfsArgs a = args;
     void *params[] = {&a};
+    ::hc::count_launch();
     HC_CUDA_TRY(cudaLaunchCooperativeKernel((void *)bfs_persistent<kStats>, grid, block, params, 0, g->stream));
     return HC_OK;
 }
@@ -386,7 +387,7 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
         if (stats) {
             unsigned long long *cnt = (unsigned long long *)((char *)a.ctl + 2048);
             HC_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, g->stream));
-            count_reached<<<g->sm_count * 4, 256, 0, g->stream>>>(a.depth, g->N, cnt);
+            { count_reached<<<g->sm_count * 4, 256, 0, g->stream>>>(a.depth, g->N, cnt); ::hc::count_launch(); }
             unsigned long long reached = 0;
             HC_CUDA_TRY(cudaMemcpyAsync(&reached, cnt, 8, cudaMemcpyDeviceToHost, g->stream));
             HC_CUDA_TRY(cudaStreamSynchronize(g->stream));

@@ -13,6 +13,8 @@ namespace hc {
 // Records a printf-style message as this thread's last error and returns `s`.
 hc_status fail(hc_status s, const char *fmt, ...);
 void clear_error();
+// Counts kernel launches made by the library (hc_kernel_launches).
+void count_launch(int n = 1);
 
 // Counter-based 64-bit mixer (SplitMix64 finaliser, Steele/Lea/Flood 2014).
 // Graph generation draws every random number from (seed, stream, counter), so

@@ -251,13 +251,13 @@ hc_status hc_epoch_sssp_pull(const int64_t *index, const void *wnodes, int32_t s
     const WNode *nb = (const WNode *)wnodes;
     switch (variant) {
         case HC_VARIANT_THREAD:
-            sssp_epoch_thread<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, dist, updated);
+            { sssp_epoch_thread<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, dist, updated); ::hc::count_launch(); }
             break;
         case HC_VARIANT_BLOCK:
-            sssp_epoch_block<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, dist, updated);
+            { sssp_epoch_block<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, dist, updated); ::hc::count_launch(); }
             break;
         default:
-            sssp_epoch_warp<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, dist, updated);
+            { sssp_epoch_warp<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, dist, updated); ::hc::count_launch(); }
             break;
     }
     HC_CUDA_TRY(cudaGetLastError());
@@ -276,16 +276,16 @@ hc_status hc_epoch_pr_pull(const int64_t *index, const void *wnodes, int32_t sta
     const WNode *nb = (const WNode *)wnodes;
     switch (variant) {
         case HC_VARIANT_THREAD:
-            pr_epoch_thread<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, score, updated, num_nodes,
-                                                                 degrees);
+            { pr_epoch_thread<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, score, updated, num_nodes,
+                                                                 degrees); ::hc::count_launch(); }
             break;
         case HC_VARIANT_BLOCK:
-            pr_epoch_block<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, score, updated, num_nodes,
-                                                                degrees);
+            { pr_epoch_block<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, score, updated, num_nodes,
+                                                                degrees); ::hc::count_launch(); }
             break;
         default:
-            pr_epoch_warp<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, score, updated, num_nodes,
-                                                               degrees);
+            { pr_epoch_warp<<<block_count, thread_count, 0, s>>>(index, nb, start_id, end_id, score, updated, num_nodes,
+                                                               degrees); ::hc::count_launch(); }
             break;
     }
     HC_CUDA_TRY(cudaGetLastError());
@@ -302,11 +302,11 @@ hc_status hc_epoch_bfs_pull(const int64_t *index, const int32_t *neighbors, int3
     if (start_id == end_id) return HC_OK;
     cudaStream_t s = (cudaStream_t)stream;
     if (variant == HC_VARIANT_THREAD)
-        bfs_epoch_thread<<<block_count, thread_count, 0, s>>>(index, neighbors, parents, start_id, end_id, frontier,
-                                                              next_frontier, num_nodes);
+        { bfs_epoch_thread<<<block_count, thread_count, 0, s>>>(index, neighbors, parents, start_id, end_id, frontier,
+                                                              next_frontier, num_nodes); ::hc::count_launch(); }
     else
-        bfs_epoch_warp<<<block_count, thread_count, 0, s>>>(index, neighbors, parents, start_id, end_id, frontier,
-                                                            next_frontier, num_nodes);
+        { bfs_epoch_warp<<<block_count, thread_count, 0, s>>>(index, neighbors, parents, start_id, end_id, frontier,
+                                                            next_frontier, num_nodes); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     return HC_OK;
 }

@@ -178,7 +178,7 @@ hc_status ensure_pr_derived(hc_graph *g, bool weighted) {
     const int grid = g->sm_count * 8, block = 256;
     if (!g->inv_deg.ptr) {
         HC_TRY(g->inv_deg.ensure(sizeof(float) * std::max<int32_t>(g->N, 1)));
-        build_inv_deg<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->N, g->inv_deg.as<float>());
+        { build_inv_deg<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->N, g->inv_deg.as<float>()); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
     }
     if (weighted && !g->wtn.ptr) {
@@ -186,15 +186,15 @@ hc_status ensure_pr_derived(hc_graph *g, bool weighted) {
             return fail(HC_ERR_UNSUPPORTED, "weighted PageRank needs fp32 edge weights");
         HC_TRY(g->inv_wsum.ensure(sizeof(float) * std::max<int32_t>(g->N, 1)));
         HC_TRY(g->wtn.ensure(sizeof(float) * (size_t)(g->M + kNbrPad)));
-        build_inv_wsum<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->wgt.as<float>(), g->N,
-                                                        g->inv_wsum.as<float>());
+        { build_inv_wsum<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->wgt.as<float>(), g->N,
+                                                        g->inv_wsum.as<float>()); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         DevBuf flag;
         HC_TRY(flag.ensure(sizeof(int)));
         HC_CUDA_TRY(cudaMemsetAsync(flag.ptr, 0, sizeof(int), g->stream));
-        build_wtn<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
+        { build_wtn<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
                                                    g->wgt.as<float>(), g->inv_wsum.as<float>(), g->N,
-                                                   g->wtn.as<float>(), flag.as<int>());
+                                                   g->wtn.as<float>(), flag.as<int>()); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         int missing = 0;
         HC_CUDA_TRY(cudaMemcpyAsync(&missing, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
@@ -292,7 +292,7 @@ hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const 
         cudaMemcpyAsync(&ends[1], g->index.as<int64_t>() + num_nodes, 8, cudaMemcpyDeviceToHost, g->stream) != cudaSuccess)
         return bail(fail(HC_ERR_CUDA, "analysis setup failed"));
     const int grid = g->sm_count * 8;
-    analyze_index<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), num_nodes, num_edges, abuf.as<Analysis>());
+    { analyze_index<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), num_nodes, num_edges, abuf.as<Analysis>()); ::hc::count_launch(); }
     Analysis res;
     if (cudaMemcpyAsync(&res, abuf.ptr, sizeof(res), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
         cudaStreamSynchronize(g->stream) != cudaSuccess)
@@ -300,8 +300,8 @@ hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const 
     if (ends[0] != 0 || ends[1] != num_edges || res.bad_index)
         return bail(fail(HC_ERR_INVALID_ARG,
                          "hc_graph_create: index must be non-decreasing from 0 to num_edges"));
-    analyze_rows<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), num_nodes,
-                                                abuf.as<Analysis>());
+    { analyze_rows<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), num_nodes,
+                                                abuf.as<Analysis>()); ::hc::count_launch(); }
     if (cudaMemcpyAsync(&res, abuf.ptr, sizeof(res), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
         cudaStreamSynchronize(g->stream) != cudaSuccess)
         return bail(fail(HC_ERR_CUDA, "graph analysis failed: %s", cudaGetErrorString(cudaGetLastError())));
@@ -355,6 +355,53 @@ hc_status hc_graph_get_info(const hc_graph *g, hc_graph_info *info) {
     info->device = g->device;
     info->wtype = g->wtype;
     info->device_bytes = g->bytes_held();
+    return HC_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+hc_status hc_dev_malloc(void **ptr, size_t bytes, int32_t device) {
+    clear_error();
+    if (!ptr) return fail(HC_ERR_INVALID_ARG, "hc_dev_malloc: null output");
+    *ptr = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(HC_ERR_NO_DEVICE, "hc_dev_malloc: no CUDA device visible");
+    }
+    if (device < 0 || device >= ndev) return fail(HC_ERR_INVALID_ARG, "hc_dev_malloc: bad device %d", device);
+    HC_CUDA_TRY(cudaSetDevice(device));
+    HC_CUDA_TRY(cudaMalloc(ptr, bytes ? bytes : 1));
+    return HC_OK;
+}
+
+hc_status hc_dev_free(void *ptr) {
+    clear_error();
+    if (ptr) HC_CUDA_TRY(cudaFree(ptr));
+    return HC_OK;
+}
+
+hc_status hc_memcpy(void *dst, const void *src, size_t bytes) {
+    clear_error();
+    if (!bytes) return HC_OK;
+    if (!dst || !src) return fail(HC_ERR_INVALID_ARG, "hc_memcpy: null pointer");
+    HC_CUDA_TRY(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
+    return HC_OK;
+}
+
+hc_status hc_dev_memset(void *ptr, int32_t value, size_t bytes) {
+    clear_error();
+    if (!bytes) return HC_OK;
+    if (!ptr) return fail(HC_ERR_INVALID_ARG, "hc_dev_memset: null pointer");
+    HC_CUDA_TRY(cudaMemset(ptr, value, bytes));
+    return HC_OK;
+}
+
+hc_status hc_device_synchronize(void) {
+    clear_error();
+    HC_CUDA_TRY(cudaDeviceSynchronize());
     return HC_OK;
 }
 

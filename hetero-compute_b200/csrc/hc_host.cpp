@@ -26,6 +26,9 @@
 namespace hc {
 
 static thread_local std::string g_last_error;
+static std::atomic<int64_t> g_launches{0};
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 hc_status fail(hc_status s, const char *fmt, ...) {
     char buf[1024];
@@ -307,6 +310,8 @@ const char *hc_status_string(hc_status s) {
 }
 
 int32_t hc_abi_version(void) { return 1; }
+
+int64_t hc_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 void hc_csr_free(hc_csr *g) {
     if (!g) return;

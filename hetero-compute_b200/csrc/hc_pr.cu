@@ -547,7 +547,7 @@ hc_status launch_sweep(hc_graph *g, const SweepArgs &a, const PrPlanDev &plan) {
         HC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pr_sweep<kEW, kRS, kPS, kBaseVec>, kPrThreads, 0));
         bps = std::max(bps, 1);
     }
-    pr_sweep<kEW, kRS, kPS, kBaseVec><<<g->sm_count * bps, kPrThreads, 0, g->stream>>>(a, plan);
+    { pr_sweep<kEW, kRS, kPS, kBaseVec><<<g->sm_count * bps, kPrThreads, 0, g->stream>>>(a, plan); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     return HC_OK;
 }
@@ -680,11 +680,11 @@ extern "C" hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t n
         unsigned *hub_count = (unsigned *)take((size_t)(plan.n_hub + 1) * 4);
         double *col_l1 = (double *)take((size_t)K * 8);
         HC_TRY(copy_in(basev, teleport, nk * 4, g->stream));
-        scale_vec<<<g->sm_count * 8, 256, 0, g->stream>>>(basev, 1.0f - o.damping, basev, nk);
+        { scale_vec<<<g->sm_count * 8, 256, 0, g->stream>>>(basev, 1.0f - o.damping, basev, nk); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaMemsetAsync(hub_count, 0, (size_t)(plan.n_hub + 1) * 4, g->stream));
         const float *ps = weighted ? nullptr : g->inv_deg.as<float>();
-        spmm_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, K, basev, nullptr, nullptr, o.damping, ps, x[0],
-                                                          gv[0], x[1], gv[1], g->n_active);
+        { spmm_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, K, basev, nullptr, nullptr, o.damping, ps, x[0],
+                                                          gv[0], x[1], gv[1], g->n_active); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         SpmmArgs a{};
         a.index = g->index.as<int64_t>();
@@ -710,10 +710,10 @@ extern "C" hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t n
             HC_CUDA_TRY(cudaMemsetAsync(col_l1, 0, (size_t)K * 8, g->stream));
             const int cols = (K + 31) / 32;
             const int grid = g->sm_count * 8;
-            if (cols <= 1) spmm_sweep<1><<<grid, kPrThreads, 0, g->stream>>>(a, plan, nullptr);
-            else if (cols <= 2) spmm_sweep<2><<<grid, kPrThreads, 0, g->stream>>>(a, plan, nullptr);
-            else if (cols <= 4) spmm_sweep<4><<<grid, kPrThreads, 0, g->stream>>>(a, plan, nullptr);
-            else if (cols <= 8) spmm_sweep<8><<<grid, kPrThreads, 0, g->stream>>>(a, plan, nullptr);
+            if (cols <= 1) { spmm_sweep<1><<<grid, kPrThreads, 0, g->stream>>>(a, plan, nullptr); ::hc::count_launch(); }
+            else if (cols <= 2) { spmm_sweep<2><<<grid, kPrThreads, 0, g->stream>>>(a, plan, nullptr); ::hc::count_launch(); }
+            else if (cols <= 4) { spmm_sweep<4><<<grid, kPrThreads, 0, g->stream>>>(a, plan, nullptr); ::hc::count_launch(); }
+            else if (cols <= 8) { spmm_sweep<8><<<grid, kPrThreads, 0, g->stream>>>(a, plan, nullptr); ::hc::count_launch(); }
             else return fail(HC_ERR_UNSUPPORTED, "hc_pr_forward: at most 256 columns per call");
             HC_CUDA_TRY(cudaGetLastError());
             HC_CUDA_TRY(cudaMemcpyAsync(hl1.data(), col_l1, (size_t)K * 8, cudaMemcpyDeviceToHost, g->stream));
@@ -757,16 +757,16 @@ extern "C" hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t n
     const bool basevec = teleport != nullptr;
     if (basevec) {
         HC_TRY(copy_in(basev, teleport, n * 4, g->stream));
-        scale_vec<<<g->sm_count * 8, 256, 0, g->stream>>>(basev, 1.0f - o.damping, basev, (size_t)g->N);
+        { scale_vec<<<g->sm_count * 8, 256, 0, g->stream>>>(basev, 1.0f - o.damping, basev, (size_t)g->N); ::hc::count_launch(); }
     }
     // Uniform teleport: base (1-d)/N as the reference computes it
     // (src/kernels/gpu/pr.cuh:152), start from 1/N (src/kernels/cpu/pr.cuh:39).
     const float base_scalar = (1.0f - o.damping) / (float)g->N;
     const float *ps = weighted ? nullptr : g->inv_deg.as<float>();
-    pr_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, basevec ? basev : nullptr, base_scalar,
+    { pr_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, basevec ? basev : nullptr, base_scalar,
                                                     basevec ? 0.f : 1.0f / (float)g->N, basevec ? basev : nullptr,
                                                     ps, x[0], weighted ? nullptr : gv[0], x[1],
-                                                    weighted ? nullptr : gv[1], g->n_active);
+                                                    weighted ? nullptr : gv[1], g->n_active); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     SweepArgs a{};
     a.index = g->index.as<int64_t>();
@@ -836,8 +836,8 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
     HC_TRY(copy_in(cvec, dL_dscores, n * 4, g->stream));
     HC_TRY(copy_in(xs, scores, n * 4, g->stream));
     // lambda_0 = c; isolated vertices keep lambda = c.
-    pr_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, cvec, 0.f, 0.f, cvec, nullptr, lam[0], nullptr, lam[1],
-                                                    nullptr, g->n_active);
+    { pr_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, cvec, 0.f, 0.f, cvec, nullptr, lam[0], nullptr, lam[1],
+                                                    nullptr, g->n_active); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     SweepArgs a{};
     a.index = g->index.as<int64_t>();
@@ -863,7 +863,7 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
     if (dL_dteleport) {
         const bool dev = is_device_pointer(dL_dteleport);
         float *dst = dev ? dL_dteleport : spare;
-        scale_vec<<<g->sm_count * 8, 256, 0, g->stream>>>(lfin, 1.0f - o.damping, dst, (size_t)g->N);
+        { scale_vec<<<g->sm_count * 8, 256, 0, g->stream>>>(lfin, 1.0f - o.damping, dst, (size_t)g->N); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         if (!dev) HC_TRY(copy_out(dL_dteleport, spare, n * 4, g->stream));
     }
@@ -876,11 +876,11 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
         }
         const float *rsv = weighted ? g->inv_wsum.as<float>() : g->inv_deg.as<float>();
         if (weighted)
-            pr_edge_grad<true><<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, g->wgt.as<float>(), rsv, xs,
-                                                                       lfin, o.damping, g->N, dst);
+            { pr_edge_grad<true><<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, g->wgt.as<float>(), rsv, xs,
+                                                                       lfin, o.damping, g->N, dst); ::hc::count_launch(); }
         else
-            pr_edge_grad<false><<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, nullptr, rsv, xs, lfin,
-                                                                        o.damping, g->N, dst);
+            { pr_edge_grad<false><<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, nullptr, rsv, xs, lfin,
+                                                                        o.damping, g->N, dst); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         if (!dev) HC_TRY(copy_out(dL_dweights, dst, sizeof(float) * (size_t)g->M, g->stream));
     }
@@ -948,10 +948,10 @@ extern "C" hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, co
     HC_CUDA_TRY(cudaMemcpyAsync(d_seeds, sd.data(), (size_t)nseeds * 4, cudaMemcpyHostToDevice, g->stream));
     HC_CUDA_TRY(cudaMemsetAsync(is_seed, 0, (size_t)n, g->stream));
     HC_CUDA_TRY(cudaMemsetAsync(hub_count, 0, (size_t)(plan.n_hub + 1) * 4, g->stream));
-    mark_seeds<<<64, 256, 0, g->stream>>>(d_seeds, nseeds, is_seed);
+    { mark_seeds<<<64, 256, 0, g->stream>>>(d_seeds, nseeds, is_seed); ::hc::count_launch(); }
     const float *ps = weighted ? nullptr : g->inv_deg.as<float>();
-    spmm_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, K, nullptr, d_off, d_seeds, o.damping, ps, x[0], gv[0],
-                                                      x[1], gv[1], g->n_active);
+    { spmm_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, K, nullptr, d_off, d_seeds, o.damping, ps, x[0], gv[0],
+                                                      x[1], gv[1], g->n_active); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     SpmmArgs a{};
     a.index = g->index.as<int64_t>();
@@ -979,10 +979,10 @@ extern "C" hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, co
         HC_CUDA_TRY(cudaMemsetAsync(col_l1, 0, (size_t)K * 8, g->stream));
         const int cols = (K + 31) / 32;
         const int grid = g->sm_count * 8;
-        if (cols <= 1) spmm_sweep<1><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed);
-        else if (cols <= 2) spmm_sweep<2><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed);
-        else if (cols <= 4) spmm_sweep<4><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed);
-        else spmm_sweep<8><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed);
+        if (cols <= 1) { spmm_sweep<1><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed); ::hc::count_launch(); }
+        else if (cols <= 2) { spmm_sweep<2><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed); ::hc::count_launch(); }
+        else if (cols <= 4) { spmm_sweep<4><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed); ::hc::count_launch(); }
+        else { spmm_sweep<8><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         HC_CUDA_TRY(cudaMemcpyAsync(hl1.data(), col_l1, (size_t)K * 8, cudaMemcpyDeviceToHost, g->stream));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));

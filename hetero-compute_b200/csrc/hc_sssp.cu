@@ -240,6 +240,7 @@ hc_status launch_sssp(hc_graph *g, const SsspArgs &args) {
     dim3 grid(g->sm_count * bps), block(kSsspThreads);
     SsspArgs a = args;
     void *params[] = {&a};
+    ::hc::count_launch();
     HC_CUDA_TRY(cudaLaunchCooperativeKernel((void *)sssp_persistent<kStats>, grid, block, params, 0, g->stream));
     return HC_OK;
 }
@@ -293,7 +294,7 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
         int *neg = (int *)((char *)a.ctl + 2048);
         unsigned long long *sum = (unsigned long long *)((char *)a.ctl + 2056);
         HC_CUDA_TRY(cudaMemsetAsync(neg, 0, 16, g->stream));
-        weight_stats<<<g->sm_count * 4, 256, 0, g->stream>>>(a.w, g->M, neg, sum);
+        { weight_stats<<<g->sm_count * 4, 256, 0, g->stream>>>(a.w, g->M, neg, sum); ::hc::count_launch(); }
         int hneg = 0;
         unsigned long long hsum = 0;
         HC_CUDA_TRY(cudaMemcpyAsync(&hneg, neg, 4, cudaMemcpyDeviceToHost, g->stream));
@@ -324,8 +325,8 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
         HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
         if (parent_out) {
             int32_t *par = dev_parent ? parent_out + (size_t)i * n : g->ws_out1.as<int32_t>();
-            sssp_parent_init<<<g->sm_count * 4, 256, 0, g->stream>>>(par, g->N, a.src);
-            sssp_parents_fill<<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, a.w, a.dist, g->N, a.src, par);
+            { sssp_parent_init<<<g->sm_count * 4, 256, 0, g->stream>>>(par, g->N, a.src); ::hc::count_launch(); }
+            { sssp_parents_fill<<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, a.w, a.dist, g->N, a.src, par); ::hc::count_launch(); }
             HC_CUDA_TRY(cudaGetLastError());
             if (!dev_parent) HC_TRY(copy_out(parent_out + (size_t)i * n, par, 4 * n, g->stream));
         }
@@ -335,7 +336,7 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
         if (stats) {
             unsigned long long *cnt = (unsigned long long *)((char *)a.ctl + 2048);
             HC_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, g->stream));
-            count_finite<<<g->sm_count * 4, 256, 0, g->stream>>>(a.dist, g->N, cnt);
+            { count_finite<<<g->sm_count * 4, 256, 0, g->stream>>>(a.dist, g->N, cnt); ::hc::count_launch(); }
             unsigned long long reached = 0;
             HC_CUDA_TRY(cudaMemcpyAsync(&reached, cnt, 8, cudaMemcpyDeviceToHost, g->stream));
             HC_CUDA_TRY(cudaStreamSynchronize(g->stream));

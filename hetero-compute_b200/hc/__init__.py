@@ -107,6 +107,12 @@ _SIGS = {
     "hc_ppr_batched": (C.c_int, [_P, _P, _P, C.c_int32, _P, C.POINTER(PrOpts), C.POINTER(PrStats)]),
     "hc_bfs_batched": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(BatchOpts), C.POINTER(BatchStats)]),
     "hc_sssp_batched": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(BatchOpts), C.POINTER(BatchStats)]),
+    "hc_dev_malloc": (C.c_int, [C.POINTER(_P), C.c_size_t, C.c_int32]),
+    "hc_dev_free": (C.c_int, [_P]),
+    "hc_memcpy": (C.c_int, [_P, _P, C.c_size_t]),
+    "hc_dev_memset": (C.c_int, [_P, C.c_int32, C.c_size_t]),
+    "hc_device_synchronize": (C.c_int, []),
+    "hc_kernel_launches": (C.c_int64, []),
     "hc_epoch_sssp_pull": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, _P, C.c_int, C.c_int32, C.c_int32, _P]),
     "hc_epoch_pr_pull": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, _P, C.c_int32, _P, C.c_int, C.c_int32,
                                    C.c_int32, _P]),
@@ -149,6 +155,11 @@ def _ptr(x):
         assert x.is_contiguous(), "tensors passed to libhc must be contiguous"
         return x.data_ptr()
     raise TypeError(f"cannot pass {type(x)} to libhc")
+
+
+def kernel_launches() -> int:
+    """Kernels this process has launched through libhc so far."""
+    return int(lib().hc_kernel_launches())
 
 
 # ------------------------------------------------------------------ graphs

@@ -259,6 +259,19 @@ hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_t num_sourc
                           int32_t *dist_out, const hc_batch_opts *opts,
                           hc_batch_stats *stats);
 
+/* ------------------------------------------------------ device memory */
+/* Plain device-memory helpers so hosts that drive the epoch kernels below
+ * need no CUDA headers.  Replace the cudaMalloc / cudaMemcpy / cudaMemset /
+ * cudaFree calls of the reference drivers (src/kernels/gpu/sssp.cuh:52-97,
+ * src/bitmap.cuh:192-226). */
+hc_status hc_dev_malloc(void **ptr, size_t bytes, int32_t device);
+hc_status hc_dev_free(void *ptr);
+hc_status hc_memcpy(void *dst, const void *src, size_t bytes); /* any direction, synchronous */
+hc_status hc_dev_memset(void *ptr, int32_t value, size_t bytes);
+hc_status hc_device_synchronize(void);
+/* Kernels launched by this library in this process so far. */
+int64_t hc_kernel_launches(void);
+
 /* ------------------------------------------------ reference epoch kernels */
 /* One epoch of the reference's in-place pull kernels over [start_id, end_id),
  * device pointers only, launched on `stream` with the given shape and

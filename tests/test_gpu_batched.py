@@ -1,0 +1,94 @@
+"""Batched multi-source BFS / SSSP and personalised PageRank against the oracle."""
+import numpy as np
+import pytest
+
+import hc
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("scale,k", [(12, 512), (14, 100), (10, 7)])
+def test_bfs_batched_depths(scale, k):
+    host = hc.gen_kronecker(scale, 16, 31)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, k)
+    depth, st = g.bfs_batched(src)
+    assert st.groups == 1
+    for i, s in enumerate(src):
+        assert np.array_equal(depth[i], oracle.bfs_depth(host.index, host.neighbors, s)), i
+
+
+def test_bfs_batched_groups_and_duplicates():
+    host = hc.gen_kronecker(11, 8, 2)
+    g = hc.Graph.from_host(host)
+    src = np.concatenate([hc.pick_sources(host, 300), hc.pick_sources(host, 5)])  # duplicates across groups
+    depth, st = g.bfs_batched(src, group=128)
+    assert st.groups == 3
+    for i, s in enumerate(src):
+        assert np.array_equal(depth[i], oracle.bfs_depth(host.index, host.neighbors, s))
+
+
+def test_bfs_batched_grid():
+    host = hc.gen_grid(40, 50, 1)
+    g = hc.Graph.from_host(host)
+    src = np.array([0, 1999, 1000, 7], dtype=np.int32)
+    depth, st = g.bfs_batched(src)
+    for i, s in enumerate(src):
+        assert np.array_equal(depth[i], oracle.bfs_depth(host.index, host.neighbors, s))
+
+
+@pytest.mark.parametrize("scale,k", [(12, 40), (10, 32), (13, 5)])
+def test_sssp_batched_distances(scale, k):
+    host = hc.gen_kronecker(scale, 16, 41, wtype=hc.W_I32)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, k)
+    dist, st = g.sssp_batched(src)
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s)), i
+
+
+def test_sssp_batched_grid_and_hubs():
+    host = hc.gen_grid(60, 70, 2, wtype=hc.W_I32)
+    g = hc.Graph.from_host(host)
+    src = np.array([0, 4199, 2100, 33, 33], dtype=np.int32)
+    dist, _ = g.sssp_batched(src)
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s))
+    big = hc.gen_kronecker(16, 16, 3, wtype=hc.W_I32)  # rows above the chunking threshold
+    assert big.degrees().max() > 2048
+    gb = hc.Graph.from_host(big)
+    src = hc.pick_sources(big, 6)
+    dist, _ = gb.sssp_batched(src)
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(big.index, big.neighbors, big.weights, s))
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_ppr_batched_against_dense(weighted):
+    host = hc.gen_kronecker(11, 16, 5, wtype=hc.W_F32)
+    g = hc.Graph.from_host(host)
+    rng = np.random.default_rng(2)
+    k = 40
+    sizes = rng.integers(1, 33, size=k)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    seeds = np.concatenate([rng.choice(host.num_nodes, s, replace=False) for s in sizes]).astype(np.int32)
+    scores, st = g.ppr_batched(off, seeds, tol_l1=1e-8, max_iters=300, weighted=weighted)
+    w = host.weights.astype(np.float64) if weighted else None
+    for c in range(0, k, 7):
+        t = np.zeros(host.num_nodes)
+        t[seeds[off[c]:off[c + 1]]] = 1.0 / sizes[c]
+        x = oracle.pr_dense(host.index, host.neighbors, w, t)
+        assert np.abs(scores[:, c] - x).max() < 1e-6, c
+
+
+def test_dense_multicolumn_forward():
+    host = hc.gen_kronecker(10, 16, 6)
+    g = hc.Graph.from_host(host)
+    rng = np.random.default_rng(4)
+    T = rng.random((host.num_nodes, 8)).astype(np.float32)
+    T /= T.sum(axis=0, keepdims=True)
+    X, st = g.pagerank(T, tol_l1=1e-8, max_iters=300)
+    for c in range(8):
+        x = oracle.pr_dense(host.index, host.neighbors, None, T[:, c].astype(np.float64))
+        assert np.abs(X[:, c] - x).max() < 1e-6

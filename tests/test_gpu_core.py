@@ -185,11 +185,15 @@ def test_pagerank_matches_reference(graphs, name):
     rec, arr, host, g = graphs[name]
     ref = arr["pr_scores"]
     s = hc.pr_pull_gpu(g)  # the reference stopping rule: no vertex moves by > 5e-8
-    err_ref = np.abs(s - ref).max()
-    assert err_ref <= 1e-5, err_ref
-    x, _ = oracle.pr_jacobi_f64(host.index, host.neighbors)
+    x, _ = oracle.pr_jacobi_f64(host.index, host.neighbors, tol=1e-15, max_iters=3000)
     err64 = np.abs(s - x).max()
-    assert err64 <= 1e-5, err64
+    assert err64 <= 1e-6, err64
+    # The reference's in-place sweep stops on a per-vertex 5e-8 rule and lands
+    # up to a few 1e-5 from the fixed point (3.7e-5 at scale 16); the distance
+    # to it is bounded by 1e-5 plus the reference's own error.
+    ref_err = np.abs(ref - x).max()
+    err_ref = np.abs(s - ref).max()
+    assert err_ref <= max(1e-5, ref_err + 1e-6), (err_ref, ref_err)
 
 
 def test_pagerank_l1_tolerance_mode():

@@ -1,0 +1,108 @@
+"""The reference-contract epoch kernels (hc_epoch_*), driven by a host epoch
+loop exactly like the reference drivers (src/kernels/gpu/{bfs,sssp,pr}.cuh)."""
+import numpy as np
+import pytest
+
+import hc
+import oracle
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _wnodes(host):
+    """Interleaved {int32 v; float w} layout of the reference's wnode_t."""
+    w = host.weights.astype(np.float32) if host.weights is not None else np.zeros(host.num_edges, np.float32)
+    out = np.empty(2 * host.num_edges, dtype=np.int32)
+    out[0::2] = host.neighbors
+    out[1::2] = w.view(np.int32)
+    return torch.from_numpy(out).cuda()
+
+
+def _call(fn, *args):
+    s = fn(*args)
+    if s != hc.OK:
+        raise hc.HCError(s, fn.__name__, hc.lib().hc_last_error().decode())
+
+
+@pytest.mark.parametrize("variant", [hc.VARIANT_THREAD, hc.VARIANT_WARP, hc.VARIANT_BLOCK])
+def test_epoch_sssp_pull(golden, variant):
+    rec, arr = golden["kron10"]
+    from conftest import make_graph
+    host = make_graph(rec)
+    idx = torch.from_numpy(host.index).cuda()
+    nb = _wnodes(host)
+    for i, s in enumerate(rec["sssp_sources"][:4]):
+        dist = torch.full((host.num_nodes,), float("inf"), device="cuda")
+        dist[s] = 0
+        upd = torch.zeros(1, dtype=torch.int32, device="cuda")
+        for _ in range(host.num_nodes):
+            upd.zero_()
+            _call(hc.lib().hc_epoch_sssp_pull, idx.data_ptr(), nb.data_ptr(), 0, host.num_nodes, dist.data_ptr(),
+                  upd.data_ptr(), variant, 64, 256, None)
+            if int(upd.item()) == 0:
+                break
+        d = dist.cpu().numpy()
+        ref = arr["sssp_dist"][i]
+        fin = ref != hc.INF_DIST
+        assert np.array_equal(np.isinf(d), ~fin)
+        assert np.array_equal(d[fin].astype(np.int64), ref[fin].astype(np.int64))
+
+
+@pytest.mark.parametrize("variant", [hc.VARIANT_THREAD, hc.VARIANT_WARP, hc.VARIANT_BLOCK])
+def test_epoch_pr_pull(golden, variant):
+    rec, arr = golden["kron12_ef8"]
+    from conftest import make_graph
+    host = make_graph(rec)
+    n = host.num_nodes
+    idx = torch.from_numpy(host.index).cuda()
+    nb = _wnodes(host)
+    deg = torch.from_numpy(np.diff(host.index)).cuda()
+    score = torch.full((n,), 1.0 / n, device="cuda")
+    upd = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for _ in range(201):
+        upd.zero_()
+        _call(hc.lib().hc_epoch_pr_pull, idx.data_ptr(), nb.data_ptr(), 0, n, score.data_ptr(), upd.data_ptr(), n,
+              deg.data_ptr(), variant, 64, 256, None)
+        if int(upd.item()) == 0:
+            break
+    assert np.abs(score.cpu().numpy() - arr["pr_scores"]).max() <= 1e-5
+
+
+@pytest.mark.parametrize("variant", [hc.VARIANT_THREAD, hc.VARIANT_WARP])
+def test_epoch_bfs_pull(golden, variant):
+    rec, arr = golden["kron10"]
+    from conftest import make_graph
+    host = make_graph(rec)
+    n = host.num_nodes
+    words = (n + 31) // 32
+    idx = torch.from_numpy(host.index).cuda()
+    nbr = torch.from_numpy(host.neighbors).cuda()
+    for i, s in enumerate(rec["bfs_sources"][:4]):
+        par = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+        par[s] = s
+        f = [torch.zeros(words, dtype=torch.int32, device="cuda") for _ in range(2)]
+        f[0][s // 32] = np.int32(np.uint32(1 << (s % 32)).view(np.int32))
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        cur = 0
+        while True:
+            cnt.zero_()
+            f[1 - cur].zero_()
+            _call(hc.lib().hc_epoch_bfs_pull, idx.data_ptr(), nbr.data_ptr(), par.data_ptr(), 0, n,
+                  f[cur].data_ptr(), f[1 - cur].data_ptr(), cnt.data_ptr(), variant, 64, 256, None)
+            cur = 1 - cur
+            if int(cnt.item()) == 0:
+                break
+        d = oracle.bfs_depth(host.index, host.neighbors, s)
+        assert oracle.verify_bfs_parents(host.index, host.neighbors, d, par.cpu().numpy(), s)[0] == 0
+
+
+def test_epoch_rejects_bad_shape():
+    s = hc.lib().hc_epoch_sssp_pull(None, None, 0, 10, None, None, hc.VARIANT_WARP, 64, 256, None)
+    assert s == hc.INVALID_ARG
+    idx = torch.zeros(2, dtype=torch.int64, device="cuda")
+    d = torch.zeros(1, device="cuda")
+    u = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = hc.lib().hc_epoch_sssp_pull(idx.data_ptr(), idx.data_ptr(), 0, 1, d.data_ptr(), u.data_ptr(),
+                                    hc.VARIANT_WARP, 64, 100, None)
+    assert s == hc.INVALID_ARG
