@@ -49,7 +49,23 @@ def parse():
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-budget-s", type=float, default=20.0)
+    p.add_argument("--mode", choices=["bench", "profile"], default="bench",
+                   help="profile: one BFS, one SSSP and one PageRank solve, untimed (for ncu captures)")
     return p.parse_args()
+
+
+def profile_case(a):
+    """One source of BFS and SSSP, then one PageRank solve: the launches an ncu
+    capture of bfs_persistent / sssp_persistent / pr_sweep selects."""
+    import hc
+    host = hc.gen_kronecker(a.scale, a.edge_factor, a.seed, hc.W_I32)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, 1)
+    g.bfs(src)
+    g.sssp(src)
+    g.pagerank(tol_l1=1e-4, max_iters=50)
+    g.close()
+    print(json.dumps({"mode": "profile", "scale": a.scale, "num_edges": host.num_edges, "source": int(src[0])}))
 
 
 def peaks():
@@ -193,6 +209,9 @@ def main():
     if a.impl == "reference":
         run_reference_arm(a)
         return
+    if a.mode == "profile":
+        profile_case(a)
+        return
     import torch
     import torch.distributed as dist
 
@@ -217,8 +236,8 @@ def main():
     torch.cuda.set_stream(stream)
     g.set_stream(stream.cuda_stream)
     k = a.sources
-    src_all = hc.pick_sources(host, k * (rank + 1))
-    src = src_all[k * rank:]
+    from hc.shard import max_over_ranks, rank_sources
+    src = rank_sources(host, k, rank)
     src_dev = torch.from_numpy(src).to(dev)
 
     depth = torch.empty((k, n), dtype=torch.int32, device=dev)
@@ -260,10 +279,7 @@ def main():
     t = np.array(times)  # ms per algorithm per step
     step_ms = t.sum(axis=1)
     total_ms = float(step_ms.sum())
-    if world > 1:
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = max_over_ranks(total_ms, dev)
     runs = 2 * k + 1
     value = world * a.steps * runs * (m / 2) / (total_ms / 1e3) / 1e9
 
@@ -285,10 +301,7 @@ def main():
         g.pagerank(None, h_scores, tol_l1=1e-4, max_iters=50)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_total = float(np.sum(e2e_ms))
-    if world > 1:
-        tt = torch.tensor([e2e_total], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt.item())
+    e2e_total = max_over_ranks(e2e_total, dev)
     e2e_value = world * len(e2e_ms) * runs * (m / 2) / (e2e_total / 1e3) / 1e9
 
     # Roofline of the dominant kernel (largest share of the step).

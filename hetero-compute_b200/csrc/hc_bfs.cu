@@ -15,6 +15,8 @@
 //   q[2]           int32[N]      frontier queues (top-down levels)
 //   tasks          int2[]        (vertex, chunk) pieces of long rows
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "hc_expand.cuh"
@@ -24,6 +26,7 @@ namespace hc {
 namespace {
 
 constexpr int kBfsThreads = 512;
+constexpr int kTraceLevels = 64;
 
 struct LevelCnt {
     int nf;                 // vertices in this frontier
@@ -37,6 +40,10 @@ struct BfsCtl {
     int conv;               // bitmap -> queue conversion counter
     int levels, td_levels, bu_levels;
     unsigned long long vscan, escan, reached;
+    struct {
+        int mode, nf;
+        unsigned long long t_ns;
+    } trace[kTraceLevels + 1];  // per-level record for HC_TRACE=1
 };
 
 struct BfsArgs {
@@ -56,6 +63,52 @@ struct BfsArgs {
 __device__ __forceinline__ uint32_t *fb_sel(const BfsArgs &a, int i) {
     return i == 0 ? a.fb0 : (i == 1 ? a.fb1 : a.fb2);
 }
+
+// Top-down edge visitor: claim an unvisited neighbour with a CAS on its
+// parent, mark it visited and in the next frontier, queue it.
+struct TopDownVisit {
+    const int64_t *index;
+    const int32_t *nbr;
+    int32_t *parent, *depth;
+    uint32_t *visited, *fnext;
+    int32_t *qnext;
+    int *qlen;
+    int next_depth;
+    unsigned long long mf;  // degree sum of the claimed vertices (this thread)
+    struct Item {
+        int32_t u, v;
+        uint32_t word;
+    };
+    __device__ __forceinline__ void load(Item &it, int32_t u, int64_t e) {
+        it.u = u;
+        it.v = nbr[e];
+    }
+    __device__ __forceinline__ void probe(Item &it) { it.word = __ldcg(visited + (it.v >> 5)); }
+    // Stages across the round's items: all CASes in flight, then the marks,
+    // then one queue append for the whole warp.
+    __device__ __forceinline__ void commit(Item (&it)[kUnroll], const bool (&act)[kUnroll]) {
+        bool take[kUnroll];
+        int32_t old[kUnroll], v[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; j++) {
+            take[j] = act[j] && !((it[j].word >> (it[j].v & 31)) & 1u);
+            old[j] = take[j] ? atomicCAS(parent + it[j].v, -1, it[j].u) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < kUnroll; j++) {
+            take[j] = take[j] && old[j] == -1;
+            v[j] = take[j] ? it[j].v : 0;
+            if (take[j]) {
+                const uint32_t bit = 1u << (v[j] & 31);
+                depth[v[j]] = next_depth;
+                atomicOr(visited + (v[j] >> 5), bit);
+                atomicOr(fnext + (v[j] >> 5), bit);
+                mf += (unsigned long long)(index[v[j] + 1] - index[v[j]]);
+            }
+        }
+        warp_append_n(take, v, qnext, qlen);
+    }
+};
 
 template <bool kStats>
 __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
@@ -120,6 +173,11 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
         int32_t *qnext = (L & 1) ? a.q0 : a.q1;
 
         if (a.direction == 0 && push && num_edges > edges_to_check / a.alpha) push = false;
+        if (gtid == 0 && L < kTraceLevels) {
+            ctl->trace[L].mode = push ? 1 : 2;
+            ctl->trace[L].nf = nf;
+            ctl->trace[L].t_ns = globaltimer_ns();
+        }
 
         if (push) {
             if (!have_queue) {
@@ -145,23 +203,8 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
             edges_to_check -= num_edges;
             td_levels++;
             const int next_depth = L + 1;
-            unsigned long long mf_local = 0;
-            auto visit = [&](bool act, int32_t u, int64_t e) {
-                bool take = false;
-                int32_t v = 0;
-                if (act) {
-                    v = a.nbr[e];
-                    const uint32_t bit = 1u << (v & 31);
-                    if (!(__ldcg(a.visited + (v >> 5)) & bit) && atomicCAS(a.parent + v, -1, u) == -1) {
-                        a.depth[v] = next_depth;
-                        atomicOr(a.visited + (v >> 5), bit);
-                        atomicOr(fnext + (v >> 5), bit);
-                        mf_local += (unsigned long long)(a.index[v + 1] - a.index[v]);
-                        take = true;
-                    }
-                }
-                warp_append(take, v, qnext, &ctl->cnt[nxt].nf);
-            };
+            TopDownVisit visit{a.index, a.nbr, a.parent, a.depth, a.visited, fnext, qnext, &ctl->cnt[nxt].nf,
+                               next_depth, 0ull};
             if (kStats) {
                 for (int i = gtid; i < nf; i += nthreads) {
                     const int32_t u = __ldcg(qcur + i);
@@ -175,7 +218,7 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
             if (nt > 0) {
                 expand_tasks(a.index, a.tasks, nt, gwarp, nwarps, visit);
             }
-            unsigned long long mf_blk = block_sum(mf_local, s_red);
+            unsigned long long mf_blk = block_sum(visit.mf, s_red);
             if (threadIdx.x == 0 && mf_blk) atomicAdd(&ctl->cnt[nxt].mf, mf_blk);
             if (!grid_barrier(&ctl->gs)) return;
             num_edges = (long long)__ldcg(&ctl->cnt[nxt].mf);
@@ -185,9 +228,14 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
             const int next_depth = L + 1;
             int found_local = 0;
             // Rows of degree >= 32: warp per vertex, 32 probes per step.
+            // AUTO = thread granularity with four probes in flight: on the
+            // degree-sorted Kronecker graphs it beats warp-per-row for the
+            // >= 32-edge prefix (0.36 vs 0.68 ms per source at scale 22), since
+            // the first probes of a sorted row usually hit.  BLOCK selects the
+            // warp path only for that prefix.
             const int n_warp = a.bu_variant == HC_VARIANT_WARP
                                    ? a.n_active
-                                   : (a.bu_variant == HC_VARIANT_THREAD ? 0 : a.n_warp_rows);
+                                   : (a.bu_variant == HC_VARIANT_BLOCK ? a.n_warp_rows : 0);
             const int n_warp_al = min(((n_warp + 31) >> 5) << 5, W_act << 5);
             for (int v = gwarp; v < n_warp_al; v += nwarps) {
                 if (v >= a.n_active) break;
@@ -230,13 +278,20 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
                 int32_t par = -1;
                 if (v < a.n_active && !((vis >> lane) & 1u)) {
                     const int64_t b = a.index[v], e = a.index[v + 1];
-                    for (int64_t i = b; i < e; i++) {
-                        const int32_t u = a.nbr[i];
-                        if ((__ldcg(fcur + (u >> 5)) >> (u & 31)) & 1u) {
-                            par = u;
-                            if (kStats) my_escan += (unsigned long long)(i - b + 1);
-                            break;
-                        }
+                    // Four probes in flight per round; any frontier neighbour is a valid parent.
+                    for (int64_t i = b; i < e && par < 0; i += 4) {
+                        int32_t u[4];
+                        uint32_t wd[4];
+#pragma unroll
+                        for (int j = 0; j < 4; j++) u[j] = i + j < e ? a.nbr[i + j] : -1;
+#pragma unroll
+                        for (int j = 0; j < 4; j++) wd[j] = u[j] >= 0 ? __ldcg(fcur + (u[j] >> 5)) : 0u;
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            if (par < 0 && u[j] >= 0 && ((wd[j] >> (u[j] & 31)) & 1u)) {
+                                par = u[j];
+                                if (kStats) my_escan += (unsigned long long)(i + j - b + 1);
+                            }
                     }
                     if (kStats) {
                         my_vscan++;
@@ -278,6 +333,7 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
     }
     if (gtid == 0) {
         ctl->levels = L;
+        ctl->trace[L < kTraceLevels ? L : kTraceLevels].t_ns = globaltimer_ns();
         ctl->td_levels = td_levels;
         ctl->bu_levels = bu_levels;
     }
@@ -405,6 +461,13 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
             stats->bu_levels += c.bu_levels;
             stats->vertices_scanned += (int64_t)c.vscan;
             stats->edges_scanned += (int64_t)c.escan;
+        }
+        if (std::getenv("HC_TRACE")) {
+            const int nl = std::min(c.levels, kTraceLevels);
+            std::fprintf(stderr, "[hc bfs] src %d: %d levels, %.1f us\n", src[i], c.levels, ms * 1e3);
+            for (int l = 0; l < nl; l++)
+                std::fprintf(stderr, "[hc bfs]   L%-3d %s nf=%-9d %8.1f us\n", l, c.trace[l].mode == 1 ? "TD" : "BU",
+                             c.trace[l].nf, (c.trace[l + 1].t_ns - c.trace[l].t_ns) * 1e-3);
         }
     }
     if (stats) {

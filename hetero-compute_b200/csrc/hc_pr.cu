@@ -27,8 +27,8 @@ namespace {
 
 constexpr int kPrThreads = 256;
 constexpr int kStreamEdges = 2048;
-constexpr int kHubEdges = 16384;
-constexpr int kHubChunk = 8192;
+constexpr int kHubEdges = 4096;
+constexpr int kHubChunk = 2048;
 constexpr int kMaxIterSlots = 4096;
 
 struct PlanHeader {
@@ -123,9 +123,17 @@ __global__ void __launch_bounds__(kPrThreads) pr_sweep(SweepArgs a, PrPlanDev pl
             const int64_t rb = a.index[h.row], re = a.index[h.row + 1];
             const int64_t b = rb + (int64_t)tk.y * kHubChunk;
             const int64_t e = min(re, b + (int64_t)kHubChunk);
-            float s = 0.f;
-            for (int64_t i = b + lane; i < e; i += 32) s += edge_val<kEW>(a, i);
-            s = warp_sum(s);
+            // Four independent partial sums keep four gathers in flight.
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+            int64_t i = b + lane;
+            for (; i + 96 < e; i += 128) {
+                s0 += edge_val<kEW>(a, i);
+                s1 += edge_val<kEW>(a, i + 32);
+                s2 += edge_val<kEW>(a, i + 64);
+                s3 += edge_val<kEW>(a, i + 96);
+            }
+            for (; i < e; i += 32) s0 += edge_val<kEW>(a, i);
+            float s = warp_sum((s0 + s1) + (s2 + s3));
             int last = 0;
             if (lane == 0) {
                 a.partials[h.first + tk.y] = s;
@@ -228,7 +236,8 @@ __global__ void __launch_bounds__(kPrThreads) pr_sweep(SweepArgs a, PrPlanDev pl
         const int slot = a.it % kMaxIterSlots;
         const double tl1 = *(volatile double *)&a.st->l1[slot];
         const int tch = *(volatile int *)&a.st->changed[slot];
-        const bool conv = (a.tol_l1 > 0.f && tl1 < (double)a.tol_l1) || (a.eps > 0.f && tch == 0);
+        // eps >= 3e38 marks the per-vertex rule as unused.
+        const bool conv = (a.tol_l1 > 0.f && tl1 < (double)a.tol_l1) || (a.eps < 3e38f && tch == 0);
         a.st->iters = a.it + 1;
         a.st->blocks_done = 0;
         // Clear the slot the next sweep will use.

@@ -13,6 +13,8 @@
 // clearing: a vertex joins the epoch-E queue by raising stamp[v] to E);
 // tasks int2[] for long rows.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <climits>
 #include <vector>
 
@@ -23,6 +25,7 @@ namespace hc {
 namespace {
 
 constexpr int kSsspThreads = 512;
+constexpr int kTraceEpochs = 96;
 
 struct SsspCtl {
     GridSync gs;
@@ -32,6 +35,10 @@ struct SsspCtl {
     int min_far;
     int epochs, phases;
     unsigned long long vproc, erelax;
+    struct {
+        int nq, phase;
+        unsigned long long t_ns;
+    } trace[kTraceEpochs + 1];  // per-epoch record for HC_TRACE=1
 };
 
 struct SsspArgs {
@@ -46,6 +53,57 @@ struct SsspArgs {
     int32_t src;
     int32_t delta;  // <= 0: no far pile (plain frontier Bellman-Ford)
     int max_epochs;
+};
+
+// Relaxation visitor: nd = dist[u] + w; lower dist[v] with atomicMin and
+// queue v once per epoch (near) or once per phase (far), by raising a stamp.
+struct RelaxVisit {
+    const int32_t *nbr, *w;
+    int32_t *dist, *stamp, *fstamp;
+    int32_t *qnext;
+    int *qlen;
+    int32_t *fpile;
+    int *fpile_len;
+    int32_t T;
+    int next_e, far_claim;
+    bool use_far;
+    unsigned long long relaxed;
+    struct Item {
+        int32_t v, nd, dv;
+    };
+    __device__ __forceinline__ void load(Item &it, int32_t u, int64_t e) {
+        it.v = nbr[e];
+        it.nd = __ldcg(dist + u) + w[e];
+    }
+    __device__ __forceinline__ void probe(Item &it) { it.dv = __ldcg(dist + it.v); }
+    // Stages across the round's items: all atomicMins in flight, then all
+    // stamp claims, then one append per queue for the whole warp.
+    __device__ __forceinline__ void commit(Item (&it)[kUnroll], const bool (&act)[kUnroll]) {
+        bool imp[kUnroll], near[kUnroll], far[kUnroll];
+        int32_t prev[kUnroll], old[kUnroll], v[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; j++) {
+            relaxed += act[j];
+            imp[j] = act[j] && it[j].nd < it[j].dv;
+            prev[j] = imp[j] ? atomicMin(dist + it[j].v, it[j].nd) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < kUnroll; j++) {
+            imp[j] = imp[j] && it[j].nd < prev[j];
+            const bool is_near = it[j].nd < T;
+            old[j] = imp[j] ? (is_near ? atomicMax(stamp + it[j].v, next_e) : atomicMax(fstamp + it[j].v, far_claim))
+                            : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < kUnroll; j++) {
+            const bool is_near = it[j].nd < T;
+            near[j] = imp[j] && is_near && old[j] < next_e;
+            far[j] = imp[j] && !is_near && old[j] < far_claim;
+            v[j] = imp[j] ? it[j].v : 0;
+        }
+        warp_append_n(near, v, qnext, qlen);
+        if (use_far) warp_append_n(far, v, fpile, fpile_len);
+    }
 };
 
 template <bool kStats>
@@ -145,24 +203,13 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
         int32_t *fpile = (phase & 1) ? a.far1 : a.far0;
         int *fpile_len = &ctl->far_len[phase & 1];
         const int next_e = E + 1;
-        auto relax = [&](bool act, int32_t u, int64_t e) {
-            bool near = false, far = false;
-            int32_t v = 0;
-            if (act) {
-                v = a.nbr[e];
-                const int32_t nd = __ldcg(a.dist + u) + a.w[e];
-                if (kStats) my_e++;
-                if (nd < __ldcg(a.dist + v)) {
-                    const int32_t prev = atomicMin(a.dist + v, nd);
-                    if (nd < prev) {
-                        if (nd < T) near = atomicMax(a.stamp + v, next_e) < next_e;
-                        else far = atomicMax(a.fstamp + v, phase + 1) < phase + 1;
-                    }
-                }
-            }
-            warp_append(near, v, qnext, &ctl->qlen[nxt]);
-            if (use_far) warp_append(far, v, fpile, fpile_len);
-        };
+        if (gtid == 0 && E < kTraceEpochs) {
+            ctl->trace[E].nq = nq;
+            ctl->trace[E].phase = phase;
+            ctl->trace[E].t_ns = globaltimer_ns();
+        }
+        RelaxVisit relax{a.nbr, a.w, a.dist, a.stamp, a.fstamp, qnext, &ctl->qlen[nxt], fpile, fpile_len,
+                         T, next_e, phase + 1, use_far, 0ull};
         if (kStats && gtid == 0) my_v += nq;
         expand_small(a.index, qcur, nq, a.tasks, &ctl->tasks[cur], gwarp, nwarps, relax);
         if (!grid_barrier(&ctl->gs)) return;
@@ -171,6 +218,7 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
             expand_tasks(a.index, a.tasks, nt, gwarp, nwarps, relax);
             if (!grid_barrier(&ctl->gs)) return;
         }
+        if (kStats) my_e += relax.relaxed;
         E++;
     }
     if (kStats) {
@@ -181,6 +229,7 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
     }
     if (gtid == 0) {
         ctl->epochs = E;
+        ctl->trace[E < kTraceEpochs ? E : kTraceEpochs].t_ns = globaltimer_ns();
         ctl->phases = phase;
     }
 }
@@ -352,6 +401,14 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
             stats->epochs = std::max(stats->epochs, c.epochs);
             stats->vertices_processed += (int64_t)c.vproc;
             stats->edges_relaxed += (int64_t)c.erelax;
+        }
+        if (std::getenv("HC_TRACE")) {
+            const int ne = std::min(c.epochs, kTraceEpochs);
+            std::fprintf(stderr, "[hc sssp] src %d: %d epochs, %d phases, delta %d, %.1f us\n", src[i], c.epochs,
+                         c.phases, a.delta, ms * 1e3);
+            for (int e = 0; e < ne; e++)
+                std::fprintf(stderr, "[hc sssp]   E%-4d phase %-4d nq=%-9d %8.1f us\n", e, c.trace[e].phase,
+                             c.trace[e].nq, (c.trace[e + 1].t_ns - c.trace[e].t_ns) * 1e-3);
         }
     }
     if (stats) {

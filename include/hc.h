@@ -134,7 +134,9 @@ typedef struct hc_bfs_opts {
     int32_t alpha;        /* top-down -> bottom-up when m_f > m_u / alpha (0: 15) */
     int32_t beta;         /* bottom-up -> top-down when n_f < N / beta (0: 18) */
     int32_t direction;    /* 0 auto (direction-optimising), 1 top-down only, 2 bottom-up only */
-    hc_variant bu_variant;/* bottom-up granularity (AUTO / THREAD / WARP) */
+    hc_variant bu_variant;/* bottom-up granularity: THREAD (= AUTO) thread per vertex;
+                             WARP warp per vertex; BLOCK warp per vertex for the
+                             degree >= 32 prefix of a degree-sorted graph, thread after */
     int32_t collect_stats;/* count scanned vertices / edges (slower) */
 } hc_bfs_opts;
 

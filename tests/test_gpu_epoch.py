@@ -66,7 +66,12 @@ def test_epoch_pr_pull(golden, variant):
               deg.data_ptr(), variant, 64, 256, None)
         if int(upd.item()) == 0:
             break
-    assert np.abs(score.cpu().numpy() - arr["pr_scores"]).max() <= 1e-5
+    # In-place sweeps stop on the per-vertex 5e-8 rule wherever their update
+    # order leaves them; hold the kernel to the reference's own accuracy.
+    x, _ = oracle.pr_jacobi_f64(host.index, host.neighbors, tol=1e-15, max_iters=3000)
+    ref_err = np.abs(arr["pr_scores"] - x).max()
+    err = np.abs(score.cpu().numpy() - x).max()
+    assert err <= max(1e-5, 1.5 * ref_err), (err, ref_err)
 
 
 @pytest.mark.parametrize("variant", [hc.VARIANT_THREAD, hc.VARIANT_WARP])
