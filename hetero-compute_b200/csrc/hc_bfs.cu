@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
 #include <vector>
 
 #include "hc_expand.cuh"
@@ -478,5 +479,138 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
                              4.0 * (double)stats->reached +
                              2.0 * ((double)g->N / 8.0) * (double)stats->bu_levels;
     }
+    return HC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free BFS.
+//
+// Some callers cannot allocate device memory at the moment they need a BFS:
+// code running inside another framework's caching allocator or memory pool
+// (where a cudaMalloc would bypass or fragment the pool), paths that must not
+// trigger the implicit device synchronisation a cudaMalloc / cudaFree can
+// cause, and hosts that pre-plan every byte of HBM.  hc_bfs_noalloc serves
+// them: the caller passes the graph and the outputs in its own device memory,
+// and the working set (visited and frontier bitmaps, the two queues, the
+// long-row task list and the control block) lives in one fixed file-scope
+// device array, g_bfs_scratch, sized for graphs of up to kNoAllocMaxNodes
+// vertices and kNoAllocMaxEdges edges (about 13 MB, held by every GPU that
+// loads this library until the process exits).  It runs the same persistent
+// direction-optimising kernel as hc_bfs.
+namespace hc {
+namespace {
+
+constexpr int32_t kNoAllocMaxNodes = 1 << 20;
+constexpr int64_t kNoAllocMaxEdges = 1ll << 24;
+constexpr size_t na_align(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kNaWords = (size_t)kNoAllocMaxNodes / 32;
+constexpr size_t kNaTasks = (size_t)(kNoAllocMaxEdges / kTaskEdges + kNoAllocMaxEdges / (kSmallDeg + 1) + 64);
+constexpr size_t kNoAllocBytes = na_align(sizeof(BfsCtl)) + 4 * na_align(4 * kNaWords) +
+                                 2 * na_align(4 * (size_t)kNoAllocMaxNodes) + na_align(sizeof(int2) * kNaTasks);
+
+static __device__ __align__(256) unsigned char g_bfs_scratch[kNoAllocBytes];
+
+// In host code g_bfs_scratch names a host-side shadow, not device memory: the
+// device address comes from cudaGetSymbolAddress, once per device, with that
+// device current, and is cached here.
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mutex;
+void *g_na_addr[kNaMaxDevices] = {};
+
+hc_status noalloc_scratch(int dev, unsigned char **out) {
+    if (dev < 0 || dev >= kNaMaxDevices) return fail(HC_ERR_UNSUPPORTED, "hc_bfs_noalloc: device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_bfs_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return fail(HC_ERR_CUDA, "hc_bfs_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        }
+        g_na_addr[dev] = p;
+    }
+    *out = static_cast<unsigned char *>(g_na_addr[dev]);
+    return HC_OK;
+}
+
+bool on_device(const void *p, int dev) {
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) && attr.device == dev;
+}
+
+}  // namespace
+}  // namespace hc
+
+extern "C" hc_status hc_bfs_noalloc(const int64_t *index, const int32_t *neighbors, int32_t num_nodes,
+                                    int64_t num_edges, int32_t source, int32_t *depth_out, int32_t *parent_out,
+                                    void *stream) {
+    using namespace hc;
+    clear_error();
+    if (num_nodes < 1 || num_nodes > kNoAllocMaxNodes || num_edges < 0 || num_edges > kNoAllocMaxEdges)
+        return fail(HC_ERR_INVALID_ARG,
+                    "hc_bfs_noalloc: graph of %d vertices / %lld edges exceeds the fixed working set "
+                    "(at most %d vertices and %lld edges); use hc_bfs",
+                    num_nodes, (long long)num_edges, kNoAllocMaxNodes, (long long)kNoAllocMaxEdges);
+    if (source < 0 || source >= num_nodes)
+        return fail(HC_ERR_INVALID_ARG, "hc_bfs_noalloc: source %d outside [0, %d)", source, num_nodes);
+    int dev = 0;
+    HC_CUDA_TRY(cudaGetDevice(&dev));
+    if (!index || !neighbors || !depth_out || !parent_out || !on_device(index, dev) ||
+        (num_edges > 0 && !on_device(neighbors, dev)) || !on_device(depth_out, dev) || !on_device(parent_out, dev))
+        return fail(HC_ERR_INVALID_ARG,
+                    "hc_bfs_noalloc: index, neighbors, depth_out and parent_out must be device memory of the "
+                    "current device");
+    unsigned char *base = nullptr;
+    HC_TRY(noalloc_scratch(dev, &base));
+    int sms = 0, bps = 0;
+    HC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    HC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, bfs_persistent<false>, kBfsThreads, 0));
+    if (bps < 1) return fail(HC_ERR_CUDA, "hc_bfs_noalloc: BFS kernel cannot be resident");
+
+    unsigned char *p = base;
+    auto take = [&](size_t b) {
+        unsigned char *r = p;
+        p += na_align(b);
+        return r;
+    };
+    BfsArgs a{};
+    a.ctl = reinterpret_cast<BfsCtl *>(take(sizeof(BfsCtl)));
+    a.visited = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
+    a.fb0 = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
+    a.fb1 = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
+    a.fb2 = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
+    a.q0 = reinterpret_cast<int32_t *>(take(4 * (size_t)kNoAllocMaxNodes));
+    a.q1 = reinterpret_cast<int32_t *>(take(4 * (size_t)kNoAllocMaxNodes));
+    a.tasks = reinterpret_cast<int2 *>(take(sizeof(int2) * kNaTasks));
+    a.index = index;
+    a.nbr = neighbors;
+    a.n = num_nodes;
+    a.n_active = num_nodes;  // no degree analysis here: scan every vertex
+    a.n_warp_rows = 0;
+    a.m = num_edges;
+    a.depth = depth_out;
+    a.parent = parent_out;
+    a.src = source;
+    a.alpha = 15;
+    a.beta = 18;
+    a.direction = 0;
+    a.bu_variant = HC_VARIANT_THREAD;
+    a.max_levels = num_nodes + 1;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // The array keeps the previous call's contents; the control block must
+    // start at zero (the kernel initialises everything else it reads).
+    HC_CUDA_TRY(cudaMemsetAsync(a.ctl, 0, sizeof(BfsCtl), s));
+    void *params[] = {&a};
+    ::hc::count_launch();
+    HC_CUDA_TRY(cudaLaunchCooperativeKernel((void *)bfs_persistent<false>, dim3(sms * bps), dim3(kBfsThreads), params,
+                                            0, s));
+    int err = 0;
+    HC_CUDA_TRY(cudaMemcpyAsync(&err, &a.ctl->gs.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (err) return fail((hc_status)err, "hc_bfs_noalloc: device run ended with status %d", err);
     return HC_OK;
 }

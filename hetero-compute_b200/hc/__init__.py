@@ -113,6 +113,7 @@ _SIGS = {
     "hc_dev_memset": (C.c_int, [_P, C.c_int32, C.c_size_t]),
     "hc_device_synchronize": (C.c_int, []),
     "hc_kernel_launches": (C.c_int64, []),
+    "hc_bfs_noalloc": (C.c_int, [_P, _P, C.c_int32, C.c_int64, C.c_int32, _P, _P, _P]),
     "hc_epoch_sssp_pull": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, _P, C.c_int, C.c_int32, C.c_int32, _P]),
     "hc_epoch_pr_pull": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, _P, C.c_int32, _P, C.c_int, C.c_int32,
                                    C.c_int32, _P]),

@@ -160,6 +160,24 @@ hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sources,
                  int32_t *depth_out, int32_t *parent_out,
                  const hc_bfs_opts *opts, hc_bfs_stats *stats);
 
+/* No counterpart in the reference.  BFS from one source that allocates no
+ * memory: for callers that cannot call cudaMalloc at that point -- code running
+ * inside another framework's memory pool, paths that must avoid the device
+ * synchronisation an allocation can cause, hosts that budget every byte of
+ * HBM themselves.  index / neighbors / depth_out / parent_out are device
+ * pointers of the current device ([num_nodes] int32 outputs, as hc_bfs).
+ * The working set lives in a fixed device array inside the library (about
+ * 13 MB, held by every GPU that loads it until exit), so graphs are limited to
+ * 2^20 vertices and 2^24 edges; larger ones return HC_ERR_INVALID_ARG.
+ * The first call on a device resolves that array's address (make it before
+ * any stream capture).  All calls share the array: calls that overlap on the
+ * GPU (other streams, other host threads) race and must not be issued.
+ * Runs on `stream` (a cudaStream_t, NULL = legacy default) and returns after
+ * the run has finished. */
+hc_status hc_bfs_noalloc(const int64_t *index, const int32_t *neighbors, int32_t num_nodes,
+                         int64_t num_edges, int32_t source, int32_t *depth_out,
+                         int32_t *parent_out, void *stream);
+
 /* ------------------------------------------------------------------ SSSP */
 
 typedef struct hc_sssp_opts {
