@@ -441,7 +441,7 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
         if (parent_out && !dev_parent) HC_TRY(copy_out(parent_out + (size_t)i * n, a.parent, 4 * n, g->stream));
         BfsCtl c;
         HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
-        if (stats) {
+        if (o.collect_stats && stats) {
             unsigned long long *cnt = (unsigned long long *)((char *)a.ctl + 2048);
             HC_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, g->stream));
             { count_reached<<<g->sm_count * 4, 256, 0, g->stream>>>(a.depth, g->N, cnt); ::hc::count_launch(); }

@@ -308,6 +308,7 @@ hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const 
     if (res.bad_nbr) return bail(fail(HC_ERR_INVALID_ARG, "hc_graph_create: neighbour id outside [0, N)"));
 
     g->degree_sorted = !res.unsorted;
+    g->rows_sorted = !res.rows_unsorted;
     g->max_degree = res.max_degree;
     g->n_active = g->degree_sorted ? res.first_zero : num_nodes;
     if (g->degree_sorted) {

@@ -3,6 +3,32 @@
 
 #include "hc_device.cuh"
 
+namespace hc {
+// Row plan shared by the PageRank sweeps and the SSSP pull sweep, built once
+// per graph from the offsets of the rows with edges:
+//   stream groups  32 consecutive rows with <= kStreamEdges edges in total
+//   long rows      <= kHubEdges edges, one warp per row
+//   hub rows       > kHubEdges edges, cut into kHubChunk-edge tasks
+constexpr int kStreamEdges = 2048;
+constexpr int kHubEdges = 4096;
+constexpr int kHubChunk = 2048;
+
+struct HubInfo {
+    int32_t row;
+    int32_t first;  // first partial slot
+    int32_t nchunks;
+    int32_t pad;
+};
+
+struct PrPlanDev {
+    const int32_t *stream;  // group ids (rows 32*id .. 32*id+31)
+    const int32_t *longrows;
+    const int2 *tasks;      // (hub index, chunk)
+    const HubInfo *hubs;
+    int n_stream, n_long, n_tasks, n_hub;
+};
+}  // namespace hc
+
 // Layout in HBM (one allocation per array, 256-byte aligned by cudaMalloc):
 //   index     int64[N+1]                 row offsets
 //   nbr       int32[M + kNbrPad]         neighbours; the pad keeps 128-bit
@@ -23,6 +49,7 @@ struct hc_graph {
     int32_t n_active = 0;      // vertices [0, n_active) may have edges
     int32_t n_warp_rows = 0;   // degree-sorted: [0, n_warp_rows) have degree >= 32 (32-aligned)
     int32_t degree_sorted = 0;
+    int32_t rows_sorted = 0;      // every row strictly increasing
     int32_t max_degree = 0;
     hc_wtype wtype = HC_W_NONE;
 
@@ -32,11 +59,16 @@ struct hc_graph {
     hc::DevBuf inv_deg;        // f32[N]: 1/deg (0 for isolated)
     hc::DevBuf inv_wsum;       // f32[N]: 1/sum_k w_uk (weighted PageRank)
     hc::DevBuf wtn;            // f32[M]: slot (v,i) holds w_{u v}/sum_k w_uk, u = nbr[v][i]
-    hc::DevBuf pr_plan;        // PageRank row blocks
-    int32_t pr_plan_blocks = 0;
-    int32_t pr_plan_tasks = 0;
-    int32_t pr_plan_huge = 0;
+    hc::DevBuf pr_plan;        // row plan (device arrays)
+    hc::PrPlanDev pr_view{};   // host copy of its pointers and counts
+    int32_t pr_partial_slots = 0;
     hc::DevBuf pr_plan_huge_rows;
+
+    // weight statistics, computed once
+    int wstats_done = 0;
+    int w_negative = 0;
+    double w_mean = 0.0;
+    int w_symmetric = 0;       // w(u->v) == w(v->u) for every edge (rows sorted)
 
     // workspaces
     hc::DevBuf ws_bfs, ws_sssp, ws_pr, ws_batch, ws_out0, ws_out1, ws_ctl;
@@ -51,4 +83,6 @@ namespace hc {
 hc_status activate(hc_graph *g);
 // Builds inv_deg (and, for weighted graphs, inv_wsum / wtn) if missing.
 hc_status ensure_pr_derived(hc_graph *g, bool weighted);
+// Builds the row plan if missing (g->pr_view, g->pr_partial_slots).
+hc_status ensure_plan(hc_graph *g);
 }  // namespace hc

@@ -26,21 +26,7 @@ namespace hc {
 namespace {
 
 constexpr int kPrThreads = 256;
-constexpr int kStreamEdges = 2048;
-constexpr int kHubEdges = 4096;
-constexpr int kHubChunk = 2048;
 constexpr int kMaxIterSlots = 4096;
-
-struct PlanHeader {
-    int n_stream, n_long, n_tasks, n_hub;
-};
-
-struct HubInfo {
-    int32_t row;
-    int32_t first;   // first partial slot
-    int32_t nchunks;
-    int32_t pad;
-};
 
 struct IterState {
     double l1[kMaxIterSlots];
@@ -49,14 +35,6 @@ struct IterState {
     int done;
     int iters;
     int pad;
-};
-
-struct PrPlanDev {
-    const int32_t *stream;   // group ids
-    const int32_t *longrows;
-    const int2 *tasks;       // (hub index, chunk)
-    const HubInfo *hubs;
-    int n_stream, n_long, n_tasks, n_hub;
 };
 
 // One pull sweep: out[v] = base_v + d * rs_v * sum_{e in row v} ew_e * gin[nbr_e].
@@ -468,6 +446,8 @@ __global__ void spmm_residual(const double *col_l1, int K, float tol, int *done_
     }
 }
 
+}  // namespace
+
 // ------------------------------------------------------------------- plan
 
 hc_status ensure_plan(hc_graph *g) {
@@ -506,47 +486,33 @@ hc_status ensure_plan(hc_graph *g) {
     const size_t b_tasks = (tasks.size() * sizeof(int2) + 255) / 256 * 256;
     const size_t b_hubs = (hubs.size() * sizeof(HubInfo) + 255) / 256 * 256;
     HC_TRY(g->pr_plan.ensure(b_hdr + b_stream + b_long + b_tasks + b_hubs + 256));
-    char *p = g->pr_plan.as<char>();
-    PlanHeader hdr{(int)stream.size(), (int)longrows.size(), (int)tasks.size(), (int)hubs.size()};
-    HC_CUDA_TRY(cudaMemcpy(p, &hdr, sizeof(hdr), cudaMemcpyHostToDevice));
-    p += b_hdr;
+    char *p = g->pr_plan.as<char>() + b_hdr;
+    PrPlanDev v{};
+    v.n_stream = (int)stream.size();
+    v.n_long = (int)longrows.size();
+    v.n_tasks = (int)tasks.size();
+    v.n_hub = (int)hubs.size();
+    v.stream = (const int32_t *)p;
     if (!stream.empty()) HC_CUDA_TRY(cudaMemcpy(p, stream.data(), stream.size() * 4, cudaMemcpyHostToDevice));
     p += b_stream;
+    v.longrows = (const int32_t *)p;
     if (!longrows.empty()) HC_CUDA_TRY(cudaMemcpy(p, longrows.data(), longrows.size() * 4, cudaMemcpyHostToDevice));
     p += b_long;
+    v.tasks = (const int2 *)p;
     if (!tasks.empty()) HC_CUDA_TRY(cudaMemcpy(p, tasks.data(), tasks.size() * sizeof(int2), cudaMemcpyHostToDevice));
     p += b_tasks;
+    v.hubs = (const HubInfo *)p;
     if (!hubs.empty()) HC_CUDA_TRY(cudaMemcpy(p, hubs.data(), hubs.size() * sizeof(HubInfo), cudaMemcpyHostToDevice));
-    g->pr_plan_blocks = (int)stream.size();
-    g->pr_plan_tasks = (int)tasks.size();
-    g->pr_plan_huge = (int)hubs.size();
-    // Remember sizes for partial buffers.
-    HC_TRY(g->pr_plan_huge_rows.ensure(sizeof(int32_t) * 4));
-    int32_t meta[4] = {partial_slots, (int32_t)longrows.size(), 0, 0};
-    HC_CUDA_TRY(cudaMemcpy(g->pr_plan_huge_rows.ptr, meta, sizeof(meta), cudaMemcpyHostToDevice));
+    g->pr_view = v;
+    g->pr_partial_slots = partial_slots;
     return HC_OK;
 }
 
+namespace {
+
 PrPlanDev plan_view(hc_graph *g, int *partial_slots) {
-    PlanHeader hdr;
-    cudaMemcpy(&hdr, g->pr_plan.ptr, sizeof(hdr), cudaMemcpyDeviceToHost);
-    int32_t meta[4];
-    cudaMemcpy(meta, g->pr_plan_huge_rows.ptr, sizeof(meta), cudaMemcpyDeviceToHost);
-    *partial_slots = meta[0];
-    char *p = g->pr_plan.as<char>() + 256;
-    PrPlanDev v;
-    v.n_stream = hdr.n_stream;
-    v.n_long = hdr.n_long;
-    v.n_tasks = hdr.n_tasks;
-    v.n_hub = hdr.n_hub;
-    v.stream = (const int32_t *)p;
-    p += ((size_t)hdr.n_stream * 4 + 255) / 256 * 256;
-    v.longrows = (const int32_t *)p;
-    p += ((size_t)hdr.n_long * 4 + 255) / 256 * 256;
-    v.tasks = (const int2 *)p;
-    p += ((size_t)hdr.n_tasks * sizeof(int2) + 255) / 256 * 256;
-    v.hubs = (const HubInfo *)p;
-    return v;
+    *partial_slots = g->pr_partial_slots;
+    return g->pr_view;
 }
 
 template <bool kEW, bool kRS, bool kPS, bool kBaseVec>

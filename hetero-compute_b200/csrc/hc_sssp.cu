@@ -2,20 +2,26 @@
 //
 // Reference path: sssp_pull_gpu (src/kernels/gpu/sssp.cuh:42-100) sweeps every
 // vertex each epoch with an in-place Bellman-Ford pull over float weights and
-// round-trips a counter to the host per epoch.  Here only vertices whose
-// distance dropped are expanded (push relaxation with int32 atomicMin), split
-// near/far by a moving threshold (Davidson et al., "Work-efficient parallel GPU
-// methods for single-source shortest paths", IPDPS 2014), and the epoch loop
-// stays on the device.  Distances are exact integers; unreachable = INT32_MAX.
+// round-trips a counter to the host per epoch.  Here the epoch loop stays on
+// the device and each epoch picks its direction:
+//   push  relax only the edges out of vertices whose distance dropped (int32
+//         atomicMin), split near/far by a moving threshold (Davidson et al.,
+//         "Work-efficient parallel GPU methods for single-source shortest
+//         paths", IPDPS 2014);
+//   pull  when the frontier's edges exceed M / pull_alpha, sweep every row
+//         with the reference's own Bellman-Ford pull (min over neighbours of
+//         dist[u] + w), which streams the CSR without per-edge atomics, then
+//         turn the vertices it lowered back into the near queue / far pile.
+// Distances are exact integers; unreachable = INT32_MAX.
 //
 // Working set (N vertices): dist int32[N]; near queues q[2] int32[N];
 // far piles far[2] int32[N]; stamp / fstamp int32[N] (queue dedup without
 // clearing: a vertex joins the epoch-E queue by raising stamp[v] to E);
-// tasks int2[] for long rows.
+// changed bitmap uint32[N/32] (pull sweeps); tasks int2[] for long rows.
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
-#include <climits>
 #include <vector>
 
 #include "hc_expand.cuh"
@@ -26,38 +32,45 @@ namespace {
 
 constexpr int kSsspThreads = 512;
 constexpr int kTraceEpochs = 96;
+constexpr int kDefaultPullAlpha = 4;
 
 struct SsspCtl {
     GridSync gs;
     int qlen[3];
     int tasks[3];
+    unsigned long long mf[3];  // degree sum of each near queue
     int far_len[2];
     int min_far;
-    int epochs, phases;
+    int epochs, phases, pulls;
     unsigned long long vproc, erelax;
     struct {
         int nq, phase;
         unsigned long long t_ns;
-    } trace[kTraceEpochs + 1];  // per-epoch record for HC_TRACE=1
+    } trace[kTraceEpochs + 1];  // per-epoch record for HC_TRACE=1 (phase < 0: pull sweep)
 };
 
 struct SsspArgs {
     const int64_t *index;
     const int32_t *nbr;
     const int32_t *w;
-    int32_t n;
+    int32_t n, n_active;
+    int64_t m;
     int32_t *dist;
     int32_t *q0, *q1, *far0, *far1, *stamp, *fstamp;
+    uint32_t *changed;
     int2 *tasks;
     SsspCtl *ctl;
+    PrPlanDev plan;
     int32_t src;
     int32_t delta;  // <= 0: no far pile (plain frontier Bellman-Ford)
+    int pull_alpha;  // <= 0: push only
     int max_epochs;
 };
 
-// Relaxation visitor: nd = dist[u] + w; lower dist[v] with atomicMin and
+// Push relaxation visitor: nd = dist[u] + w; lower dist[v] with atomicMin and
 // queue v once per epoch (near) or once per phase (far), by raising a stamp.
 struct RelaxVisit {
+    const int64_t *index;
     const int32_t *nbr, *w;
     int32_t *dist, *stamp, *fstamp;
     int32_t *qnext;
@@ -68,6 +81,7 @@ struct RelaxVisit {
     int next_e, far_claim;
     bool use_far;
     unsigned long long relaxed;
+    unsigned long long mf;  // degree sum of this thread's near appends
     struct Item {
         int32_t v, nd, dv;
     };
@@ -100,27 +114,123 @@ struct RelaxVisit {
             near[j] = imp[j] && is_near && old[j] < next_e;
             far[j] = imp[j] && !is_near && old[j] < far_claim;
             v[j] = imp[j] ? it[j].v : 0;
+            if (near[j]) mf += (unsigned long long)(index[v[j] + 1] - index[v[j]]);
         }
         warp_append_n(near, v, qnext, qlen);
         if (use_far) warp_append_n(far, v, fpile, fpile_len);
     }
 };
 
+__device__ __forceinline__ int32_t pull_val(const SsspArgs &a, int64_t e) {
+    const int32_t du = __ldcg(a.dist + a.nbr[e]);
+    return du == kInfDist ? kInfDist : du + a.w[e];
+}
+
+// One Bellman-Ford pull over every row with edges (the reference's epoch,
+// src/kernels/gpu/sssp.cuh:120-281), on the shared row plan: hub chunks and
+// long rows reduce with a warp min and lower dist by atomicMin; stream groups
+// (32 rows, one warp) reduce with a segmented warp min and own their rows and
+// their changed-bitmap word.  Lowered vertices are marked in `changed`.
+template <bool kStats>
+__device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwarps, int32_t (*s_acc)[32],
+                                           unsigned long long &my_e) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const PrPlanDev &p = a.plan;
+    const int total = p.n_tasks + p.n_long + p.n_stream;
+    for (int item = gwarp; item < total; item += nwarps) {
+        if (item < p.n_tasks + p.n_long) {
+            int32_t r;
+            int64_t b, e;
+            if (item < p.n_tasks) {
+                const int2 tk = p.tasks[item];
+                r = p.hubs[tk.x].row;
+                const int64_t rb = a.index[r], re = a.index[r + 1];
+                b = rb + (int64_t)tk.y * kHubChunk;
+                e = min(re, b + (int64_t)kHubChunk);
+            } else {
+                r = p.longrows[item - p.n_tasks];
+                b = a.index[r];
+                e = a.index[r + 1];
+            }
+            int32_t m0 = kInfDist, m1 = kInfDist, m2 = kInfDist, m3 = kInfDist;
+            int64_t i = b + lane;
+            for (; i + 96 < e; i += 128) {
+                m0 = min(m0, pull_val(a, i));
+                m1 = min(m1, pull_val(a, i + 32));
+                m2 = min(m2, pull_val(a, i + 64));
+                m3 = min(m3, pull_val(a, i + 96));
+            }
+            for (; i < e; i += 32) m0 = min(m0, pull_val(a, i));
+            const int32_t m = warp_min(min(min(m0, m1), min(m2, m3)));
+            if (lane == 0) {
+                if (m < __ldcg(a.dist + r) && m < atomicMin(a.dist + r, m))
+                    atomicOr(a.changed + (r >> 5), 1u << (r & 31));
+                if (kStats) my_e += (unsigned long long)(e - b);
+            }
+        } else {
+            const int32_t r0 = p.stream[item - p.n_tasks - p.n_long] * 32;
+            const int32_t r = r0 + lane;
+            const int32_t rc = min(r, a.n_active);
+            const int64_t s0 = a.index[r0];
+            const int32_t rel = (int32_t)(a.index[rc] - s0);
+            const int32_t gend = (int32_t)(a.index[min(r0 + 32, a.n_active)] - s0);
+            s_acc[wib][lane] = kInfDist;
+            __syncwarp();
+            for (int k0 = 0; k0 < gend; k0 += 32) {
+                const int k = k0 + lane;
+                const bool act = k < gend;
+                int lo = 0;
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const int c = __shfl_sync(kFull, rel, lo + st);
+                    if (c <= k) lo += st;
+                }
+                const int owner = act ? lo : 32;
+                int32_t v = act ? pull_val(a, s0 + k) : kInfDist;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int32_t y = __shfl_up_sync(kFull, v, o);
+                    const int ow = __shfl_up_sync(kFull, owner, o);
+                    if (lane >= o && ow == owner) v = min(v, y);
+                }
+                const int next_owner = __shfl_down_sync(kFull, owner, 1);
+                if (act && (lane == 31 || next_owner != owner)) s_acc[wib][owner] = min(s_acc[wib][owner], v);
+                __syncwarp();
+            }
+            const int32_t m = s_acc[wib][lane];
+            bool ch = false;
+            if (r < a.n_active && m < __ldcg(a.dist + r)) {
+                a.dist[r] = m;  // the group is the only writer of its rows
+                ch = true;
+            }
+            const unsigned bal = __ballot_sync(kFull, ch);
+            if (lane == 0) {
+                if (bal) a.changed[r0 >> 5] = bal;
+                if (kStats) my_e += (unsigned long long)gend;
+            }
+            __syncwarp();
+        }
+    }
+}
+
 template <bool kStats>
 __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
     __shared__ unsigned long long s_red[32];
     __shared__ int s_min[32];
+    __shared__ int32_t s_acc[kSsspThreads / 32][32];
     SsspCtl *ctl = a.ctl;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthreads = gridDim.x * blockDim.x;
     const int gwarp = gtid >> 5, nwarps = nthreads >> 5;
     const int lane = threadIdx.x & 31;
+    const int W_act = (a.n_active + 31) >> 5;
 
     for (int i = gtid; i < a.n; i += nthreads) {
         a.dist[i] = kInfDist;
         a.stamp[i] = -1;
         a.fstamp[i] = -1;
     }
+    for (int i = gtid; i < W_act; i += nthreads) a.changed[i] = 0;
     const unsigned long long t_start = globaltimer_ns();
     if (!grid_barrier(&ctl->gs)) return;
     if (gtid == 0) {
@@ -128,13 +238,14 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
         a.stamp[a.src] = 0;
         a.q0[0] = a.src;
         ctl->qlen[0] = 1;
+        ctl->mf[0] = (unsigned long long)(a.index[a.src + 1] - a.index[a.src]);
         ctl->min_far = kInfDist;
     }
     if (!grid_barrier(&ctl->gs)) return;
 
     const bool use_far = a.delta > 0;
     int32_t T = use_far ? a.delta : kInfDist;
-    int E = 0, phase = 0;
+    int E = 0, phase = 0, pulls = 0;
     unsigned long long my_v = 0, my_e = 0;
 
     for (;;) {
@@ -164,12 +275,13 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
                 if (threadIdx.x == 0 && x < kInfDist) atomicMin(&ctl->min_far, x);
             }
             if (!grid_barrier(&ctl->gs)) return;
-            const int32_t mf = __ldcg(&ctl->min_far);
-            if (mf == kInfDist) break;
+            const int32_t mfar = __ldcg(&ctl->min_far);
+            if (mfar == kInfDist) break;
             const int32_t T_old = T;
-            const long long tn = ((long long)mf / a.delta + 1) * (long long)a.delta;
+            const long long tn = ((long long)mfar / a.delta + 1) * (long long)a.delta;
             T = (int32_t)(tn < (long long)kInfDist ? tn : (long long)kInfDist);
             // Split: [T_old, T) joins the epoch-E queue, >= T stays far.
+            unsigned long long mf_split = 0;
             for (int i0 = gwarp * 32; i0 < fl; i0 += nwarps * 32) {
                 const int i = i0 + lane;
                 bool to_near = false, to_far = false;
@@ -179,10 +291,13 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
                     const int32_t d = __ldcg(a.dist + v);
                     if (d >= T_old && d < T) to_near = atomicMax(a.stamp + v, E) < E;
                     else if (d >= T) to_far = atomicMax(a.fstamp + v, phase + 2) < phase + 2;
+                    if (to_near) mf_split += (unsigned long long)(a.index[v + 1] - a.index[v]);
                 }
                 warp_append(to_near, v, qcur, &ctl->qlen[cur]);
                 warp_append(to_far, v, fnew, &ctl->far_len[(phase + 1) & 1]);
             }
+            mf_split = block_sum(mf_split, s_red);
+            if (threadIdx.x == 0 && mf_split) atomicAdd(&ctl->mf[cur], mf_split);
             if (!grid_barrier(&ctl->gs)) return;
             if (gtid == 0) {
                 ctl->far_len[phase & 1] = 0;
@@ -199,26 +314,67 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
         if (gtid == 0) {
             ctl->qlen[old] = 0;
             ctl->tasks[old] = 0;
+            ctl->mf[old] = 0;
         }
         int32_t *fpile = (phase & 1) ? a.far1 : a.far0;
         int *fpile_len = &ctl->far_len[phase & 1];
         const int next_e = E + 1;
+        const unsigned long long mfc = __ldcg(&ctl->mf[cur]);
+        const bool pull = a.pull_alpha > 0 && (double)mfc * (double)a.pull_alpha > (double)a.m;
         if (gtid == 0 && E < kTraceEpochs) {
             ctl->trace[E].nq = nq;
-            ctl->trace[E].phase = phase;
+            ctl->trace[E].phase = pull ? -1 - phase : phase;
             ctl->trace[E].t_ns = globaltimer_ns();
         }
-        RelaxVisit relax{a.nbr, a.w, a.dist, a.stamp, a.fstamp, qnext, &ctl->qlen[nxt], fpile, fpile_len,
-                         T, next_e, phase + 1, use_far, 0ull};
         if (kStats && gtid == 0) my_v += nq;
-        expand_small(a.index, qcur, nq, a.tasks, &ctl->tasks[cur], gwarp, nwarps, relax);
-        if (!grid_barrier(&ctl->gs)) return;
-        const int nt = __ldcg(&ctl->tasks[cur]);
-        if (nt > 0) {
-            expand_tasks(a.index, a.tasks, nt, gwarp, nwarps, relax);
+        if (pull) {
+            pulls++;
+            pull_sweep<kStats>(a, gwarp, nwarps, s_acc, my_e);
             if (!grid_barrier(&ctl->gs)) return;
+            // Lowered vertices back into the near queue / far pile.
+            unsigned long long mf_next = 0;
+            for (int w0 = gwarp * 32; w0 < W_act; w0 += nwarps * 32) {
+                const int w = w0 + lane;
+                uint32_t bits = 0;
+                if (w < W_act) {
+                    bits = __ldcg(a.changed + w);
+                    if (bits) a.changed[w] = 0;
+                }
+                while (__any_sync(kFull, bits != 0)) {
+                    bool near = false, far = false;
+                    int32_t v = 0;
+                    if (bits) {
+                        v = w * 32 + __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        const int32_t d = __ldcg(a.dist + v);
+                        if (d < T) near = atomicMax(a.stamp + v, next_e) < next_e;
+                        else far = atomicMax(a.fstamp + v, phase + 1) < phase + 1;
+                        if (near) mf_next += (unsigned long long)(a.index[v + 1] - a.index[v]);
+                    }
+                    warp_append(near, v, qnext, &ctl->qlen[nxt]);
+                    if (use_far) warp_append(far, v, fpile, fpile_len);
+                }
+            }
+            mf_next = block_sum(mf_next, s_red);
+            if (threadIdx.x == 0 && mf_next) atomicAdd(&ctl->mf[nxt], mf_next);
+            if (!grid_barrier(&ctl->gs)) return;
+        } else {
+            RelaxVisit relax{a.index, a.nbr, a.w, a.dist, a.stamp, a.fstamp, qnext, &ctl->qlen[nxt], fpile,
+                             fpile_len, T, next_e, phase + 1, use_far, 0ull, 0ull};
+            expand_small(a.index, qcur, nq, a.tasks, &ctl->tasks[cur], gwarp, nwarps, relax);
+            unsigned long long mfb = block_sum(relax.mf, s_red);
+            if (threadIdx.x == 0 && mfb) atomicAdd(&ctl->mf[nxt], mfb);
+            relax.mf = 0;
+            if (!grid_barrier(&ctl->gs)) return;
+            const int nt = __ldcg(&ctl->tasks[cur]);
+            if (nt > 0) {
+                expand_tasks(a.index, a.tasks, nt, gwarp, nwarps, relax);
+                mfb = block_sum(relax.mf, s_red);
+                if (threadIdx.x == 0 && mfb) atomicAdd(&ctl->mf[nxt], mfb);
+                if (!grid_barrier(&ctl->gs)) return;
+            }
+            if (kStats) my_e += relax.relaxed;
         }
-        if (kStats) my_e += relax.relaxed;
         E++;
     }
     if (kStats) {
@@ -229,8 +385,9 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
     }
     if (gtid == 0) {
         ctl->epochs = E;
-        ctl->trace[E < kTraceEpochs ? E : kTraceEpochs].t_ns = globaltimer_ns();
         ctl->phases = phase;
+        ctl->pulls = pulls;
+        ctl->trace[E < kTraceEpochs ? E : kTraceEpochs].t_ns = globaltimer_ns();
     }
 }
 
@@ -266,13 +423,30 @@ __global__ void count_finite(const int32_t *dist, int32_t n, unsigned long long 
     if (threadIdx.x == 0 && c) atomicAdd(out, c);
 }
 
-__global__ void weight_stats(const int32_t *w, int64_t m, int *neg, unsigned long long *sum) {
+// Negative weights, their sum, and whether w(u->v) == w(v->u) everywhere
+// (binary search of the reverse slot; rows must be sorted).
+__global__ void weight_stats(const int64_t *index, const int32_t *nbr, const int32_t *w, int32_t n, int check_sym,
+                             int *neg, int *asym, unsigned long long *sum) {
     __shared__ unsigned long long s_red[32];
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
     unsigned long long s = 0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t x = w[i];
-        if (x < 0) *neg = 1;
-        s += (unsigned long long)max(x, 0);
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const int64_t b = index[v], e = index[v + 1];
+        for (int64_t i = b + lane; i < e; i += 32) {
+            const int32_t x = w[i];
+            if (x < 0) *neg = 1;
+            s += (unsigned long long)max(x, 0);
+            if (check_sym) {
+                const int32_t u = nbr[i];
+                int64_t lo = index[u], hi = index[u + 1];
+                while (lo < hi) {
+                    const int64_t mid = (lo + hi) >> 1;
+                    if (nbr[mid] < v) lo = mid + 1; else hi = mid;
+                }
+                if (lo >= index[u + 1] || nbr[lo] != v || w[lo] != x) *asym = 1;
+            }
+        }
     }
     s = block_sum(s, s_red);
     if (threadIdx.x == 0 && s) atomicAdd(sum, s);
@@ -291,6 +465,32 @@ hc_status launch_sssp(hc_graph *g, const SsspArgs &args) {
     void *params[] = {&a};
     ::hc::count_launch();
     HC_CUDA_TRY(cudaLaunchCooperativeKernel((void *)sssp_persistent<kStats>, grid, block, params, 0, g->stream));
+    return HC_OK;
+}
+
+hc_status ensure_weight_stats(hc_graph *g) {
+    if (g->wstats_done) return HC_OK;
+    DevBuf buf;
+    HC_TRY(buf.ensure(64));
+    HC_CUDA_TRY(cudaMemsetAsync(buf.ptr, 0, 64, g->stream));
+    int *flags = buf.as<int>();
+    unsigned long long *sum = reinterpret_cast<unsigned long long *>(buf.as<char>() + 16);
+    {
+        weight_stats<<<g->sm_count * 8, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
+                                                             g->wgt.as<int32_t>(), g->N, g->rows_sorted, flags,
+                                                             flags + 1, sum);
+        ::hc::count_launch();
+    }
+    HC_CUDA_TRY(cudaGetLastError());
+    int hf[2] = {0, 0};
+    unsigned long long hsum = 0;
+    HC_CUDA_TRY(cudaMemcpyAsync(hf, flags, 8, cudaMemcpyDeviceToHost, g->stream));
+    HC_CUDA_TRY(cudaMemcpyAsync(&hsum, sum, 8, cudaMemcpyDeviceToHost, g->stream));
+    HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    g->w_negative = hf[0];
+    g->w_symmetric = g->rows_sorted && !hf[1];
+    g->w_mean = g->M ? (double)hsum / (double)g->M : 1.0;
+    g->wstats_done = 1;
     return HC_OK;
 }
 
@@ -313,9 +513,15 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
     for (int32_t s : src)
         if (s < 0 || s >= g->N) return fail(HC_ERR_INVALID_ARG, "hc_sssp: source %d outside [0, %d)", s, g->N);
 
+    // Weights must be non-negative; the mean weight sets the default delta.
+    HC_TRY(ensure_weight_stats(g));
+    if (g->w_negative) return fail(HC_ERR_INVALID_ARG, "hc_sssp: negative edge weight");
+    HC_TRY(ensure_plan(g));
+
     const int64_t n = g->N;
+    const int64_t W = (n + 31) / 32;
     const int64_t ntasks = max_expand_tasks(g->M, n);
-    HC_TRY(g->ws_sssp.ensure(sizeof(int32_t) * 6 * n + sizeof(int2) * ntasks + 2048));
+    HC_TRY(g->ws_sssp.ensure(sizeof(int32_t) * 6 * n + 4 * W + sizeof(int2) * ntasks + 4096));
     HC_TRY(g->ws_ctl.ensure(4096));
     char *p = g->ws_sssp.as<char>();
     auto take = [&](size_t b) {
@@ -328,35 +534,26 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
     a.nbr = g->nbr.as<int32_t>();
     a.w = g->wgt.as<int32_t>();
     a.n = g->N;
+    a.n_active = g->n_active;
+    a.m = g->M;
     a.q0 = (int32_t *)take(4 * n);
     a.q1 = (int32_t *)take(4 * n);
     a.far0 = (int32_t *)take(4 * n);
     a.far1 = (int32_t *)take(4 * n);
     a.stamp = (int32_t *)take(4 * n);
     a.fstamp = (int32_t *)take(4 * n);
+    a.changed = (uint32_t *)take(4 * W);
     a.tasks = (int2 *)take(sizeof(int2) * ntasks);
     a.ctl = g->ws_ctl.as<SsspCtl>();
+    a.plan = g->pr_view;
     a.max_epochs = o.max_epochs > 0 ? o.max_epochs : 0x7fffffff;
-
-    // Weights must be non-negative; the mean weight sets the default delta.
-    {
-        int *neg = (int *)((char *)a.ctl + 2048);
-        unsigned long long *sum = (unsigned long long *)((char *)a.ctl + 2056);
-        HC_CUDA_TRY(cudaMemsetAsync(neg, 0, 16, g->stream));
-        { weight_stats<<<g->sm_count * 4, 256, 0, g->stream>>>(a.w, g->M, neg, sum); ::hc::count_launch(); }
-        int hneg = 0;
-        unsigned long long hsum = 0;
-        HC_CUDA_TRY(cudaMemcpyAsync(&hneg, neg, 4, cudaMemcpyDeviceToHost, g->stream));
-        HC_CUDA_TRY(cudaMemcpyAsync(&hsum, sum, 8, cudaMemcpyDeviceToHost, g->stream));
-        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        if (hneg) return fail(HC_ERR_INVALID_ARG, "hc_sssp: negative edge weight");
-        if (o.delta == 0) {
-            const double wavg = g->M ? (double)hsum / (double)g->M : 1.0;
-            const double davg = g->n_active ? (double)g->M / (double)g->n_active : 1.0;
-            a.delta = (int32_t)std::max(1.0, std::min(1e9, wavg * 32.0 / std::max(davg, 1.0)));
-        } else {
-            a.delta = o.delta;
-        }
+    // The pull sweep reads w(u->v) from v's row: only valid when weights are symmetric.
+    a.pull_alpha = !g->w_symmetric ? 0 : (o.pull_alpha == 0 ? kDefaultPullAlpha : std::max(o.pull_alpha, 0));
+    if (o.delta == 0) {
+        const double davg = g->n_active ? (double)g->M / (double)g->n_active : 1.0;
+        a.delta = (int32_t)std::max(1.0, std::min(1e9, g->w_mean * 32.0 / std::max(davg, 1.0)));
+    } else {
+        a.delta = o.delta;
     }
 
     const bool dev_dist = is_device_pointer(dist_out);
@@ -382,7 +579,7 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
         if (dist_out && !dev_dist) HC_TRY(copy_out(dist_out + (size_t)i * n, a.dist, 4 * n, g->stream));
         SsspCtl c;
         HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
-        if (stats) {
+        if (o.collect_stats && stats) {
             unsigned long long *cnt = (unsigned long long *)((char *)a.ctl + 2048);
             HC_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, g->stream));
             { count_finite<<<g->sm_count * 4, 256, 0, g->stream>>>(a.dist, g->N, cnt); ::hc::count_launch(); }
@@ -404,11 +601,13 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
         }
         if (std::getenv("HC_TRACE")) {
             const int ne = std::min(c.epochs, kTraceEpochs);
-            std::fprintf(stderr, "[hc sssp] src %d: %d epochs, %d phases, delta %d, %.1f us\n", src[i], c.epochs,
-                         c.phases, a.delta, ms * 1e3);
-            for (int e = 0; e < ne; e++)
-                std::fprintf(stderr, "[hc sssp]   E%-4d phase %-4d nq=%-9d %8.1f us\n", e, c.trace[e].phase,
-                             c.trace[e].nq, (c.trace[e + 1].t_ns - c.trace[e].t_ns) * 1e-3);
+            std::fprintf(stderr, "[hc sssp] src %d: %d epochs (%d pull), %d phases, delta %d, %.1f us\n", src[i],
+                         c.epochs, c.pulls, c.phases, a.delta, ms * 1e3);
+            for (int e = 0; e < ne; e++) {
+                const int ph = c.trace[e].phase;
+                std::fprintf(stderr, "[hc sssp]   E%-4d %s phase %-4d nq=%-9d %8.1f us\n", e, ph < 0 ? "pull" : "push",
+                             ph < 0 ? -1 - ph : ph, c.trace[e].nq, (c.trace[e + 1].t_ns - c.trace[e].t_ns) * 1e-3);
+            }
         }
     }
     if (stats) {

@@ -58,7 +58,7 @@ class BfsStats(C.Structure):
 
 
 class SsspOpts(C.Structure):
-    _fields_ = [("delta", C.c_int32), ("max_epochs", C.c_int32), ("collect_stats", C.c_int32)]
+    _fields_ = [("delta", C.c_int32), ("max_epochs", C.c_int32), ("collect_stats", C.c_int32), ("pull_alpha", C.c_int32)]
 
 
 class SsspStats(C.Structure):
@@ -309,14 +309,15 @@ class Graph:
         _check(lib().hc_bfs(self._h, _ptr(src), k, _ptr(depth), _ptr(parent), C.byref(o), C.byref(st)), "hc_bfs")
         return depth, parent, st
 
-    def sssp(self, sources, dist=None, parent=None, *, delta=0, max_epochs=0, stats=False, want_parent=False):
+    def sssp(self, sources, dist=None, parent=None, *, delta=0, max_epochs=0, stats=False, want_parent=False,
+             pull_alpha=0):
         src = np.ascontiguousarray(sources, dtype=np.int32) if not hasattr(sources, "data_ptr") else sources
         k = len(src)
         if dist is None:
             dist = np.empty((k, self.num_nodes), dtype=np.int32)
         if parent is None and want_parent:
             parent = np.empty((k, self.num_nodes), dtype=np.int32)
-        o = SsspOpts(delta, max_epochs, 1 if stats else 0)
+        o = SsspOpts(delta, max_epochs, 1 if stats else 0, pull_alpha)
         st = SsspStats()
         _check(lib().hc_sssp(self._h, _ptr(src), k, _ptr(dist), _ptr(parent), C.byref(o), C.byref(st)), "hc_sssp")
         return dist, parent, st

@@ -136,6 +136,31 @@ def test_sssp_distances_bit_exact(graphs, name, delta):
         assert oracle.verify_sp_tree(host.index, host.neighbors, host.weights, dist[i], parent[i], s) == 0
 
 
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("delta,pull_alpha", [(0, -1), (0, 1000000), (-1, 1000000), (64, 2)])
+def test_sssp_push_pull_modes_bit_exact(graphs, name, delta, pull_alpha):
+    """pull_alpha -1: push epochs only; 1e6: nearly every epoch is a pull sweep."""
+    rec, arr, host, g = graphs[name]
+    src = rec["sssp_sources"]
+    dist, _, _ = g.sssp(src, delta=delta, pull_alpha=pull_alpha)
+    for i, s in enumerate(src):
+        assert digest(dist[i]) == rec["sssp_dist_sha256"][i], (name, i, delta, pull_alpha)
+
+
+def test_sssp_asymmetric_weights_use_push():
+    """With w(u->v) != w(v->u) the pull sweep is disabled; push semantics (weight from u's row) hold."""
+    host = hc.gen_kronecker(12, 8, 3)
+    rng = np.random.default_rng(0)
+    w = rng.integers(1, 256, size=host.num_edges).astype(np.int32)
+    g = hc.Graph(host.index, host.neighbors, w)
+    src = hc.pick_sources(host, 3)
+    dist, parent, _ = g.sssp(src, pull_alpha=1000000, want_parent=True)
+    for i, s in enumerate(src):
+        d = oracle.sssp_dijkstra(host.index, host.neighbors, w, s)
+        assert np.array_equal(dist[i], d)
+        assert oracle.verify_sp_tree(host.index, host.neighbors, w, d, parent[i], s) == 0
+
+
 def test_sssp_grid_against_dijkstra():
     host = hc.gen_grid(200, 300, 3, wtype=hc.W_I32)
     g = hc.Graph.from_host(host)
