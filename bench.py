@@ -51,7 +51,152 @@ def parse():
     p.add_argument("--cpu-budget-s", type=float, default=20.0)
     p.add_argument("--mode", choices=["bench", "profile"], default="bench",
                    help="profile: one BFS, one SSSP and one PageRank solve, untimed (for ncu captures)")
+    p.add_argument("--suite", choices=["plain", "batched", "adjoint", "grid"], default="plain",
+                   help="batched: 512 BFS / 512 SSSP sources and 256 PPR columns in batched launches vs "
+                        "sequential plain launches (Kronecker scale 24); adjoint: PageRank forward vs "
+                        "forward + adjoint (scale 24, fp32 weights, and an Erdos-Renyi 2^24 graph); "
+                        "grid: SSSP on the 4096^2 grid from 16 sources")
     return p.parse_args()
+
+
+def _time_cuda(fn, torch, dev, reps=1):
+    """Device time of fn() in ms: events on the current stream, synchronised on both sides."""
+    s = torch.cuda.current_stream(dev)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1) / reps
+
+
+def run_suite(a):
+    """The batched / adjoint / grid comparisons (one JSON line each, rank 0, one GPU)."""
+    import torch
+
+    import hc
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    scale = a.scale if a.scale != 22 else 24
+    out = {"suite": a.suite, "metric": METRIC, "unit": "GTEPS", "data": "synthetic", "warmup": a.warmup,
+           "steps": a.steps}
+    t0 = time.time()
+    if a.suite == "batched":
+        host = hc.gen_kronecker(scale, a.edge_factor, a.seed, hc.W_I32)
+        g = hc.Graph.from_host(host)
+        g.set_stream(stream.cuda_stream)
+        n, m = host.num_nodes, host.num_edges
+        k = 512
+        src = hc.pick_sources(host, k)
+        src_t = torch.from_numpy(src).to(dev)
+        out["config"] = {"workload": f"kronecker-s{scale}-ef{a.edge_factor}: {k} BFS + {k} SSSP sources, "
+                                     f"256 PPR teleports (1-32 seeds each)", "num_nodes": n, "num_edges": m,
+                         "graph_gen_s": time.time() - t0}
+        depth = torch.empty((k, n), dtype=torch.int32, device=dev)
+        for _ in range(max(1, a.warmup)):
+            g.bfs_batched(src_t[:64].cpu().numpy(), depth[:64])
+        tb = _time_cuda(lambda: g.bfs_batched(src, depth), torch, dev, a.steps)
+        one = torch.empty((1, n), dtype=torch.int32, device=dev)
+        par = torch.empty((1, n), dtype=torch.int32, device=dev)
+
+        def seq_bfs():
+            for s in src:
+                g.bfs(np.array([s], dtype=np.int32), one, par)
+        ts = _time_cuda(seq_bfs, torch, dev, 1)
+        out["bfs"] = {"batched_ms": tb, "sequential_ms": ts, "batched_gteps": k * (m / 2) / tb / 1e6,
+                      "sequential_gteps": k * (m / 2) / ts / 1e6, "speedup": ts / tb}
+        del depth
+        dist_b = torch.empty((k, n), dtype=torch.int32, device=dev)
+        g.sssp_batched(src[:32], dist_b[:32])
+        tb = _time_cuda(lambda: g.sssp_batched(src, dist_b), torch, dev, 1)
+
+        def seq_sssp():
+            for s in src:
+                g.sssp(np.array([s], dtype=np.int32), one)
+        g.sssp(src[:2], dist_b[:2])
+        ts = _time_cuda(seq_sssp, torch, dev, 1)
+        out["sssp"] = {"batched_ms": tb, "sequential_ms": ts, "batched_gteps": k * (m / 2) / tb / 1e6,
+                       "sequential_gteps": k * (m / 2) / ts / 1e6, "speedup": ts / tb}
+        del dist_b
+        rng = np.random.default_rng(a.seed)
+        cols = 256
+        sizes = rng.integers(1, 33, size=cols)
+        off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+        active = np.flatnonzero(host.degrees() > 0)
+        seeds = np.concatenate([rng.choice(active, s, replace=False) for s in sizes]).astype(np.int32)
+        sc = torch.empty((n, cols), dtype=torch.float32, device=dev)
+        _, pst = g.ppr_batched(off, seeds, sc, tol_l1=1e-4, max_iters=50)
+        tb = _time_cuda(lambda: g.ppr_batched(off, seeds, sc, tol_l1=1e-4, max_iters=50), torch, dev, 1)
+        del sc
+        x1 = torch.empty(n, dtype=torch.float32, device=dev)
+        tele = torch.zeros(n, dtype=torch.float32, device=dev)
+
+        def seq_ppr():
+            for c in range(cols):
+                tele.zero_()
+                tele[torch.from_numpy(seeds[off[c]:off[c + 1]]).to(dev).long()] = 1.0 / sizes[c]
+                g.pagerank(tele, x1, tol_l1=1e-4, max_iters=50)
+        ts = _time_cuda(seq_ppr, torch, dev, 1)
+        out["ppr"] = {"columns": cols, "batched_ms": tb, "sequential_ms": ts, "speedup": ts / tb,
+                      "batched_iterations": int(pst.iterations),
+                      "batched_gteps": cols * (m / 2) / tb / 1e6, "sequential_gteps": cols * (m / 2) / ts / 1e6}
+        out["value"] = out["bfs"]["batched_gteps"]
+    elif a.suite == "adjoint":
+        res = {}
+        for name, maker in [("kronecker", lambda: hc.gen_kronecker(scale, a.edge_factor, a.seed, hc.W_F32)),
+                            ("erdos_renyi", lambda: hc.gen_uniform(24, 8, a.seed, hc.W_F32))]:
+            host = maker()
+            g = hc.Graph.from_host(host)
+            g.set_stream(stream.cuda_stream)
+            n, m = host.num_nodes, host.num_edges
+            rng = np.random.default_rng(a.seed)
+            c = torch.from_numpy(rng.standard_normal(n).astype(np.float32)).to(dev)
+            t = torch.full((n,), 1.0 / n, dtype=torch.float32, device=dev)
+            x = torch.empty(n, dtype=torch.float32, device=dev)
+            dt = torch.empty(n, dtype=torch.float32, device=dev)
+            dw = torch.empty(m, dtype=torch.float32, device=dev)
+            opts = dict(tol_l1=1e-6, max_iters=200, weighted=True)
+            g.pagerank(t, x, **opts)
+            g.pagerank_backward(x, c, dteleport=dt, dweights=dw, tol_l1=1e-6, max_iters=200, weighted=True)
+            tf = _time_cuda(lambda: g.pagerank(t, x, **opts), torch, dev, a.steps)
+            _, fst = g.pagerank(t, x, **opts)
+            tfb = _time_cuda(lambda: (g.pagerank(t, x, **opts),
+                                      g.pagerank_backward(x, c, dteleport=dt, dweights=dw, tol_l1=1e-6,
+                                                          max_iters=200, weighted=True)), torch, dev, a.steps)
+            _, _, bst = g.pagerank_backward(x, c, dteleport=dt, dweights=dw, tol_l1=1e-6, max_iters=200,
+                                            weighted=True)
+            res[name] = {"num_nodes": n, "num_edges": m, "forward_ms": tf, "forward_adjoint_ms": tfb,
+                         "ratio": tfb / tf, "forward_iterations": int(fst.iterations),
+                         "adjoint_iterations": int(bst.iterations),
+                         "forward_gbs": fst.bytes_model / (fst.ms / 1e3) / 1e9 if fst.ms else None}
+            g.close()
+        out["config"] = {"workload": f"pagerank fp32 weights row-normalised, L = c.x, tol_l1 1e-6: "
+                                     f"kronecker-s{scale}-ef{a.edge_factor} and erdos-renyi 2^24 (8 pairs/vertex)"}
+        out["adjoint"] = res
+        out["value"] = res["kronecker"]["ratio"]
+        out["unit"] = "forward+adjoint / forward"
+    else:
+        host = hc.gen_grid(4096, 4096, a.seed, hc.W_I32)
+        g = hc.Graph.from_host(host)
+        g.set_stream(stream.cuda_stream)
+        n, m = host.num_nodes, host.num_edges
+        src = hc.pick_sources(host, 16)
+        d = torch.empty((16, n), dtype=torch.int32, device=dev)
+        g.sssp(src[:1], d[:1])
+        res = {}
+        for delta in [0, 256, 1024, 4096]:
+            ms = _time_cuda(lambda: g.sssp(src, d, delta=delta), torch, dev, 1)
+            _, _, st = g.sssp(src[:1], d[:1], delta=delta, stats=True)
+            res[str(delta)] = {"ms_per_source": ms / 16, "gteps": 16 * (m / 2) / ms / 1e6, "epochs": int(st.epochs)}
+        out["config"] = {"workload": "grid 4096x4096, 4-neighbour, int32 weights [1,255], SSSP x16",
+                         "num_nodes": n, "num_edges": m}
+        out["grid_sssp"] = res
+        out["value"] = max(r["gteps"] for r in res.values())
+    print(json.dumps(out), flush=True)
 
 
 def profile_case(a):
@@ -211,6 +356,9 @@ def main():
         return
     if a.mode == "profile":
         profile_case(a)
+        return
+    if a.suite != "plain":
+        run_suite(a)
         return
     import torch
     import torch.distributed as dist

@@ -244,6 +244,14 @@ __global__ void pr_init(int32_t n, const float *basev, float base_scalar, float 
     }
 }
 
+__global__ void sum_abs(const float *v, int32_t n, double *out) {
+    __shared__ double s_red[32];
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += fabs((double)v[i]);
+    s = block_sum(s, s_red);
+    if (threadIdx.x == 0 && s != 0.0) atomicAdd(out, s);
+}
+
 __global__ void scale_vec(const float *in, float s, float *out, size_t n) {
     for (size_t v = blockIdx.x * (size_t)blockDim.x + threadIdx.x; v < n; v += (size_t)gridDim.x * blockDim.x)
         out[v] = s * in[v];
@@ -825,7 +833,17 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
     a.partials = partials;
     a.hub_count = hub_count;
     a.st = reinterpret_cast<IterState *>(g->ws_ctl.ptr);
-    a.tol_l1 = o.tol_l1;
+    // The adjoint's L1 rule is relative to sum |dL/dx| (lambda scales with it).
+    {
+        HC_TRY(g->pinned.ensure(64));
+        double *hacc = g->pinned.as<double>();
+        double *dacc = reinterpret_cast<double *>(spare);  // scratch until the solve ends
+        HC_CUDA_TRY(cudaMemsetAsync(dacc, 0, sizeof(double), g->stream));
+        { sum_abs<<<g->sm_count * 4, 256, 0, g->stream>>>(cvec, g->N, dacc); ::hc::count_launch(); }
+        HC_CUDA_TRY(cudaMemcpyAsync(hacc, dacc, sizeof(double), cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        a.tol_l1 = (float)(o.tol_l1 * *hacc);
+    }
     a.eps = o.eps_vertex > 0.f ? o.eps_vertex : 3.4e38f;
     a.max_iters = o.max_iters;
     a.n_active = g->n_active;

@@ -241,6 +241,8 @@ hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t ncols,
  * dL/dteleport = (1-d) lambda and, if dL_dweights != NULL, the gradient
  * with respect to the raw edge weights (CSR slot order; unit weights when the
  * graph is unweighted), chained through the row normalisation.
+ * Here opts->tol_l1 is relative: the solve stops when sum |lambda_new -
+ * lambda_old| < tol_l1 * sum |dL/dx|.
  * No counterpart in the reference. */
 hc_status hc_pr_backward(hc_graph *g, const float *scores, const float *dL_dscores,
                          float *dL_dteleport, float *dL_dweights,

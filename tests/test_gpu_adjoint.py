@@ -41,7 +41,7 @@ def test_adjoint_matches_dense_solve(wgraph, ugraph, weighted):
     c, t, x64, dt64, dw64 = _case(host, weighted, 5)
     x, st = g.pagerank(t.astype(np.float32), weighted=weighted, tol_l1=1e-10, max_iters=400)
     assert np.abs(x - x64).max() < 1e-7
-    dt, dw, bst = g.pagerank_backward(x, c.astype(np.float32), weighted=weighted, tol_l1=1e-6, max_iters=500)
+    dt, dw, bst = g.pagerank_backward(x, c.astype(np.float32), weighted=weighted, tol_l1=1e-9, max_iters=500)
     e_t = np.abs(dt - dt64).max() / np.abs(dt64).max()
     e_w = np.abs(dw - dw64).max() / np.abs(dw64).max()
     assert e_t < 1e-5, e_t
@@ -52,7 +52,7 @@ def test_adjoint_matches_finite_differences(wgraph):
     host, g = wgraph
     c, t, x64, _, _ = _case(host, True, 6)
     x, _ = g.pagerank(t.astype(np.float32), weighted=True, tol_l1=1e-10, max_iters=400)
-    dt, dw, _ = g.pagerank_backward(x, c.astype(np.float32), weighted=True, tol_l1=1e-6, max_iters=500)
+    dt, dw, _ = g.pagerank_backward(x, c.astype(np.float32), weighted=True, tol_l1=1e-9, max_iters=500)
     rng = np.random.default_rng(9)
     w = host.weights.astype(np.float64)
     h = 1e-6
