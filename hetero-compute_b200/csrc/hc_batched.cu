@@ -2,21 +2,28 @@
 //
 // The reference runs sources one after another, each a full driver call
 // (src/benchmarks/gpu_benchmark.cuh:577-586).  Here a group of sources shares
-// every sweep over the CSR:
+// every sweep over the CSR.
 //
 // BFS (bit-sliced frontiers, after Then et al., "The more the merrier:
-// efficient multi-source graph traversal", VLDB 2014): per vertex, K64 64-bit
-// words of `seen`, `front` and `next` bits, one bit per source, vertex-major so
-// a neighbour's frontier is one contiguous 8*K64-byte gather.  A level is a
-// pull over every vertex still missing some source: next[v] = OR_u front[u]
-// & ~seen[v], skipping neighbours whose frontier is empty (1-bit activity
-// map).  K64 lanes of a warp own one vertex.
+// efficient multi-source graph traversal", VLDB 2014).  Per vertex, K64 64-bit
+// words: `seen` (updated in place by the vertex's owner) and the frontier
+// `front` (double-buffered; valid only where the 1-bit activity map is set).
+// A level is a pull: next[v] = OR over neighbours u with an active frontier of
+// front[u], minus seen[v].
+//   - one thread per vertex, so a warp holds 32 consecutive vertices and the
+//     depth rows of each source are written 128 bytes at a time;
+//   - four neighbours in flight per thread (probe + 8*K64-byte gather each);
+//   - a `done` bitmap skips vertices every source has reached;
+//   - rows longer than kMsHub edges are cut into kMsTask-edge tasks whose
+//     warps OR their partial words into a per-row accumulator; the last task
+//     of a row (per-row counter) applies the update.
 //
-// SSSP: distances vertex-major dist[v][32] (one lane per source, 128-byte rows),
-// an activity mask per vertex (bit s = distance for source s dropped last
-// epoch) and a queue of active vertices.  An epoch relaxes every edge out of
-// the queue for all sources whose bit is set, int32 atomicMin per lane.  Rows
-// longer than kLongRow are cut into chunks processed by a second launch.
+// SSSP: distances vertex-major dist[v][32] (one lane per source, 128-byte
+// rows), an activity mask per vertex (bit s = distance for source s dropped
+// last epoch) and a queue of active vertices.  An epoch relaxes every edge out
+// of the queue for the sources whose bit is set; a warp keeps four edges in
+// flight (row loads, then atomicMins, then activity updates).  Rows longer
+// than kLongRow are cut into chunks processed by a second launch.
 #include <algorithm>
 #include <vector>
 
@@ -27,15 +34,20 @@ namespace {
 
 // ------------------------------------------------------------------- BFS
 
+constexpr int kMsHub = 256;   // rows with more edges are split into tasks
+constexpr int kMsTask = 256;  // edges per task
+constexpr int kMsThreads = 256;
+
+struct MsPlan {
+    const int32_t *hub_rows;  // rows with more than kMsHub edges
+    const int2 *tasks;        // (hub index, chunk)
+    int n_hubs, n_tasks;
+};
+
 template <int K64>
-__global__ void msbfs_init(int32_t n, int nsrc, const int32_t *src, uint64_t *seen, uint64_t *front,
-                           uint32_t *act, int W) {
-    const size_t total = (size_t)n * K64;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        seen[i] = 0;
-        front[i] = 0;
-    }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < W; i += gridDim.x * blockDim.x) act[i] = 0;
+__device__ __forceinline__ uint64_t full_mask(int word, int nsrc) {
+    const int bits = min(64, max(0, nsrc - word * 64));
+    return bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
 }
 
 template <int K64>
@@ -50,63 +62,174 @@ __global__ void msbfs_seed(int nsrc, const int32_t *src, uint64_t *seen, uint64_
     }
 }
 
-// One pull level.  Lane j of a K64-lane group owns word j of vertex v.
+// front words of source-active vertices are gathered only where act has the bit.
 template <int K64>
-__global__ void __launch_bounds__(256) msbfs_level(const int64_t *index, const int32_t *nbr, int32_t n_active,
-                                                   int nsrc, const uint64_t *seen_in, uint64_t *seen_out,
-                                                   const uint64_t *front, uint64_t *next, const uint32_t *act,
-                                                   uint32_t *act_next, int32_t *depth, int64_t n, int level,
-                                                   unsigned long long *found) {
-    constexpr int G = 32 / K64;  // vertices per warp
-    const int lane = threadIdx.x & 31;
-    const int sub = lane % K64, grp = lane / K64;
-    const unsigned gmask = (K64 == 32 ? 0xffffffffu : ((1u << K64) - 1u)) << (grp * K64);
-    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    // Valid-source mask of this lane's word.
-    const int bits_here = min(64, max(0, nsrc - sub * 64));
-    const uint64_t fm = bits_here >= 64 ? ~0ull : ((1ull << bits_here) - 1ull);
-    unsigned long long my_found = 0;
-    for (int32_t vb = gwarp * G; vb < n_active; vb += nwarps * G) {
-        const int32_t v = vb + grp;
-        const bool valid = v < n_active;
-        uint64_t s = valid ? seen_in[(size_t)v * K64 + sub] : fm;
-        uint64_t acc = 0;
-        // Vertex done for every source: skip its row (group-uniform).
-        const bool need = __any_sync(kFull, valid && (s & fm) != fm);
-        if (need) {
-            const bool mine = __any_sync(gmask, (s & fm) != fm) && valid;
-            int64_t b = 0, e = 0;
-            if (mine) {
-                b = index[v];
-                e = index[v + 1];
-            }
-            for (int64_t i = b; i < e; i++) {
-                const int32_t u = nbr[i];
-                if ((act[u >> 5] >> (u & 31)) & 1u) acc |= front[(size_t)u * K64 + sub];
-            }
-        }
-        const uint64_t nw = acc & ~s & fm;
-        if (valid) {
-            next[(size_t)v * K64 + sub] = nw;
-            seen_out[(size_t)v * K64 + sub] = s | nw;
-            if (nw && depth) {
-                uint64_t x = nw;
-                while (x) {
-                    const int b = __ffsll((long long)x) - 1;
-                    x &= x - 1;
-                    depth[(size_t)(sub * 64 + b) * n + v] = level + 1;
-                }
-            }
-        }
-        const bool any_new = __any_sync(gmask, nw != 0);
-        if (valid && sub == 0 && any_new) {
-            atomicOr(act_next + (v >> 5), 1u << (v & 31));
-            my_found++;
+__device__ __forceinline__ void or_front(const uint64_t *front, const uint32_t *act, int32_t u, uint64_t (&acc)[K64]) {
+    if ((__ldg(act + (u >> 5)) >> (u & 31)) & 1u) {
+        const uint64_t *f = front + (size_t)u * K64;
+#pragma unroll
+        for (int j = 0; j < K64; j++) acc[j] |= __ldg(f + j);
+    }
+}
+
+// Writes depth = level for every (source bit, vertex) in nw, one coalesced
+// masked store per source with a new bit among the warp's 32 vertices.
+template <int K64>
+__device__ __forceinline__ void write_depths_warp(const uint64_t (&nw)[K64], int32_t v, bool valid, int32_t *depth,
+                                                  int64_t n, int level) {
+#pragma unroll
+    for (int j = 0; j < K64; j++) {
+        uint64_t any = nw[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) any |= __shfl_xor_sync(kFull, any, o);
+        while (any) {
+            const int b = __ffsll((long long)any) - 1;
+            any &= any - 1;
+            if (valid && ((nw[j] >> b) & 1ull)) depth[(size_t)(j * 64 + b) * n + v] = level;
         }
     }
-    my_found = warp_sum(my_found);
+}
+
+template <int K64>
+__global__ void __launch_bounds__(kMsThreads) msbfs_pull(const int64_t *index, const int32_t *nbr, int32_t n_active,
+                                                         int nsrc, uint64_t *seen, const uint64_t *front,
+                                                         uint64_t *next, const uint32_t *act, uint32_t *act_next,
+                                                         uint32_t *done, int32_t *depth, int64_t n, int level,
+                                                         unsigned long long *found) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long my_found = 0;
+    for (int32_t tile = gwarp; tile * 32 < n_active; tile += nwarps) {
+        const int32_t v = tile * 32 + lane;
+        const uint32_t dw = __ldcg(done + tile);
+        bool work = v < n_active && !((dw >> lane) & 1u);
+        int64_t b = 0, e = 0;
+        if (work) {
+            b = index[v];
+            e = index[v + 1];
+            work = e - b <= kMsHub;  // longer rows: hub tasks
+        }
+        if (!__any_sync(kFull, work)) continue;
+        uint64_t acc[K64];
+#pragma unroll
+        for (int j = 0; j < K64; j++) acc[j] = 0;
+        if (work) {
+            int64_t i = b;
+            for (; i + 3 < e; i += 4) {
+                const int32_t u0 = nbr[i], u1 = nbr[i + 1], u2 = nbr[i + 2], u3 = nbr[i + 3];
+                or_front<K64>(front, act, u0, acc);
+                or_front<K64>(front, act, u1, acc);
+                or_front<K64>(front, act, u2, acc);
+                or_front<K64>(front, act, u3, acc);
+            }
+            for (; i < e; i++) or_front<K64>(front, act, nbr[i], acc);
+        }
+        uint64_t nw[K64];
+        bool any = false, full = true;
+        if (work) {
+            uint64_t *sv = seen + (size_t)v * K64;
+#pragma unroll
+            for (int j = 0; j < K64; j++) {
+                const uint64_t fm = full_mask<K64>(j, nsrc);
+                const uint64_t s = sv[j];
+                nw[j] = acc[j] & ~s & fm;
+                any |= nw[j] != 0;
+                full &= ((s | nw[j]) & fm) == fm;
+            }
+            if (any) {
+                uint64_t *fv = next + (size_t)v * K64;
+#pragma unroll
+                for (int j = 0; j < K64; j++) {
+                    sv[j] |= nw[j];
+                    fv[j] = nw[j];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < K64; j++) nw[j] = 0;
+            full = false;
+        }
+        const unsigned ab = __ballot_sync(kFull, any), fb = __ballot_sync(kFull, work && full);
+        if (lane == 0) {
+            if (ab) atomicOr(act_next + tile, ab);
+            if (fb) atomicOr(done + tile, fb);
+            my_found += __popc(ab);
+        }
+        if (depth && ab) write_depths_warp<K64>(nw, v, work, depth, n, level + 1);
+    }
     if (lane == 0 && my_found) atomicAdd(found, my_found);
+}
+
+// Hub rows: a warp per (row, chunk); partial words OR into acc[h]; the last
+// chunk of the row (counter) applies the update and resets acc / counter.
+template <int K64>
+__global__ void __launch_bounds__(kMsThreads) msbfs_hub(const int64_t *index, const int32_t *nbr, MsPlan plan,
+                                                        int nsrc, uint64_t *seen, const uint64_t *front,
+                                                        uint64_t *next, const uint32_t *act, uint32_t *act_next,
+                                                        uint32_t *done, uint64_t *hub_acc, unsigned *hub_cnt,
+                                                        int32_t *depth, int64_t n, int level,
+                                                        unsigned long long *found) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int t = gwarp; t < plan.n_tasks; t += nwarps) {
+        const int2 tk = plan.tasks[t];
+        const int32_t r = plan.hub_rows[tk.x];
+        if ((__ldcg(done + (r >> 5)) >> (r & 31)) & 1u) continue;  // same answer for every chunk of r
+        const int64_t rb = index[r], re = index[r + 1];
+        const int64_t b = rb + (int64_t)tk.y * kMsTask, e = min(re, b + (int64_t)kMsTask);
+        const int nchunks = (int)((re - rb + kMsTask - 1) / kMsTask);
+        uint64_t acc[K64];
+#pragma unroll
+        for (int j = 0; j < K64; j++) acc[j] = 0;
+        for (int64_t i = b + lane; i < e; i += 32) or_front<K64>(front, act, nbr[i], acc);
+#pragma unroll
+        for (int j = 0; j < K64; j++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[j] |= __shfl_xor_sync(kFull, acc[j], o);
+        }
+        uint64_t mine = 0;
+#pragma unroll
+        for (int j = 0; j < K64; j++)
+            if (lane == j) mine = acc[j];
+        if (lane < K64 && mine) atomicOr((unsigned long long *)&hub_acc[(size_t)tk.x * K64 + lane], mine);
+        __threadfence();
+        int last = 0;
+        if (lane == 0) last = atomicAdd(hub_cnt + tk.x, 1u) == (unsigned)(nchunks - 1);
+        last = __shfl_sync(kFull, last, 0);
+        if (!last) continue;
+        __threadfence();
+        uint64_t nw = 0;
+        bool full = true;
+        if (lane < K64) {
+            const uint64_t w = atomicExch((unsigned long long *)&hub_acc[(size_t)tk.x * K64 + lane], 0ull);
+            const uint64_t fm = full_mask<K64>(lane, nsrc);
+            const uint64_t s = seen[(size_t)r * K64 + lane];
+            nw = w & ~s & fm;
+            full = ((s | nw) & fm) == fm;
+            if (nw) seen[(size_t)r * K64 + lane] = s | nw;
+            next[(size_t)r * K64 + lane] = nw;
+        }
+        const unsigned ab = __ballot_sync(kFull, nw != 0);
+        const unsigned fb = __ballot_sync(kFull, lane < K64 && !full);
+        if (lane == 0) {
+            hub_cnt[tk.x] = 0;
+            if (ab) {
+                atomicOr(act_next + (r >> 5), 1u << (r & 31));
+                atomicAdd(found, 1ull);
+            }
+            if (!fb) atomicOr(done + (r >> 5), 1u << (r & 31));
+        }
+        if (depth && lane < K64) {
+            uint64_t x = nw;
+            while (x) {
+                const int bb = __ffsll((long long)x) - 1;
+                x &= x - 1;
+                depth[(size_t)(lane * 64 + bb) * n + r] = level + 1;
+            }
+        }
+    }
 }
 
 // ------------------------------------------------------------------ SSSP
@@ -136,7 +259,9 @@ __global__ void mssp_seed(int nsrc, const int32_t *src, int32_t *dist, uint32_t 
     }
 }
 
-// Relax 32 consecutive edges [e0, e1) of row u for the sources in `m`.
+// Relax edges [e0, e1) of row u for the sources in `m` (lane = source), four
+// edges in flight: all distance-row loads, then all atomicMins, then the
+// activity updates of the four target vertices by lanes 0..3.
 __device__ __forceinline__ void mssp_relax_range(const int32_t *nbr, const int32_t *w, int32_t *dist, uint32_t m,
                                                  int32_t du, int64_t e0, int64_t e1, uint32_t *act_next,
                                                  int32_t *qnext, int *qlen, unsigned long long &relaxed) {
@@ -150,19 +275,37 @@ __device__ __forceinline__ void mssp_relax_range(const int32_t *nbr, const int32
             vv = nbr[my];
             ww = w[my];
         }
-        for (int j = 0; j < cnt; j++) {
-            const int32_t v = __shfl_sync(kFull, vv, j);
-            const int32_t wt = __shfl_sync(kFull, ww, j);
-            bool imp = false;
-            if (on) {
-                const int32_t nd = du + wt;
-                int32_t *dp = dist + (size_t)v * 32 + lane;
-                if (nd < __ldcg(dp)) imp = nd < atomicMin(dp, nd);
+        for (int j0 = 0; j0 < cnt; j0 += 4) {
+            int32_t v[4], nd[4], d[4], prev[4];
+            bool ok[4], imp[4];
+            unsigned bal[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int idx = j0 + k;
+                v[k] = __shfl_sync(kFull, vv, idx & 31);
+                nd[k] = du + __shfl_sync(kFull, ww, idx & 31);
+                ok[k] = on && idx < cnt;
             }
-            const unsigned bal = __ballot_sync(kFull, imp);
-            if (bal && lane == 0) {
-                const uint32_t old = atomicOr(act_next + v, bal);
-                if (old == 0) qnext[atomicAdd(qlen, 1)] = v;
+#pragma unroll
+            for (int k = 0; k < 4; k++) d[k] = ok[k] ? __ldcg(dist + (size_t)v[k] * 32 + lane) : kInfDist;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                imp[k] = ok[k] && nd[k] < d[k];
+                prev[k] = imp[k] ? atomicMin(dist + (size_t)v[k] * 32 + lane, nd[k]) : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) bal[k] = __ballot_sync(kFull, imp[k] && nd[k] < prev[k]);
+            const unsigned mybal = lane == 0 ? bal[0] : lane == 1 ? bal[1] : lane == 2 ? bal[2] : lane == 3 ? bal[3] : 0u;
+            const int32_t myv = lane == 0 ? v[0] : lane == 1 ? v[1] : lane == 2 ? v[2] : v[3];
+            bool app = false;
+            if (mybal) app = atomicOr(act_next + myv, mybal) == 0u;
+            const unsigned ap = __ballot_sync(kFull, app);
+            if (ap) {
+                int base_q = 0;
+                const int leader = __ffs(ap) - 1;
+                if (lane == leader) base_q = atomicAdd(qlen, __popc(ap));
+                base_q = __shfl_sync(kFull, base_q, leader);
+                if (app) qnext[base_q + __popc(ap & ((1u << lane) - 1u))] = myv;
             }
         }
         relaxed += (unsigned long long)cnt * __popc(m);
@@ -248,46 +391,102 @@ using namespace hc;
 
 namespace {
 
+// Hub rows (> kMsHub edges) and their (row, chunk) tasks, built once per graph.
+hc_status ensure_ms_plan(hc_graph *g, MsPlan *plan) {
+    if (g->ms_hubs >= 0) {
+        const size_t b_rows = ((size_t)g->ms_hubs * 4 + 255) / 256 * 256;
+        plan->hub_rows = g->ws_plan_ms.as<const int32_t>();
+        plan->tasks = reinterpret_cast<const int2 *>(g->ws_plan_ms.as<const char>() + b_rows);
+        plan->n_hubs = g->ms_hubs;
+        plan->n_tasks = g->ms_tasks;
+        return HC_OK;
+    }
+    const int32_t na = g->n_active;
+    std::vector<int64_t> idx((size_t)na + 1);
+    HC_CUDA_TRY(cudaMemcpy(idx.data(), g->index.as<int64_t>(), sizeof(int64_t) * ((size_t)na + 1),
+                           cudaMemcpyDeviceToHost));
+    std::vector<int32_t> rows;
+    std::vector<int2> tasks;
+    for (int32_t r = 0; r < na; r++) {
+        const int64_t d = idx[r + 1] - idx[r];
+        if (d > kMsHub) {
+            const int nc = (int)((d + kMsTask - 1) / kMsTask);
+            for (int c = 0; c < nc; c++) tasks.push_back(make_int2((int)rows.size(), c));
+            rows.push_back(r);
+        }
+    }
+    const size_t b_rows = (rows.size() * 4 + 255) / 256 * 256;
+    HC_TRY(g->ws_plan_ms.ensure(b_rows + tasks.size() * sizeof(int2) + 256));
+    char *p = g->ws_plan_ms.as<char>();
+    if (!rows.empty()) HC_CUDA_TRY(cudaMemcpy(p, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice));
+    if (!tasks.empty())
+        HC_CUDA_TRY(cudaMemcpy(p + b_rows, tasks.data(), tasks.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    plan->hub_rows = (const int32_t *)p;
+    plan->tasks = (const int2 *)(p + b_rows);
+    plan->n_hubs = (int)rows.size();
+    plan->n_tasks = (int)tasks.size();
+    g->ms_hubs = plan->n_hubs;
+    g->ms_tasks = plan->n_tasks;
+    return HC_OK;
+}
+
 template <int K64>
-hc_status run_msbfs(hc_graph *g, const int32_t *d_src, int nsrc, int32_t *depth, const hc_batch_opts &o,
-                    int *levels_out, double *bytes) {
+hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int nsrc, int32_t *depth,
+                    const hc_batch_opts &o, int *levels_out, double *bytes) {
     const int64_t n = g->N;
     const int W = (int)((n + 31) / 32);
     const size_t nk = (size_t)n * K64;
-    HC_TRY(g->ws_batch.ensure(nk * 8 * 4 + (size_t)W * 4 * 2 + 4096));
+    const size_t hk = (size_t)std::max(plan.n_hubs, 1) * K64;
+    HC_TRY(g->ws_batch.ensure(nk * 8 * 3 + (size_t)W * 4 * 3 + hk * 8 + (size_t)std::max(plan.n_hubs, 1) * 4 + 8192));
     char *p = g->ws_batch.as<char>();
     auto take = [&](size_t b) {
         char *r = p;
         p += (b + 255) / 256 * 256;
         return r;
     };
-    uint64_t *seen[2] = {(uint64_t *)take(nk * 8), (uint64_t *)take(nk * 8)};
+    uint64_t *seen = (uint64_t *)take(nk * 8);
     uint64_t *fr[2] = {(uint64_t *)take(nk * 8), (uint64_t *)take(nk * 8)};
     uint32_t *act[2] = {(uint32_t *)take((size_t)W * 4), (uint32_t *)take((size_t)W * 4)};
+    uint32_t *done = (uint32_t *)take((size_t)W * 4);
+    uint64_t *hub_acc = (uint64_t *)take(hk * 8);
+    unsigned *hub_cnt = (unsigned *)take((size_t)std::max(plan.n_hubs, 1) * 4);
     unsigned long long *found = (unsigned long long *)take(64);
-    const int grid = g->sm_count * 8;
-    { msbfs_init<K64><<<grid, 256, 0, g->stream>>>(g->N, nsrc, d_src, seen[0], fr[0], act[0], W); ::hc::count_launch(); }
-    HC_CUDA_TRY(cudaMemsetAsync(act[1], 0, (size_t)W * 4, g->stream));
+    HC_CUDA_TRY(cudaMemsetAsync(seen, 0, nk * 8, g->stream));
+    HC_CUDA_TRY(cudaMemsetAsync(act[0], 0, (size_t)W * 4, g->stream));
+    HC_CUDA_TRY(cudaMemsetAsync(done, 0, (size_t)W * 4, g->stream));
+    HC_CUDA_TRY(cudaMemsetAsync(hub_acc, 0, hk * 8, g->stream));
+    HC_CUDA_TRY(cudaMemsetAsync(hub_cnt, 0, (size_t)std::max(plan.n_hubs, 1) * 4, g->stream));
     if (depth) HC_CUDA_TRY(cudaMemsetAsync(depth, 0xff, sizeof(int32_t) * (size_t)nsrc * n, g->stream));
-    { msbfs_seed<K64><<<(nsrc + 255) / 256, 256, 0, g->stream>>>(nsrc, d_src, seen[0], fr[0], act[0], depth, n); ::hc::count_launch(); }
+    { msbfs_seed<K64><<<(nsrc + 255) / 256, 256, 0, g->stream>>>(nsrc, d_src, seen, fr[0], act[0], depth, n); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     const int max_levels = o.max_epochs > 0 ? o.max_epochs : g->N + 1;
+    const int grid = g->sm_count * 8;
+    HC_TRY(g->pinned.ensure(64));
+    volatile unsigned long long *hfound = g->pinned.as<unsigned long long>();
     int level = 0;
     double b = 0;
     for (; level < max_levels; level++) {
         const int c = level & 1;
         HC_CUDA_TRY(cudaMemsetAsync(found, 0, 8, g->stream));
         HC_CUDA_TRY(cudaMemsetAsync(act[c ^ 1], 0, (size_t)W * 4, g->stream));
-        { msbfs_level<K64><<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->n_active, nsrc,
-                                                      seen[c], seen[c ^ 1], fr[c], fr[c ^ 1], act[c], act[c ^ 1],
-                                                      depth, n, level, found); ::hc::count_launch(); }
+        if (plan.n_tasks > 0) {
+            msbfs_hub<K64><<<grid, kMsThreads, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), plan, nsrc,
+                                                               seen, fr[c], fr[c ^ 1], act[c], act[c ^ 1], done,
+                                                               hub_acc, hub_cnt, depth, n, level, found);
+            ::hc::count_launch();
+        }
+        {
+            msbfs_pull<K64><<<grid, kMsThreads, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
+                                                                g->n_active, nsrc, seen, fr[c], fr[c ^ 1], act[c],
+                                                                act[c ^ 1], done, depth, n, level, found);
+            ::hc::count_launch();
+        }
         HC_CUDA_TRY(cudaGetLastError());
-        unsigned long long h = 0;
-        HC_CUDA_TRY(cudaMemcpyAsync(&h, found, 8, cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaMemcpyAsync((void *)hfound, found, 8, cudaMemcpyDeviceToHost, g->stream));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        // Offsets + neighbours once per level, plus seen/next words per vertex.
+        // Offsets + neighbours once per level, plus seen / frontier words per vertex.
         b += 8.0 * (n + 1) + 4.0 * g->M + 3.0 * 8.0 * K64 * (double)g->n_active;
-        if (h == 0) {
+        if (*hfound == 0) {
             level++;
             break;
         }
@@ -314,13 +513,11 @@ extern "C" hc_status hc_bfs_batched(hc_graph *g, const int32_t *sources, int32_t
     const int group = o.group > 0 ? std::min(o.group, 512) : 512;
     const int64_t n = g->N;
     const bool dev_out = is_device_pointer(depth_out);
-    int32_t *d_src = nullptr;
-    HC_CUDA_TRY(cudaMalloc(&d_src, sizeof(int32_t) * num_sources));
-    struct Free {
-        int32_t *p;
-        ~Free() { cudaFree(p); }
-    } fr{d_src};
-    HC_CUDA_TRY(cudaMemcpy(d_src, src.data(), sizeof(int32_t) * num_sources, cudaMemcpyHostToDevice));
+    MsPlan plan{};
+    HC_TRY(ensure_ms_plan(g, &plan));
+    HC_TRY(g->ws_src.ensure(sizeof(int32_t) * (size_t)num_sources));
+    int32_t *d_src = g->ws_src.as<int32_t>();
+    HC_CUDA_TRY(cudaMemcpyAsync(d_src, src.data(), sizeof(int32_t) * num_sources, cudaMemcpyHostToDevice, g->stream));
     HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     int max_levels = 0, groups = 0;
     double bytes = 0;
@@ -338,11 +535,12 @@ extern "C" hc_status hc_bfs_batched(hc_graph *g, const int32_t *sources, int32_t
         int lv = 0;
         double b = 0;
         const int k64 = (k + 63) / 64;
-        if (k64 <= 1) HC_TRY(run_msbfs<1>(g, d_src + s0, k, dep, o, &lv, &b));
-        else if (k64 <= 2) HC_TRY(run_msbfs<2>(g, d_src + s0, k, dep, o, &lv, &b));
-        else if (k64 <= 4) HC_TRY(run_msbfs<4>(g, d_src + s0, k, dep, o, &lv, &b));
-        else HC_TRY(run_msbfs<8>(g, d_src + s0, k, dep, o, &lv, &b));
-        if (depth_out && !dev_out) HC_TRY(copy_out(depth_out + (size_t)s0 * n, dep, sizeof(int32_t) * (size_t)k * n, g->stream));
+        if (k64 <= 1) HC_TRY(run_msbfs<1>(g, plan, d_src + s0, k, dep, o, &lv, &b));
+        else if (k64 <= 2) HC_TRY(run_msbfs<2>(g, plan, d_src + s0, k, dep, o, &lv, &b));
+        else if (k64 <= 4) HC_TRY(run_msbfs<4>(g, plan, d_src + s0, k, dep, o, &lv, &b));
+        else HC_TRY(run_msbfs<8>(g, plan, d_src + s0, k, dep, o, &lv, &b));
+        if (depth_out && !dev_out)
+            HC_TRY(copy_out(depth_out + (size_t)s0 * n, dep, sizeof(int32_t) * (size_t)k * n, g->stream));
         max_levels = std::max(max_levels, lv);
         bytes += b;
     }
@@ -392,6 +590,8 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
     if (dist_out && !dev_out) HC_TRY(g->ws_out0.ensure(sizeof(int32_t) * (size_t)32 * n));
     const int grid = g->sm_count * 8;
     const int max_epochs = o.max_epochs > 0 ? o.max_epochs : 0x7fffffff;
+    HC_TRY(g->pinned.ensure(64));
+    volatile int *hq = g->pinned.as<int>();
     HC_CUDA_TRY(cudaMemsetAsync(relaxed, 0, 8, g->stream));
     HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     int epochs_max = 0, groups = 0;
@@ -401,9 +601,9 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
         { mssp_init<<<grid, 256, 0, g->stream>>>(g->N, dist, act[0], act[1]); ::hc::count_launch(); }
         { mssp_seed<<<1, 32, 0, g->stream>>>(k, d_src, dist, act[0], q[0], &ctr[0]); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
-        int nq = 0;
-        HC_CUDA_TRY(cudaMemcpyAsync(&nq, &ctr[0], 4, cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaMemcpyAsync((void *)hq, &ctr[0], 4, cudaMemcpyDeviceToHost, g->stream));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        int nq = *hq;
         int ep = 0;
         for (; nq > 0; ep++) {
             if (ep >= max_epochs) return fail(HC_ERR_NOT_CONVERGED, "hc_sssp_batched: epoch cap reached");
@@ -418,8 +618,9 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
                                                     relaxed); ::hc::count_launch(); }
             { mssp_clear<<<(nq + 255) / 256, 256, 0, g->stream>>>(q[c], nq, act[c]); ::hc::count_launch(); }
             HC_CUDA_TRY(cudaGetLastError());
-            HC_CUDA_TRY(cudaMemcpyAsync(&nq, &ctr[c ^ 1], 4, cudaMemcpyDeviceToHost, g->stream));
+            HC_CUDA_TRY(cudaMemcpyAsync((void *)hq, &ctr[c ^ 1], 4, cudaMemcpyDeviceToHost, g->stream));
             HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            nq = *hq;
         }
         epochs_max = std::max(epochs_max, ep);
         if (dist_out) {

@@ -215,7 +215,7 @@ hc_status ensure_pr_derived(hc_graph *g, bool weighted) {
 int64_t hc_graph::bytes_held() const {
     const hc::DevBuf *bufs[] = {&index, &nbr, &wgt, &inv_deg, &inv_wsum, &wtn, &pr_plan,
                                 &pr_plan_huge_rows, &ws_bfs, &ws_sssp, &ws_pr, &ws_batch,
-                                &ws_out0, &ws_out1, &ws_ctl};
+                                &ws_out0, &ws_out1, &ws_ctl, &ws_plan_ms, &ws_src};
     int64_t t = 0;
     for (auto *b : bufs) t += (int64_t)b->bytes;
     return t;
@@ -328,7 +328,7 @@ hc_status hc_graph_destroy(hc_graph *g) {
     if (g->stream && g->stream != g->own_stream) cudaStreamSynchronize(g->stream);
     DevBuf *bufs[] = {&g->index, &g->nbr, &g->wgt, &g->inv_deg, &g->inv_wsum, &g->wtn, &g->pr_plan,
                       &g->pr_plan_huge_rows, &g->ws_bfs, &g->ws_sssp, &g->ws_pr, &g->ws_batch,
-                      &g->ws_out0, &g->ws_out1, &g->ws_ctl};
+                      &g->ws_out0, &g->ws_out1, &g->ws_ctl, &g->ws_plan_ms, &g->ws_src};
     for (auto *b : bufs) b->release();
     g->pinned.release();
     if (g->ev_start) cudaEventDestroy(g->ev_start);

@@ -70,8 +70,12 @@ struct hc_graph {
     double w_mean = 0.0;
     int w_symmetric = 0;       // w(u->v) == w(v->u) for every edge (rows sorted)
 
+    // batched-BFS hub plan (rows above its split threshold, (row, chunk) tasks)
+    hc::DevBuf ws_plan_ms;
+    int32_t ms_hubs = -1, ms_tasks = 0;
+
     // workspaces
-    hc::DevBuf ws_bfs, ws_sssp, ws_pr, ws_batch, ws_out0, ws_out1, ws_ctl;
+    hc::DevBuf ws_bfs, ws_sssp, ws_pr, ws_batch, ws_out0, ws_out1, ws_ctl, ws_src;
     hc::PinnedBuf pinned;
 
     int bfs_grid = 0, sssp_grid = 0;
