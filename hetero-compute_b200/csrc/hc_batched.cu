@@ -452,6 +452,7 @@ hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int n
     unsigned *hub_cnt = (unsigned *)take((size_t)std::max(plan.n_hubs, 1) * 4);
     unsigned long long *found = (unsigned long long *)take(64);
     HC_CUDA_TRY(cudaMemsetAsync(seen, 0, nk * 8, g->stream));
+    HC_CUDA_TRY(cudaMemsetAsync(fr[0], 0, nk * 8, g->stream));  // the seed ORs into it
     HC_CUDA_TRY(cudaMemsetAsync(act[0], 0, (size_t)W * 4, g->stream));
     HC_CUDA_TRY(cudaMemsetAsync(done, 0, (size_t)W * 4, g->stream));
     HC_CUDA_TRY(cudaMemsetAsync(hub_acc, 0, hk * 8, g->stream));
