@@ -25,6 +25,9 @@
 // flight (row loads, then atomicMins, then activity updates).  Rows longer
 // than kLongRow are cut into chunks processed by a second launch.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "hc_graph.cuh"
@@ -232,6 +235,133 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_hub(const int64_t *index, co
     }
 }
 
+// Push levels (sparse frontiers).  The active vertices become (vertex, chunk)
+// tasks of kMsPushChunk edges; each edge ORs the source's frontier words, minus
+// the target's seen words, into an accumulator x[v] and queues v once per
+// level; a finalize pass applies x to seen / next / depth and clears it.
+constexpr int kMsPushChunk = 2048;
+
+__global__ void msbfs_push_tasks(const int64_t *index, const uint32_t *act, int32_t n_active, int2 *tasks,
+                                 int *ntasks, unsigned long long *fedges) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long my_e = 0;
+    const int words = (n_active + 31) >> 5;
+    for (int w = gwarp; w < words; w += nwarps) {
+        const uint32_t bits = __ldcg(act + w);
+        const int32_t v = w * 32 + lane;
+        int nc = 0;
+        if ((bits >> lane) & 1u) {
+            const int64_t d = index[v + 1] - index[v];
+            my_e += (unsigned long long)d;
+            nc = (int)((d + kMsPushChunk - 1) / kMsPushChunk);
+        }
+        int total;
+        const int excl = warp_exclusive_scan(nc, &total);
+        int base = 0;
+        if (lane == 0 && total) base = atomicAdd(ntasks, total);
+        base = __shfl_sync(kFull, base, 0);
+        for (int c = 0; c < nc; c++) tasks[base + excl + c] = make_int2(v, c);
+    }
+    my_e = warp_sum(my_e);
+    if (lane == 0 && my_e) atomicAdd(fedges, my_e);
+}
+
+template <int K64>
+__global__ void __launch_bounds__(kMsThreads) msbfs_push(const int64_t *index, const int32_t *nbr, const int2 *tasks,
+                                                         const int *ntasks, const uint64_t *front,
+                                                         const uint64_t *seen, uint64_t *xacc, uint32_t *touched,
+                                                         int32_t *tlist, int *tlen) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nt = *ntasks;
+    for (int t = gwarp; t < nt; t += nwarps) {
+        const int2 tk = tasks[t];
+        const int32_t u = tk.x;
+        uint64_t fu[K64];
+#pragma unroll
+        for (int j = 0; j < K64; j++) fu[j] = __ldg(front + (size_t)u * K64 + j);
+        const int64_t rb = index[u], re = index[u + 1];
+        const int64_t b = rb + (int64_t)tk.y * kMsPushChunk, e = min(re, b + (int64_t)kMsPushChunk);
+        for (int64_t i0 = b; i0 < e; i0 += 32) {
+            const int64_t i = i0 + lane;
+            bool take = false;
+            int32_t v = 0;
+            if (i < e) {
+                v = nbr[i];
+                const uint64_t *sv = seen + (size_t)v * K64;
+                bool any = false;
+#pragma unroll
+                for (int j = 0; j < K64; j++) {
+                    const uint64_t nw = fu[j] & ~__ldcg(sv + j);
+                    if (nw) {
+                        atomicOr((unsigned long long *)&xacc[(size_t)v * K64 + j], nw);
+                        any = true;
+                    }
+                }
+                if (any) {
+                    const uint32_t bit = 1u << (v & 31);
+                    take = !(atomicOr(touched + (v >> 5), bit) & bit);
+                }
+            }
+            const unsigned bal = __ballot_sync(kFull, take);
+            if (bal) {
+                const int leader = __ffs(bal) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(tlen, __popc(bal));
+                base = __shfl_sync(kFull, base, leader);
+                if (take) tlist[base + __popc(bal & ((1u << lane) - 1u))] = v;
+            }
+        }
+    }
+}
+
+template <int K64>
+__global__ void msbfs_push_finalize(const int32_t *tlist, const int *tlen, int nsrc, uint64_t *seen, uint64_t *xacc,
+                                    uint64_t *next, uint32_t *touched, uint32_t *act_next, uint32_t *done,
+                                    int32_t *depth, int64_t n, int level, unsigned long long *found) {
+    const int nt = *tlen;
+    unsigned long long my_found = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+        const int32_t v = tlist[i];
+        atomicAnd(touched + (v >> 5), ~(1u << (v & 31)));
+        bool any = false, full = true;
+        uint64_t nw[K64];
+#pragma unroll
+        for (int j = 0; j < K64; j++) {
+            const uint64_t fm = full_mask<K64>(j, nsrc);
+            const uint64_t x = xacc[(size_t)v * K64 + j];
+            xacc[(size_t)v * K64 + j] = 0;
+            const uint64_t s = seen[(size_t)v * K64 + j];
+            nw[j] = x & ~s & fm;
+            any |= nw[j] != 0;
+            full &= ((s | nw[j]) & fm) == fm;
+            if (nw[j]) seen[(size_t)v * K64 + j] = s | nw[j];
+            next[(size_t)v * K64 + j] = nw[j];
+        }
+        if (any) {
+            atomicOr(act_next + (v >> 5), 1u << (v & 31));
+            my_found++;
+            if (depth) {
+#pragma unroll
+                for (int j = 0; j < K64; j++) {
+                    uint64_t x = nw[j];
+                    while (x) {
+                        const int b = __ffsll((long long)x) - 1;
+                        x &= x - 1;
+                        depth[(size_t)(j * 64 + b) * n + v] = level + 1;
+                    }
+                }
+            }
+        }
+        if (full) atomicOr(done + (v >> 5), 1u << (v & 31));
+    }
+    my_found = warp_sum(my_found);
+    if ((threadIdx.x & 31) == 0 && my_found) atomicAdd(found, my_found);
+}
+
 // ------------------------------------------------------------------ SSSP
 
 constexpr int kLongRow = 2048;
@@ -437,7 +567,9 @@ hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int n
     const int W = (int)((n + 31) / 32);
     const size_t nk = (size_t)n * K64;
     const size_t hk = (size_t)std::max(plan.n_hubs, 1) * K64;
-    HC_TRY(g->ws_batch.ensure(nk * 8 * 3 + (size_t)W * 4 * 3 + hk * 8 + (size_t)std::max(plan.n_hubs, 1) * 4 + 8192));
+    const size_t max_ptasks = (size_t)(g->M / kMsPushChunk) + (size_t)n + 64;
+    HC_TRY(g->ws_batch.ensure(nk * 8 * 4 + (size_t)W * 4 * 4 + hk * 8 + (size_t)std::max(plan.n_hubs, 1) * 4 +
+                              (size_t)n * 4 + max_ptasks * sizeof(int2) + 16384));
     char *p = g->ws_batch.as<char>();
     auto take = [&](size_t b) {
         char *r = p;
@@ -451,6 +583,14 @@ hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int n
     uint64_t *hub_acc = (uint64_t *)take(hk * 8);
     unsigned *hub_cnt = (unsigned *)take((size_t)std::max(plan.n_hubs, 1) * 4);
     unsigned long long *found = (unsigned long long *)take(64);
+    uint64_t *xacc = (uint64_t *)take(nk * 8);
+    uint32_t *touched = (uint32_t *)take((size_t)W * 4);
+    int32_t *tlist = (int32_t *)take((size_t)n * 4);
+    int2 *ptasks = (int2 *)take(max_ptasks * sizeof(int2));
+    int *pctr = (int *)take(64);  // [0] push tasks, [1] touched count
+    unsigned long long *fedges = (unsigned long long *)take(64);
+    HC_CUDA_TRY(cudaMemsetAsync(xacc, 0, nk * 8, g->stream));
+    HC_CUDA_TRY(cudaMemsetAsync(touched, 0, (size_t)W * 4, g->stream));
     HC_CUDA_TRY(cudaMemsetAsync(seen, 0, nk * 8, g->stream));
     HC_CUDA_TRY(cudaMemsetAsync(fr[0], 0, nk * 8, g->stream));  // the seed ORs into it
     HC_CUDA_TRY(cudaMemsetAsync(act[0], 0, (size_t)W * 4, g->stream));
@@ -466,10 +606,52 @@ hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int n
     volatile unsigned long long *hfound = g->pinned.as<unsigned long long>();
     int level = 0;
     double b = 0;
+    const bool trace = std::getenv("HC_TRACE") != nullptr;
     for (; level < max_levels; level++) {
         const int c = level & 1;
+        const auto t0 = std::chrono::steady_clock::now();
         HC_CUDA_TRY(cudaMemsetAsync(found, 0, 8, g->stream));
         HC_CUDA_TRY(cudaMemsetAsync(act[c ^ 1], 0, (size_t)W * 4, g->stream));
+        // Direction: push while the frontier's edges are below M / kPushAlpha.
+        HC_CUDA_TRY(cudaMemsetAsync(pctr, 0, 64, g->stream));
+        HC_CUDA_TRY(cudaMemsetAsync(fedges, 0, 8, g->stream));
+        {
+            msbfs_push_tasks<<<grid, kMsThreads, 0, g->stream>>>(g->index.as<int64_t>(), act[c], g->n_active, ptasks,
+                                                                 pctr, fedges);
+            ::hc::count_launch();
+        }
+        HC_CUDA_TRY(cudaMemcpyAsync((void *)hfound, fedges, 8, cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        const unsigned long long fe = *hfound;
+        constexpr double kPushAlpha = 10.0;
+        const bool push = (double)fe * kPushAlpha < (double)g->M;
+        if (push) {
+            {
+                msbfs_push<K64><<<grid, kMsThreads, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
+                                                                    ptasks, pctr, fr[c], seen, xacc, touched, tlist,
+                                                                    pctr + 1);
+                ::hc::count_launch();
+            }
+            {
+                msbfs_push_finalize<K64><<<grid, kMsThreads, 0, g->stream>>>(tlist, pctr + 1, nsrc, seen, xacc,
+                                                                             fr[c ^ 1], touched, act[c ^ 1], done,
+                                                                             depth, n, level, found);
+                ::hc::count_launch();
+            }
+            HC_CUDA_TRY(cudaGetLastError());
+            HC_CUDA_TRY(cudaMemcpyAsync((void *)hfound, found, 8, cudaMemcpyDeviceToHost, g->stream));
+            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            b += 16.0 * (double)fe / 8.0 + 4.0 * (double)fe;
+            if (trace)
+                std::fprintf(stderr, "[hc msbfs] L%-3d push fedges=%-11llu found=%-9llu %8.1f us\n", level, fe,
+                             (unsigned long long)*hfound,
+                             std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count());
+            if (*hfound == 0) {
+                level++;
+                break;
+            }
+            continue;
+        }
         if (plan.n_tasks > 0) {
             msbfs_hub<K64><<<grid, kMsThreads, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), plan, nsrc,
                                                                seen, fr[c], fr[c ^ 1], act[c], act[c ^ 1], done,
@@ -487,6 +669,10 @@ hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int n
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
         // Offsets + neighbours once per level, plus seen / frontier words per vertex.
         b += 8.0 * (n + 1) + 4.0 * g->M + 3.0 * 8.0 * K64 * (double)g->n_active;
+        if (trace)
+            std::fprintf(stderr, "[hc msbfs] L%-3d pull fedges=%-11llu found=%-9llu %8.1f us\n", level, fe,
+                         (unsigned long long)*hfound,
+                         std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count());
         if (*hfound == 0) {
             level++;
             break;
