@@ -362,158 +362,6 @@ __global__ void msbfs_push_finalize(const int32_t *tlist, const int *tlen, int n
     if ((threadIdx.x & 31) == 0 && my_found) atomicAdd(found, my_found);
 }
 
-// ------------------------------------------------------------------ SSSP
-
-constexpr int kLongRow = 2048;
-
-__global__ void mssp_init(int32_t n, int32_t *dist, uint32_t *act0, uint32_t *act1) {
-    const size_t total = (size_t)n * 32;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
-        dist[i] = kInfDist;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        act0[i] = 0;
-        act1[i] = 0;
-    }
-}
-
-__global__ void mssp_seed(int nsrc, const int32_t *src, int32_t *dist, uint32_t *act, int32_t *queue, int *qlen) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int q = 0;
-        for (int s = 0; s < nsrc; s++) {
-            const int32_t v = src[s];
-            dist[(size_t)v * 32 + s] = 0;
-            if (act[v] == 0) queue[q++] = v;
-            act[v] |= 1u << s;
-        }
-        *qlen = q;
-    }
-}
-
-// Relax edges [e0, e1) of row u for the sources in `m` (lane = source), four
-// edges in flight: all distance-row loads, then all atomicMins, then the
-// activity updates of the four target vertices by lanes 0..3.
-__device__ __forceinline__ void mssp_relax_range(const int32_t *nbr, const int32_t *w, int32_t *dist, uint32_t m,
-                                                 int32_t du, int64_t e0, int64_t e1, uint32_t *act_next,
-                                                 int32_t *qnext, int *qlen, unsigned long long &relaxed) {
-    const int lane = threadIdx.x & 31;
-    const bool on = (m >> lane) & 1u;
-    for (int64_t base = e0; base < e1; base += 32) {
-        const int64_t my = base + lane;
-        const int cnt = (int)((e1 - base) < 32 ? (e1 - base) : 32);
-        int32_t vv = 0, ww = 0;
-        if (my < e1) {
-            vv = nbr[my];
-            ww = w[my];
-        }
-        for (int j0 = 0; j0 < cnt; j0 += 4) {
-            int32_t v[4], nd[4], d[4], prev[4];
-            bool ok[4], imp[4];
-            unsigned bal[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int idx = j0 + k;
-                v[k] = __shfl_sync(kFull, vv, idx & 31);
-                nd[k] = du + __shfl_sync(kFull, ww, idx & 31);
-                ok[k] = on && idx < cnt;
-            }
-#pragma unroll
-            for (int k = 0; k < 4; k++) d[k] = ok[k] ? __ldcg(dist + (size_t)v[k] * 32 + lane) : kInfDist;
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                imp[k] = ok[k] && nd[k] < d[k];
-                prev[k] = imp[k] ? atomicMin(dist + (size_t)v[k] * 32 + lane, nd[k]) : 0;
-            }
-#pragma unroll
-            for (int k = 0; k < 4; k++) bal[k] = __ballot_sync(kFull, imp[k] && nd[k] < prev[k]);
-            const unsigned mybal = lane == 0 ? bal[0] : lane == 1 ? bal[1] : lane == 2 ? bal[2] : lane == 3 ? bal[3] : 0u;
-            const int32_t myv = lane == 0 ? v[0] : lane == 1 ? v[1] : lane == 2 ? v[2] : v[3];
-            bool app = false;
-            if (mybal) app = atomicOr(act_next + myv, mybal) == 0u;
-            const unsigned ap = __ballot_sync(kFull, app);
-            if (ap) {
-                int base_q = 0;
-                const int leader = __ffs(ap) - 1;
-                if (lane == leader) base_q = atomicAdd(qlen, __popc(ap));
-                base_q = __shfl_sync(kFull, base_q, leader);
-                if (app) qnext[base_q + __popc(ap & ((1u << lane) - 1u))] = myv;
-            }
-        }
-        relaxed += (unsigned long long)cnt * __popc(m);
-    }
-}
-
-__global__ void __launch_bounds__(256) mssp_epoch(const int64_t *index, const int32_t *nbr, const int32_t *w,
-                                                  int32_t *dist, const int32_t *qcur, int nq, const uint32_t *act_cur,
-                                                  uint32_t *act_next, int32_t *qnext, int *qnext_len, int2 *tasks,
-                                                  int *ntasks, unsigned long long *relaxed) {
-    const int lane = threadIdx.x & 31;
-    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    unsigned long long rel = 0;
-    for (int qi = gwarp; qi < nq; qi += nwarps) {
-        const int32_t u = qcur[qi];
-        const uint32_t m = act_cur[u];
-        const int64_t b = index[u], e = index[u + 1];
-        if (e - b > kLongRow) {
-            if (lane == 0) {
-                const int nc = (int)((e - b + kLongRow - 1) / kLongRow);
-                const int t0 = atomicAdd(ntasks, nc);
-                for (int c = 0; c < nc; c++) tasks[t0 + c] = make_int2(u, c);
-            }
-            continue;
-        }
-        const int32_t du = __ldcg(dist + (size_t)u * 32 + lane);
-        mssp_relax_range(nbr, w, dist, m, du, b, e, act_next, qnext, qnext_len, rel);
-    }
-    rel = warp_sum(rel);
-    if (lane == 0 && rel) atomicAdd(relaxed, rel);
-}
-
-__global__ void __launch_bounds__(256) mssp_tasks(const int64_t *index, const int32_t *nbr, const int32_t *w,
-                                                  int32_t *dist, const int2 *tasks, const int *ntasks,
-                                                  const uint32_t *act_cur, uint32_t *act_next, int32_t *qnext,
-                                                  int *qnext_len, unsigned long long *relaxed) {
-    const int lane = threadIdx.x & 31;
-    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const int nt = *ntasks;
-    unsigned long long rel = 0;
-    for (int t = gwarp; t < nt; t += nwarps) {
-        const int2 tk = tasks[t];
-        const int32_t u = tk.x;
-        const uint32_t m = act_cur[u];
-        const int64_t rb = index[u], re = index[u + 1];
-        const int64_t b = rb + (int64_t)tk.y * kLongRow;
-        const int64_t e = (re < b + kLongRow) ? re : b + kLongRow;
-        const int32_t du = __ldcg(dist + (size_t)u * 32 + lane);
-        mssp_relax_range(nbr, w, dist, m, du, b, e, act_next, qnext, qnext_len, rel);
-    }
-    rel = warp_sum(rel);
-    if (lane == 0 && rel) atomicAdd(relaxed, rel);
-}
-
-__global__ void mssp_clear(const int32_t *q, int nq, uint32_t *act) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) act[q[i]] = 0;
-}
-
-// dist[v][32] -> out[s][v] for the group's sources, 32x32 tiles through shared memory.
-__global__ void mssp_transpose(const int32_t *dist, int32_t n, int nsrc, int32_t *out) {
-    __shared__ int32_t tile[32][33];
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-    for (int64_t vb = (int64_t)blockIdx.x * 32; vb < n; vb += (int64_t)gridDim.x * 32) {
-        for (int r = ty; r < 32; r += 8) {
-            const int64_t v = vb + r;
-            tile[r][tx] = v < n ? dist[(size_t)v * 32 + tx] : 0;
-        }
-        __syncthreads();
-        for (int s = ty; s < nsrc; s += 8) {
-            const int64_t v = vb + tx;
-            if (v < n) out[(size_t)s * n + v] = tile[tx][s];
-        }
-        __syncthreads();
-    }
-}
-
 }  // namespace
 }  // namespace hc
 
@@ -740,96 +588,6 @@ extern "C" hc_status hc_bfs_batched(hc_graph *g, const int32_t *sources, int32_t
         stats->groups = groups;
         stats->bytes_model = bytes;
         stats->ms = ms;
-    }
-    return HC_OK;
-}
-
-extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_t num_sources, int32_t *dist_out,
-                                     const hc_batch_opts *opts, hc_batch_stats *stats) {
-    clear_error();
-    HC_TRY(activate(g));
-    if (!sources || num_sources < 1) return fail(HC_ERR_INVALID_ARG, "hc_sssp_batched: bad source list");
-    if (g->wtype != HC_W_I32) return fail(HC_ERR_UNSUPPORTED, "hc_sssp_batched: graph needs int32 edge weights");
-    hc_batch_opts o{};
-    if (opts) o = *opts;
-    if (stats) std::memset(stats, 0, sizeof(*stats));
-    std::vector<int32_t> src(num_sources);
-    HC_CUDA_TRY(cudaMemcpy(src.data(), sources, sizeof(int32_t) * num_sources, cudaMemcpyDefault));
-    for (int32_t s : src)
-        if (s < 0 || s >= g->N) return fail(HC_ERR_INVALID_ARG, "hc_sssp_batched: source %d out of range", s);
-    const int64_t n = g->N;
-    const int64_t max_tasks = 2 * (g->M / kLongRow) + n / kLongRow + 64;
-    HC_TRY(g->ws_batch.ensure((size_t)n * 32 * 4 + (size_t)n * 4 * 4 + sizeof(int2) * max_tasks + 8192));
-    char *p = g->ws_batch.as<char>();
-    auto take = [&](size_t b) {
-        char *r = p;
-        p += (b + 255) / 256 * 256;
-        return r;
-    };
-    int32_t *dist = (int32_t *)take((size_t)n * 32 * 4);
-    uint32_t *act[2] = {(uint32_t *)take((size_t)n * 4), (uint32_t *)take((size_t)n * 4)};
-    int32_t *q[2] = {(int32_t *)take((size_t)n * 4), (int32_t *)take((size_t)n * 4)};
-    int2 *tasks = (int2 *)take(sizeof(int2) * max_tasks);
-    int *ctr = (int *)take(256);  // [0],[1] queue lengths, [2] tasks
-    unsigned long long *relaxed = (unsigned long long *)take(64);
-    int32_t *d_src = (int32_t *)take(sizeof(int32_t) * 32);
-    const bool dev_out = is_device_pointer(dist_out);
-    if (dist_out && !dev_out) HC_TRY(g->ws_out0.ensure(sizeof(int32_t) * (size_t)32 * n));
-    const int grid = g->sm_count * 8;
-    const int max_epochs = o.max_epochs > 0 ? o.max_epochs : 0x7fffffff;
-    HC_TRY(g->pinned.ensure(64));
-    volatile int *hq = g->pinned.as<int>();
-    HC_CUDA_TRY(cudaMemsetAsync(relaxed, 0, 8, g->stream));
-    HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
-    int epochs_max = 0, groups = 0;
-    for (int s0 = 0; s0 < num_sources; s0 += 32, groups++) {
-        const int k = std::min(32, num_sources - s0);
-        HC_CUDA_TRY(cudaMemcpyAsync(d_src, src.data() + s0, sizeof(int32_t) * k, cudaMemcpyHostToDevice, g->stream));
-        { mssp_init<<<grid, 256, 0, g->stream>>>(g->N, dist, act[0], act[1]); ::hc::count_launch(); }
-        { mssp_seed<<<1, 32, 0, g->stream>>>(k, d_src, dist, act[0], q[0], &ctr[0]); ::hc::count_launch(); }
-        HC_CUDA_TRY(cudaGetLastError());
-        HC_CUDA_TRY(cudaMemcpyAsync((void *)hq, &ctr[0], 4, cudaMemcpyDeviceToHost, g->stream));
-        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        int nq = *hq;
-        int ep = 0;
-        for (; nq > 0; ep++) {
-            if (ep >= max_epochs) return fail(HC_ERR_NOT_CONVERGED, "hc_sssp_batched: epoch cap reached");
-            const int c = ep & 1;
-            HC_CUDA_TRY(cudaMemsetAsync(&ctr[c ^ 1], 0, 4, g->stream));
-            HC_CUDA_TRY(cudaMemsetAsync(&ctr[2], 0, 4, g->stream));
-            { mssp_epoch<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->wgt.as<int32_t>(),
-                                                    dist, q[c], nq, act[c], act[c ^ 1], q[c ^ 1], &ctr[c ^ 1], tasks,
-                                                    &ctr[2], relaxed); ::hc::count_launch(); }
-            { mssp_tasks<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->wgt.as<int32_t>(),
-                                                    dist, tasks, &ctr[2], act[c], act[c ^ 1], q[c ^ 1], &ctr[c ^ 1],
-                                                    relaxed); ::hc::count_launch(); }
-            { mssp_clear<<<(nq + 255) / 256, 256, 0, g->stream>>>(q[c], nq, act[c]); ::hc::count_launch(); }
-            HC_CUDA_TRY(cudaGetLastError());
-            HC_CUDA_TRY(cudaMemcpyAsync((void *)hq, &ctr[c ^ 1], 4, cudaMemcpyDeviceToHost, g->stream));
-            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-            nq = *hq;
-        }
-        epochs_max = std::max(epochs_max, ep);
-        if (dist_out) {
-            int32_t *dst = dev_out ? dist_out + (size_t)s0 * n : g->ws_out0.as<int32_t>();
-            { mssp_transpose<<<grid, 256, 0, g->stream>>>(dist, g->N, k, dst); ::hc::count_launch(); }
-            HC_CUDA_TRY(cudaGetLastError());
-            if (!dev_out) HC_TRY(copy_out(dist_out + (size_t)s0 * n, dst, sizeof(int32_t) * (size_t)k * n, g->stream));
-        }
-    }
-    HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
-    HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    float ms = 0;
-    HC_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_start, g->ev_stop));
-    unsigned long long rel = 0;
-    HC_CUDA_TRY(cudaMemcpy(&rel, relaxed, 8, cudaMemcpyDeviceToHost));
-    if (stats) {
-        stats->epochs = epochs_max;
-        stats->groups = groups;
-        stats->ms = ms;
-        // 8 B (neighbour + weight) per edge visit of a row, amortised over the
-        // group's lanes, plus a 128-byte distance row per relaxed edge visit.
-        stats->bytes_model = (double)rel / 32.0 * (8.0 + 128.0);
     }
     return HC_OK;
 }
