@@ -1,4 +1,4 @@
-// Batched multi-source BFS and SSSP.
+// Batched multi-source BFS (batched SSSP lives in hc_batched_sssp.cu).
 //
 // The reference runs sources one after another, each a full driver call
 // (src/benchmarks/gpu_benchmark.cuh:577-586).  Here a group of sources shares
@@ -17,13 +17,6 @@
 //   - rows longer than kMsHub edges are cut into kMsTask-edge tasks whose
 //     warps OR their partial words into a per-row accumulator; the last task
 //     of a row (per-row counter) applies the update.
-//
-// SSSP: distances vertex-major dist[v][32] (one lane per source, 128-byte
-// rows), an activity mask per vertex (bit s = distance for source s dropped
-// last epoch) and a queue of active vertices.  An epoch relaxes every edge out
-// of the queue for the sources whose bit is set; a warp keeps four edges in
-// flight (row loads, then atomicMins, then activity updates).  Rows longer
-// than kLongRow are cut into chunks processed by a second launch.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>

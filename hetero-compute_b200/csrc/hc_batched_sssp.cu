@@ -10,10 +10,18 @@
 // drive the epochs: every edge out of the queue is relaxed for the active
 // lanes, a warp keeping four edges in flight (row loads, then atomicMins, then
 // the activity updates of the four targets).  Rows longer than kLongRow are
-// cut into chunks processed by a second launch.  Wider groups amortise the row
-// reads over more sources; the frontiers of Kronecker sources overlap, so the
-// union frontier grows more slowly than the group.
+// cut into chunks processed by a second launch.  While the queue covers a
+// large part of the graph (and weights are symmetric) an epoch is a pull
+// instead: a warp per row takes the minimum over its active neighbours and
+// writes the row once, so the hub rows that most edges point at are read, not
+// hammered with atomics.  Wider groups amortise the row reads over more
+// sources; the frontiers of Kronecker sources overlap, so the union frontier
+// grows more slowly than the group.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "hc_graph.cuh"
@@ -22,6 +30,8 @@ namespace hc {
 namespace {
 
 constexpr int kLongRow = 2048;
+// Pull epochs run while the queue holds more than n_active / kPullDiv vertices.
+constexpr int kPullDiv = 8;
 
 template <int SPL>
 __device__ __forceinline__ void load_row(const int32_t *p, int32_t (&d)[SPL]) {
@@ -32,11 +42,14 @@ __device__ __forceinline__ void load_row(const int32_t *p, int32_t (&d)[SPL]) {
         d[0] = x.x;
         d[1] = x.y;
     } else {
-        const int4 x = __ldcg(reinterpret_cast<const int4 *>(p));
-        d[0] = x.x;
-        d[1] = x.y;
-        d[2] = x.z;
-        d[3] = x.w;
+#pragma unroll
+        for (int h = 0; h < SPL / 4; h++) {
+            const int4 x = __ldcg(reinterpret_cast<const int4 *>(p) + h);
+            d[4 * h] = x.x;
+            d[4 * h + 1] = x.y;
+            d[4 * h + 2] = x.z;
+            d[4 * h + 3] = x.w;
+        }
     }
 }
 
@@ -101,14 +114,20 @@ __device__ __forceinline__ void relax_range(const int32_t *nbr, const int32_t *w
                     for (int s = 0; s < SPL; s++) d[k][s] = kInfDist;
                 }
             }
+            // The update is a fire-and-forget atomicMin; the target is marked
+            // active whenever the loaded value was larger, which covers every
+            // real improvement (values only fall between the load and the
+            // atomic) at the price of an occasional redundant rescan.
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 imp[k] = false;
 #pragma unroll
                 for (int s = 0; s < SPL; s++) {
                     const int32_t nd = du[s] == kInfDist ? kInfDist : du[s] + wt[k];
-                    if (ok[k] && nd < d[k][s] && nd < atomicMin(dist + (size_t)v[k] * K + lane * SPL + s, nd))
+                    if (ok[k] && nd < d[k][s]) {
+                        atomicMin(dist + (size_t)v[k] * K + lane * SPL + s, nd);
                         imp[k] = true;
+                    }
                 }
             }
             unsigned bal[4];
@@ -127,7 +146,7 @@ __device__ __forceinline__ void relax_range(const int32_t *nbr, const int32_t *w
                 if (app) qnext[base_q + __popc(ap & ((1u << lane) - 1u))] = myv;
             }
         }
-        relaxed += (unsigned long long)cnt * __popc(m) * SPL;
+        if (lane == 0) relaxed += (unsigned long long)cnt * __popc(m) * SPL;
     }
 }
 
@@ -185,6 +204,153 @@ __global__ void __launch_bounds__(256) mssp_tasks(const int64_t *index, const in
     if (lane == 0 && rel) atomicAdd(relaxed, rel);
 }
 
+// Pull epoch, used while the queue covers a large part of the graph (weights
+// symmetric, so w(u->v) is read from v's row).  Items [0, n_rows) are rows of
+// at most kLongRow edges, one warp each, the only writer of that row; items
+// past n_rows are kLongRow-edge chunks of the longer rows, which merge with
+// atomicMin.  A warp takes the minimum over the neighbours whose activity
+// mask has its lane's bit, four neighbours in flight, and writes the row and
+// its activity mask once.
+template <int SPL>
+__global__ void __launch_bounds__(256) mssp_pull(const int64_t *index, const int32_t *nbr, const int32_t *w,
+                                                 int32_t *dist, int32_t n_rows, const int2 *tasks, int ntasks,
+                                                 const uint32_t *act_cur, uint32_t *act_next,
+                                                 unsigned long long *relaxed) {
+    constexpr int K = 32 * SPL;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long rel = 0;
+    const int64_t total = (int64_t)n_rows + ntasks;
+    for (int64_t it = gwarp; it < total; it += nwarps) {
+        int32_t v;
+        int64_t b, e;
+        bool chunk;
+        if (it < n_rows) {
+            v = (int32_t)it;
+            b = index[v];
+            e = index[v + 1];
+            if (e == b || e - b > kLongRow) continue;
+            chunk = false;
+        } else {
+            const int2 tk = tasks[it - n_rows];
+            v = tk.x;
+            const int64_t re = index[v + 1];
+            b = index[v] + (int64_t)tk.y * kLongRow;
+            e = (re < b + kLongRow) ? re : b + kLongRow;
+            chunk = true;
+        }
+        int32_t *row = dist + (size_t)v * K + lane * SPL;
+        int32_t dv[SPL], best[SPL];
+        load_row<SPL>(row, dv);
+#pragma unroll
+        for (int s = 0; s < SPL; s++) best[s] = dv[s];
+        for (int64_t base = b; base < e; base += 32) {
+            const int64_t my = base + lane;
+            int32_t uu = 0, ww = 0;
+            uint32_t aa = 0;
+            if (my < e) {
+                uu = nbr[my];
+                ww = w[my];
+                aa = __ldcg(act_cur + uu);
+            }
+            rel += (unsigned long long)__popc(aa) * SPL;
+            unsigned live = __ballot_sync(kFull, aa != 0u);
+            while (live) {
+                int32_t u[4], wt[4], d[4][SPL];
+                bool on[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const bool have = live != 0u;
+                    const int idx = have ? __ffs(live) - 1 : 0;
+                    if (have) live &= live - 1u;
+                    u[k] = __shfl_sync(kFull, uu, idx);
+                    wt[k] = __shfl_sync(kFull, ww, idx);
+                    const uint32_t a = __shfl_sync(kFull, aa, idx);
+                    on[k] = have && ((a >> lane) & 1u);
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (on[k]) {
+                        load_row<SPL>(dist + (size_t)u[k] * K + lane * SPL, d[k]);
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < SPL; s++) d[k][s] = kInfDist;
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+#pragma unroll
+                    for (int s = 0; s < SPL; s++)
+                        if (d[k][s] != kInfDist && d[k][s] + wt[k] < best[s]) best[s] = d[k][s] + wt[k];
+                }
+            }
+        }
+        bool imp = false;
+#pragma unroll
+        for (int s = 0; s < SPL; s++) imp |= best[s] < dv[s];
+        const unsigned bal = __ballot_sync(kFull, imp);
+        if (!bal) continue;
+        if (chunk) {
+#pragma unroll
+            for (int s = 0; s < SPL; s++)
+                if (best[s] < dv[s]) atomicMin(row + s, best[s]);
+            if (lane == 0) atomicOr(act_next + v, bal);
+        } else {
+            if (imp) {
+#pragma unroll
+                for (int s = 0; s < SPL; s++) row[s] = best[s];
+            }
+            if (lane == 0) act_next[v] = bal;
+        }
+    }
+    rel = warp_sum(rel);
+    if (lane == 0 && rel) atomicAdd(relaxed, rel);
+}
+
+// Queue of the vertices with a non-zero activity mask, in vertex order.
+__global__ void mssp_compact(const uint32_t *act, int32_t n, int32_t *q, int *qlen) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) {
+        const int64_t v = base + lane;
+        const bool on = v < n && act[v] != 0u;
+        const unsigned bal = __ballot_sync(kFull, on);
+        if (!bal) continue;
+        int q0 = 0;
+        if (lane == 0) q0 = atomicAdd(qlen, __popc(bal));
+        q0 = __shfl_sync(kFull, q0, 0);
+        if (on) q[q0 + __popc(bal & ((1u << lane) - 1u))] = (int32_t)v;
+    }
+}
+
+// (row, chunk) tasks for the rows longer than kLongRow.
+__global__ void mssp_plan(const int64_t *index, int32_t n, int2 *tasks, int *ntasks) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t deg = index[v + 1] - index[v];
+        if (deg <= kLongRow) continue;
+        const int nc = (int)((deg + kLongRow - 1) / kLongRow);
+        const int t0 = atomicAdd(ntasks, nc);
+        for (int c = 0; c < nc; c++) tasks[t0 + c] = make_int2((int32_t)v, c);
+    }
+}
+
+hc_status ensure_pull_plan(hc_graph *g) {
+    if (g->mssp_tasks >= 0) return HC_OK;
+    const int64_t max_tasks = 2 * (g->M / kLongRow) + 1;
+    HC_TRY(g->ws_plan_mssp.ensure(sizeof(int2) * max_tasks + 256));
+    int *cnt = reinterpret_cast<int *>(g->ws_plan_mssp.as<char>() + sizeof(int2) * max_tasks);
+    HC_CUDA_TRY(cudaMemsetAsync(cnt, 0, 4, g->stream));
+    { mssp_plan<<<g->sm_count * 8, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->N, g->ws_plan_mssp.as<int2>(), cnt); ::hc::count_launch(); }
+    HC_CUDA_TRY(cudaGetLastError());
+    int h = 0;
+    HC_CUDA_TRY(cudaMemcpyAsync(&h, cnt, 4, cudaMemcpyDeviceToHost, g->stream));
+    HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    g->mssp_tasks = h;
+    return HC_OK;
+}
+
 __global__ void mssp_clear(const int32_t *q, int nq, uint32_t *act) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) act[q[i]] = 0;
 }
@@ -211,8 +377,8 @@ __global__ void mssp_transpose(const int32_t *dist, int32_t n, int nsrc, int32_t
 }
 
 template <int SPL>
-hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int max_epochs, int *epochs_out,
-                    unsigned long long *relaxed) {
+hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int max_epochs, int pull_div,
+                    int *epochs_out, unsigned long long *relaxed) {
     constexpr int K = 32 * SPL;
     const int64_t n = g->N;
     const int64_t max_tasks = 2 * (g->M / kLongRow) + n / kLongRow + 64;
@@ -228,7 +394,7 @@ hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int 
     int32_t *q[2] = {(int32_t *)take((size_t)n * 4), (int32_t *)take((size_t)n * 4)};
     int2 *tasks = (int2 *)take(sizeof(int2) * max_tasks);
     int *ctr = (int *)take(256);  // [0],[1] queue lengths, [2] tasks
-    int32_t *d_src = (int32_t *)take(sizeof(int32_t) * 128);
+    int32_t *d_src = (int32_t *)take(sizeof(int32_t) * K);
     const int grid = g->sm_count * 8;
     HC_TRY(g->pinned.ensure(64));
     volatile int *hq = g->pinned.as<int>();
@@ -240,11 +406,26 @@ hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int 
     HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
     int nq = *hq;
     int ep = 0;
+    const bool trace = std::getenv("HC_TRACE") != nullptr;
     for (; nq > 0; ep++) {
+        const auto t0 = std::chrono::steady_clock::now();
         if (ep >= max_epochs) return fail(HC_ERR_NOT_CONVERGED, "hc_sssp_batched: epoch cap reached");
         const int c = ep & 1;
         HC_CUDA_TRY(cudaMemsetAsync(&ctr[c ^ 1], 0, 4, g->stream));
         HC_CUDA_TRY(cudaMemsetAsync(&ctr[2], 0, 4, g->stream));
+        // Pull while the queue holds more than n_active / pull_div vertices.
+        const bool pull = pull_div > 0 && (int64_t)nq * pull_div > g->n_active;
+        if (pull) {
+            {
+                mssp_pull<SPL><<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
+                                                            g->wgt.as<int32_t>(), dist, g->n_active,
+                                                            g->ws_plan_mssp.as<int2>(), g->mssp_tasks, act[c],
+                                                            act[c ^ 1], relaxed);
+                ::hc::count_launch();
+            }
+            { mssp_clear<<<(nq + 255) / 256, 256, 0, g->stream>>>(q[c], nq, act[c]); ::hc::count_launch(); }
+            { mssp_compact<<<grid, 256, 0, g->stream>>>(act[c ^ 1], g->N, q[c ^ 1], &ctr[c ^ 1]); ::hc::count_launch(); }
+        } else {
         {
             mssp_epoch<SPL><<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
                                                          g->wgt.as<int32_t>(), dist, q[c], nq, act[c], act[c ^ 1],
@@ -258,9 +439,18 @@ hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int 
             ::hc::count_launch();
         }
         { mssp_clear<<<(nq + 255) / 256, 256, 0, g->stream>>>(q[c], nq, act[c]); ::hc::count_launch(); }
+        }
         HC_CUDA_TRY(cudaGetLastError());
         HC_CUDA_TRY(cudaMemcpyAsync((void *)hq, &ctr[c ^ 1], 4, cudaMemcpyDeviceToHost, g->stream));
+        if (trace) HC_CUDA_TRY(cudaMemcpyAsync((void *)(hq + 2), relaxed, 8, cudaMemcpyDeviceToHost, g->stream));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (trace) {
+            const double us = std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+            unsigned long long r = 0;
+            std::memcpy(&r, (const void *)(hq + 2), 8);
+            std::fprintf(stderr, "mssp K=%d epoch %d %s queue %d next %d relaxed(total) %llu  %.1f us\n", K, ep,
+                         pull ? "pull" : "push", nq, *hq, r, us);
+        }
         nq = *hq;
     }
     *epochs_out = ep;
@@ -289,8 +479,26 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
     HC_CUDA_TRY(cudaMemcpy(src.data(), sources, sizeof(int32_t) * num_sources, cudaMemcpyDefault));
     for (int32_t s : src)
         if (s < 0 || s >= g->N) return fail(HC_ERR_INVALID_ARG, "hc_sssp_batched: source %d out of range", s);
-    // Group width: 32, 64 or 128 sources (0 = the default 128).
-    const int group = o.group <= 0 ? 128 : (o.group <= 32 ? 32 : (o.group <= 64 ? 64 : 128));
+    // Group width: 32, 64, 128 or 256 sources.  The default is the widest
+    // whose distance matrix (N x width x 4 bytes) takes at most 40% of the
+    // free device memory, 80% with the staging buffer of host outputs (wider
+    // groups share each row read among more sources).
+    int group = o.group <= 32 ? 32 : o.group <= 64 ? 64 : o.group <= 128 ? 128 : 256;
+    if (o.group <= 0) {
+        size_t free_b = 0, total_b = 0;
+        HC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        free_b += g->ws_batch.bytes + g->ws_out0.bytes;  // workspaces are reused
+        // Host outputs also stage each group's rows in a device buffer.
+        const double copies = (dist_out && !is_device_pointer(dist_out)) ? 2.0 : 1.0;
+        group = 256;
+        while (group > 32 && (double)g->N * group * 4.0 * copies > 0.4 * copies * (double)free_b) group /= 2;
+    }
+    // Weights must be non-negative; pull epochs need symmetric weights.
+    HC_TRY(ensure_weight_stats(g));
+    if (g->w_negative) return fail(HC_ERR_INVALID_ARG, "hc_sssp_batched: negative edge weight");
+    int pull_div = g->w_symmetric ? kPullDiv : 0;
+    if (const char *e = std::getenv("HC_MSSP_PULL_DIV")) pull_div = g->w_symmetric ? std::atoi(e) : 0;
+    if (pull_div > 0) HC_TRY(ensure_pull_plan(g));
     const int64_t n = g->N;
     const bool dev_out = is_device_pointer(dist_out);
     if (dist_out && !dev_out) HC_TRY(g->ws_out0.ensure(sizeof(int32_t) * (size_t)group * n));
@@ -305,9 +513,10 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
         int32_t *dst = nullptr;
         if (dist_out) dst = dev_out ? dist_out + (size_t)s0 * n : g->ws_out0.as<int32_t>();
         int ep = 0;
-        if (group == 32) HC_TRY(run_group<1>(g, src.data() + s0, k, dst, max_epochs, &ep, relaxed));
-        else if (group == 64) HC_TRY(run_group<2>(g, src.data() + s0, k, dst, max_epochs, &ep, relaxed));
-        else HC_TRY(run_group<4>(g, src.data() + s0, k, dst, max_epochs, &ep, relaxed));
+        if (group == 32) HC_TRY(run_group<1>(g, src.data() + s0, k, dst, max_epochs, pull_div, &ep, relaxed));
+        else if (group == 64) HC_TRY(run_group<2>(g, src.data() + s0, k, dst, max_epochs, pull_div, &ep, relaxed));
+        else if (group == 128) HC_TRY(run_group<4>(g, src.data() + s0, k, dst, max_epochs, pull_div, &ep, relaxed));
+        else HC_TRY(run_group<8>(g, src.data() + s0, k, dst, max_epochs, pull_div, &ep, relaxed));
         if (dist_out && !dev_out)
             HC_TRY(copy_out(dist_out + (size_t)s0 * n, dst, sizeof(int32_t) * (size_t)k * n, g->stream));
         epochs_max = std::max(epochs_max, ep);

@@ -73,6 +73,9 @@ struct hc_graph {
     // batched-BFS hub plan (rows above its split threshold, (row, chunk) tasks)
     hc::DevBuf ws_plan_ms;
     int32_t ms_hubs = -1, ms_tasks = 0;
+    // batched-SSSP pull plan: (row, chunk) tasks of the rows above its chunk size
+    hc::DevBuf ws_plan_mssp;
+    int32_t mssp_tasks = -1;
 
     // workspaces
     hc::DevBuf ws_bfs, ws_sssp, ws_pr, ws_batch, ws_out0, ws_out1, ws_ctl, ws_src;
@@ -89,4 +92,6 @@ hc_status activate(hc_graph *g);
 hc_status ensure_pr_derived(hc_graph *g, bool weighted);
 // Builds the row plan if missing (g->pr_view, g->pr_partial_slots).
 hc_status ensure_plan(hc_graph *g);
+// Computes w_negative, w_mean and w_symmetric once (int32 weights).
+hc_status ensure_weight_stats(hc_graph *g);
 }  // namespace hc

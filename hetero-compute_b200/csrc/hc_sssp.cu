@@ -468,6 +468,8 @@ hc_status launch_sssp(hc_graph *g, const SsspArgs &args) {
     return HC_OK;
 }
 
+}  // namespace
+
 hc_status ensure_weight_stats(hc_graph *g) {
     if (g->wstats_done) return HC_OK;
     DevBuf buf;
@@ -494,7 +496,6 @@ hc_status ensure_weight_stats(hc_graph *g) {
     return HC_OK;
 }
 
-}  // namespace
 }  // namespace hc
 
 using namespace hc;

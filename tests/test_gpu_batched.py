@@ -48,6 +48,44 @@ def test_sssp_batched_distances(scale, k):
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s)), i
 
 
+@pytest.mark.parametrize("group", [32, 64, 128, 256])
+def test_sssp_batched_group_widths(group):
+    host = hc.gen_kronecker(11, 16, 42, wtype=hc.W_I32)
+    g = hc.Graph.from_host(host)
+    src = np.concatenate([hc.pick_sources(host, 150), hc.pick_sources(host, 3)])  # ragged last group, duplicates
+    dist, st = g.sssp_batched(src, group=group)
+    assert st.groups == -(-len(src) // group)
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s)), i
+    torch = pytest.importorskip("torch")
+    dd = torch.empty((len(src), host.num_nodes), dtype=torch.int32, device="cuda")
+    g.sssp_batched(src, dd, group=group)
+    assert np.array_equal(dd.cpu().numpy(), dist)
+
+
+@pytest.mark.parametrize("pull_div", ["0", "8", "1000000"])
+def test_sssp_batched_push_and_pull_epochs(monkeypatch, pull_div):
+    """Push only, the default switch, and pull for every epoch."""
+    monkeypatch.setenv("HC_MSSP_PULL_DIV", pull_div)
+    big = hc.gen_kronecker(16, 16, 3, wtype=hc.W_I32)  # rows above the chunk size
+    g = hc.Graph.from_host(big)
+    src = hc.pick_sources(big, 70)
+    dist, _ = g.sssp_batched(src, group=64)
+    for i in range(0, 70, 9):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(big.index, big.neighbors, big.weights, src[i])), i
+
+
+def test_sssp_batched_asymmetric_weights():
+    """w(u->v) != w(v->u): epochs stay push, weights read from u's row."""
+    host = hc.gen_kronecker(12, 8, 3)
+    w = np.random.default_rng(0).integers(1, 256, size=host.num_edges).astype(np.int32)
+    g = hc.Graph(host.index, host.neighbors, w)
+    src = hc.pick_sources(host, 40)
+    dist, _ = g.sssp_batched(src)
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, w, s)), i
+
+
 def test_sssp_batched_grid_and_hubs():
     host = hc.gen_grid(60, 70, 2, wtype=hc.W_I32)
     g = hc.Graph.from_host(host)
