@@ -40,6 +40,33 @@ struct MsPlan {
     int n_hubs, n_tasks;
 };
 
+// Level control in device memory.  The kernels of a level read the level
+// number and the push/pull choice from here, so the same launch sequence runs
+// from the host loop and as the body of a graph's while node, whose condition
+// msbfs_end sets.
+struct MsCtl {
+    unsigned long long found;   // vertices that gained a frontier bit this level
+    unsigned long long fedges;  // edges out of the current frontier
+    int ptasks;                 // push tasks queued
+    int tlen;                   // touched vertices (push)
+    int level;
+    int fin;                    // a level found nothing: the traversal is over
+    int stop;                   // ended early; status says why
+    int status;
+    int max_levels;
+    int pad;
+    long long m;
+    double bytes;               // bytes model, summed over levels
+    unsigned long long t0;
+};
+// Push while the frontier's edges times kMsPushAlpha stay below M.
+constexpr double kMsPushAlpha = 10.0;
+// Wall-clock bound of one group's level loop (checked between levels).
+constexpr unsigned long long kMsLimitNs = 60ull * 1000000000ull;
+
+__device__ __forceinline__ bool ms_live(const MsCtl *c) { return !c->stop && !c->fin; }
+__device__ __forceinline__ bool ms_push(const MsCtl *c) { return (double)c->fedges * kMsPushAlpha < (double)c->m; }
+
 template <int K64>
 __device__ __forceinline__ uint64_t full_mask(int word, int nsrc) {
     const int bits = min(64, max(0, nsrc - word * 64));
@@ -90,8 +117,10 @@ template <int K64>
 __global__ void __launch_bounds__(kMsThreads) msbfs_pull(const int64_t *index, const int32_t *nbr, int32_t n_active,
                                                          int nsrc, uint64_t *seen, const uint64_t *front,
                                                          uint64_t *next, const uint32_t *act, uint32_t *act_next,
-                                                         uint32_t *done, int32_t *depth, int64_t n, int level,
-                                                         unsigned long long *found) {
+                                                         uint32_t *done, int32_t *depth, int64_t n, MsCtl *ctl) {
+    if (!ms_live(ctl) || ms_push(ctl)) return;
+    const int level = ctl->level;
+    unsigned long long *found = &ctl->found;
     const int lane = threadIdx.x & 31;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -164,8 +193,10 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_hub(const int64_t *index, co
                                                         int nsrc, uint64_t *seen, const uint64_t *front,
                                                         uint64_t *next, const uint32_t *act, uint32_t *act_next,
                                                         uint32_t *done, uint64_t *hub_acc, unsigned *hub_cnt,
-                                                        int32_t *depth, int64_t n, int level,
-                                                        unsigned long long *found) {
+                                                        int32_t *depth, int64_t n, MsCtl *ctl) {
+    if (!ms_live(ctl) || ms_push(ctl)) return;
+    const int level = ctl->level;
+    unsigned long long *found = &ctl->found;
     const int lane = threadIdx.x & 31;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -235,7 +266,10 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_hub(const int64_t *index, co
 constexpr int kMsPushChunk = 2048;
 
 __global__ void msbfs_push_tasks(const int64_t *index, const uint32_t *act, int32_t n_active, int2 *tasks,
-                                 int *ntasks, unsigned long long *fedges) {
+                                 MsCtl *ctl) {
+    if (!ms_live(ctl)) return;
+    int *ntasks = &ctl->ptasks;
+    unsigned long long *fedges = &ctl->fedges;
     const int lane = threadIdx.x & 31;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -263,13 +297,14 @@ __global__ void msbfs_push_tasks(const int64_t *index, const uint32_t *act, int3
 
 template <int K64>
 __global__ void __launch_bounds__(kMsThreads) msbfs_push(const int64_t *index, const int32_t *nbr, const int2 *tasks,
-                                                         const int *ntasks, const uint64_t *front,
-                                                         const uint64_t *seen, uint64_t *xacc, uint32_t *touched,
-                                                         int32_t *tlist, int *tlen) {
+                                                         const uint64_t *front, const uint64_t *seen, uint64_t *xacc,
+                                                         uint32_t *touched, int32_t *tlist, MsCtl *ctl) {
+    if (!ms_live(ctl) || !ms_push(ctl)) return;
+    int *tlen = &ctl->tlen;
     const int lane = threadIdx.x & 31;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const int nt = *ntasks;
+    const int nt = ctl->ptasks;
     for (int t = gwarp; t < nt; t += nwarps) {
         const int2 tk = tasks[t];
         const int32_t u = tk.x;
@@ -312,10 +347,13 @@ __global__ void __launch_bounds__(kMsThreads) msbfs_push(const int64_t *index, c
 }
 
 template <int K64>
-__global__ void msbfs_push_finalize(const int32_t *tlist, const int *tlen, int nsrc, uint64_t *seen, uint64_t *xacc,
-                                    uint64_t *next, uint32_t *touched, uint32_t *act_next, uint32_t *done,
-                                    int32_t *depth, int64_t n, int level, unsigned long long *found) {
-    const int nt = *tlen;
+__global__ void msbfs_push_finalize(const int32_t *tlist, int nsrc, uint64_t *seen, uint64_t *xacc, uint64_t *next,
+                                    uint32_t *touched, uint32_t *act_next, uint32_t *done, int32_t *depth, int64_t n,
+                                    MsCtl *ctl) {
+    if (!ms_live(ctl) || !ms_push(ctl)) return;
+    const int nt = ctl->tlen;
+    const int level = ctl->level;
+    unsigned long long *found = &ctl->found;
     unsigned long long my_found = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
         const int32_t v = tlist[i];
@@ -353,6 +391,53 @@ __global__ void msbfs_push_finalize(const int32_t *tlist, const int *tlen, int n
     }
     my_found = warp_sum(my_found);
     if ((threadIdx.x & 31) == 0 && my_found) atomicAdd(found, my_found);
+}
+
+__global__ void msbfs_ctl_init(MsCtl *ctl, int max_levels, long long m) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        MsCtl c{};
+        c.max_levels = max_levels;
+        c.m = m;
+        c.t0 = globaltimer_ns();
+        *ctl = c;
+    }
+}
+
+// Opens a level: clears the next activity bitmap and the level's counters.
+__global__ void msbfs_begin(MsCtl *ctl, uint32_t *act_next, int words) {
+    if (!ms_live(ctl)) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) act_next[i] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->found = 0;
+        ctl->fedges = 0;
+        ctl->ptasks = 0;
+        ctl->tlen = 0;
+    }
+}
+
+// Closes a level: adds its bytes to the model, counts it, and decides whether
+// another level runs (something found, under the level cap and the time
+// bound); inside a graph it sets the while node's condition.
+__global__ void msbfs_end(MsCtl *ctl, double pull_bytes, cudaGraphConditionalHandle cond, int use_cond) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    bool go = false;
+    if (ms_live(ctl)) {
+        const double fe = (double)ctl->fedges;
+        ctl->bytes += ms_push(ctl) ? 16.0 * fe / 8.0 + 4.0 * fe : pull_bytes;
+        ctl->level++;
+        if (ctl->found == 0) {
+            ctl->fin = 1;
+        } else if (ctl->level >= ctl->max_levels) {
+            ctl->stop = 1;
+            ctl->status = HC_ERR_NOT_CONVERGED;
+        } else if (globaltimer_ns() - ctl->t0 > kMsLimitNs) {
+            ctl->stop = 1;
+            ctl->status = HC_ERR_TIMEOUT;
+        } else {
+            go = true;
+        }
+    }
+    if (use_cond) cudaGraphSetConditional(cond, go ? 1u : 0u);
 }
 
 }  // namespace
@@ -423,13 +508,11 @@ hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int n
     uint32_t *done = (uint32_t *)take((size_t)W * 4);
     uint64_t *hub_acc = (uint64_t *)take(hk * 8);
     unsigned *hub_cnt = (unsigned *)take((size_t)std::max(plan.n_hubs, 1) * 4);
-    unsigned long long *found = (unsigned long long *)take(64);
     uint64_t *xacc = (uint64_t *)take(nk * 8);
     uint32_t *touched = (uint32_t *)take((size_t)W * 4);
     int32_t *tlist = (int32_t *)take((size_t)n * 4);
     int2 *ptasks = (int2 *)take(max_ptasks * sizeof(int2));
-    int *pctr = (int *)take(64);  // [0] push tasks, [1] touched count
-    unsigned long long *fedges = (unsigned long long *)take(64);
+    MsCtl *ctl = (MsCtl *)take(sizeof(MsCtl));
     HC_CUDA_TRY(cudaMemsetAsync(xacc, 0, nk * 8, g->stream));
     HC_CUDA_TRY(cudaMemsetAsync(touched, 0, (size_t)W * 4, g->stream));
     HC_CUDA_TRY(cudaMemsetAsync(seen, 0, nk * 8, g->stream));
@@ -440,85 +523,68 @@ hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int n
     HC_CUDA_TRY(cudaMemsetAsync(hub_cnt, 0, (size_t)std::max(plan.n_hubs, 1) * 4, g->stream));
     if (depth) HC_CUDA_TRY(cudaMemsetAsync(depth, 0xff, sizeof(int32_t) * (size_t)nsrc * n, g->stream));
     { msbfs_seed<K64><<<(nsrc + 255) / 256, 256, 0, g->stream>>>(nsrc, d_src, seen, fr[0], act[0], depth, n); ::hc::count_launch(); }
-    HC_CUDA_TRY(cudaGetLastError());
     const int max_levels = o.max_epochs > 0 ? o.max_epochs : g->N + 1;
+    { msbfs_ctl_init<<<1, 32, 0, g->stream>>>(ctl, max_levels, (long long)g->M); ::hc::count_launch(); }
+    HC_CUDA_TRY(cudaGetLastError());
     const int grid = g->sm_count * 8;
-    HC_TRY(g->pinned.ensure(64));
-    volatile unsigned long long *hfound = g->pinned.as<unsigned long long>();
-    int level = 0;
-    double b = 0;
+    // Offsets + neighbours once per pull level, plus seen / frontier words per vertex.
+    const double pull_bytes = 8.0 * (n + 1) + 4.0 * g->M + 3.0 * 8.0 * K64 * (double)g->n_active;
+    const int64_t *index = g->index.as<int64_t>();
+    const int32_t *nbr = g->nbr.as<int32_t>();
+    // One level of parity c: begin, push (tasks, edges, finalize) and pull
+    // (hub tasks, rows) kernels, each returning at once when the level is of
+    // the other kind, and the end kernel.
+    auto launch_level = [&](cudaStream_t st, int c, cudaGraphConditionalHandle cond, int use_cond) {
+        msbfs_begin<<<grid, 256, 0, st>>>(ctl, act[c ^ 1], W);
+        msbfs_push_tasks<<<grid, kMsThreads, 0, st>>>(index, act[c], g->n_active, ptasks, ctl);
+        msbfs_push<K64><<<grid, kMsThreads, 0, st>>>(index, nbr, ptasks, fr[c], seen, xacc, touched, tlist, ctl);
+        msbfs_push_finalize<K64><<<grid, kMsThreads, 0, st>>>(tlist, nsrc, seen, xacc, fr[c ^ 1], touched, act[c ^ 1],
+                                                              done, depth, n, ctl);
+        if (plan.n_tasks > 0)
+            msbfs_hub<K64><<<grid, kMsThreads, 0, st>>>(index, nbr, plan, nsrc, seen, fr[c], fr[c ^ 1], act[c],
+                                                        act[c ^ 1], done, hub_acc, hub_cnt, depth, n, ctl);
+        msbfs_pull<K64><<<grid, kMsThreads, 0, st>>>(index, nbr, g->n_active, nsrc, seen, fr[c], fr[c ^ 1], act[c],
+                                                     act[c ^ 1], done, depth, n, ctl);
+        msbfs_end<<<1, 32, 0, st>>>(ctl, pull_bytes, cond, use_cond);
+    };
+    const int per_level = plan.n_tasks > 0 ? 7 : 6;
+    HC_TRY(g->pinned.ensure(sizeof(MsCtl) + 64));
+    MsCtl *hctl = g->pinned.as<MsCtl>();
     const bool trace = std::getenv("HC_TRACE") != nullptr;
-    for (; level < max_levels; level++) {
-        const int c = level & 1;
-        const auto t0 = std::chrono::steady_clock::now();
-        HC_CUDA_TRY(cudaMemsetAsync(found, 0, 8, g->stream));
-        HC_CUDA_TRY(cudaMemsetAsync(act[c ^ 1], 0, (size_t)W * 4, g->stream));
-        // Direction: push while the frontier's edges are below M / kPushAlpha.
-        HC_CUDA_TRY(cudaMemsetAsync(pctr, 0, 64, g->stream));
-        HC_CUDA_TRY(cudaMemsetAsync(fedges, 0, 8, g->stream));
-        {
-            msbfs_push_tasks<<<grid, kMsThreads, 0, g->stream>>>(g->index.as<int64_t>(), act[c], g->n_active, ptasks,
-                                                                 pctr, fedges);
-            ::hc::count_launch();
-        }
-        HC_CUDA_TRY(cudaMemcpyAsync((void *)hfound, fedges, 8, cudaMemcpyDeviceToHost, g->stream));
+    if (o.use_graph != HC_GRAPH_OFF && !trace) {
+        // The graph's body is two levels (parity 0 then 1).
+        WhileGraph wg;
+        auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle cond) {
+            launch_level(cs, 0, cond, 1);
+            launch_level(cs, 1, cond, 1);
+        };
+        HC_TRY(wg.build(body, "hc_bfs_batched"));
+        HC_CUDA_TRY(cudaGraphLaunch(wg.exec, g->stream));
+        HC_CUDA_TRY(cudaMemcpyAsync(hctl, ctl, sizeof(MsCtl), cudaMemcpyDeviceToHost, g->stream));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        const unsigned long long fe = *hfound;
-        constexpr double kPushAlpha = 10.0;
-        const bool push = (double)fe * kPushAlpha < (double)g->M;
-        if (push) {
-            {
-                msbfs_push<K64><<<grid, kMsThreads, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
-                                                                    ptasks, pctr, fr[c], seen, xacc, touched, tlist,
-                                                                    pctr + 1);
-                ::hc::count_launch();
-            }
-            {
-                msbfs_push_finalize<K64><<<grid, kMsThreads, 0, g->stream>>>(tlist, pctr + 1, nsrc, seen, xacc,
-                                                                             fr[c ^ 1], touched, act[c ^ 1], done,
-                                                                             depth, n, level, found);
-                ::hc::count_launch();
-            }
+        ::hc::count_launch(2 * per_level * ((hctl->level + 1) / 2));
+    } else {
+        for (int level = 0;; level++) {
+            const auto t0 = std::chrono::steady_clock::now();
+            launch_level(g->stream, level & 1, 0, 0);
+            ::hc::count_launch(per_level);
             HC_CUDA_TRY(cudaGetLastError());
-            HC_CUDA_TRY(cudaMemcpyAsync((void *)hfound, found, 8, cudaMemcpyDeviceToHost, g->stream));
+            HC_CUDA_TRY(cudaMemcpyAsync(hctl, ctl, sizeof(MsCtl), cudaMemcpyDeviceToHost, g->stream));
             HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-            b += 16.0 * (double)fe / 8.0 + 4.0 * (double)fe;
             if (trace)
-                std::fprintf(stderr, "[hc msbfs] L%-3d push fedges=%-11llu found=%-9llu %8.1f us\n", level, fe,
-                             (unsigned long long)*hfound,
+                std::fprintf(stderr, "[hc msbfs] L%-3d %s fedges=%-11llu found=%-9llu %8.1f us\n", level,
+                             (double)hctl->fedges * kMsPushAlpha < (double)g->M ? "push" : "pull", hctl->fedges,
+                             hctl->found,
                              std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count());
-            if (*hfound == 0) {
-                level++;
-                break;
-            }
-            continue;
-        }
-        if (plan.n_tasks > 0) {
-            msbfs_hub<K64><<<grid, kMsThreads, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), plan, nsrc,
-                                                               seen, fr[c], fr[c ^ 1], act[c], act[c ^ 1], done,
-                                                               hub_acc, hub_cnt, depth, n, level, found);
-            ::hc::count_launch();
-        }
-        {
-            msbfs_pull<K64><<<grid, kMsThreads, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
-                                                                g->n_active, nsrc, seen, fr[c], fr[c ^ 1], act[c],
-                                                                act[c ^ 1], done, depth, n, level, found);
-            ::hc::count_launch();
-        }
-        HC_CUDA_TRY(cudaGetLastError());
-        HC_CUDA_TRY(cudaMemcpyAsync((void *)hfound, found, 8, cudaMemcpyDeviceToHost, g->stream));
-        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        // Offsets + neighbours once per level, plus seen / frontier words per vertex.
-        b += 8.0 * (n + 1) + 4.0 * g->M + 3.0 * 8.0 * K64 * (double)g->n_active;
-        if (trace)
-            std::fprintf(stderr, "[hc msbfs] L%-3d pull fedges=%-11llu found=%-9llu %8.1f us\n", level, fe,
-                         (unsigned long long)*hfound,
-                         std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count());
-        if (*hfound == 0) {
-            level++;
-            break;
+            if (hctl->stop || hctl->fin) break;
         }
     }
+    if (hctl->stop) {
+        if (hctl->status == HC_ERR_TIMEOUT) return fail(HC_ERR_TIMEOUT, "hc_bfs_batched: group time limit reached");
+        return fail(HC_ERR_NOT_CONVERGED, "hc_bfs_batched: level cap reached");
+    }
+    const int level = hctl->level;
+    const double b = hctl->bytes;
     *levels_out = level;
     *bytes = b;
     return HC_OK;

@@ -30,8 +30,34 @@ namespace hc {
 namespace {
 
 constexpr int kLongRow = 2048;
-// Pull epochs run while the queue holds more than n_active / kPullDiv vertices.
-constexpr int kPullDiv = 8;
+// An epoch is a pull when the edges out of its queue, times kPullAlpha, exceed
+// M: a pull reads every row of the distance matrix once, a push only the rows
+// its queue's edges reach.
+constexpr int kPullAlpha = 2;
+// Wall-clock bound of one group's epoch loop (checked between epochs).
+constexpr unsigned long long kGroupLimitNs = 60ull * 1000000000ull;
+
+// Epoch control in device memory.  Every kernel of an epoch reads the queue
+// length and the push/pull choice from here, so the same launch sequence runs
+// from the host loop and as the body of a graph's while node, whose condition
+// mssp_end sets.
+struct MsspCtl {
+    int qlen[2];                    // queue lengths; parity c reads qlen[c], fills qlen[c ^ 1]
+    unsigned long long qedges[2];   // edges out of the vertices of each queue
+    int ntasks;                     // long-row chunks queued by the push epoch
+    int epochs;
+    int stop;                       // the loop ended early (status says why)
+    int status;
+    int pull_alpha;                 // 0: push only
+    int max_epochs;
+    long long m;
+    unsigned long long t0;
+};
+
+__device__ __forceinline__ int ctl_queue(const MsspCtl *ctl, int c) { return ctl->stop ? 0 : ctl->qlen[c]; }
+__device__ __forceinline__ bool ctl_pull(const MsspCtl *ctl, int c) {
+    return ctl->pull_alpha > 0 && (double)ctl->qedges[c] * ctl->pull_alpha > (double)ctl->m;
+}
 
 template <int SPL>
 __device__ __forceinline__ void load_row(const int32_t *p, int32_t (&d)[SPL]) {
@@ -65,25 +91,38 @@ __global__ void mssp_init(int32_t n, int32_t *dist, uint32_t *act0, uint32_t *ac
 }
 
 template <int SPL>
-__global__ void mssp_seed(int nsrc, const int32_t *src, int32_t *dist, uint32_t *act, int32_t *queue, int *qlen) {
+__global__ void mssp_seed(int nsrc, const int32_t *src, const int64_t *index, int32_t *dist, uint32_t *act,
+                          int32_t *queue, MsspCtl *ctl, int pull_alpha, long long m, int max_epochs) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         int q = 0;
+        unsigned long long qe = 0;
         for (int s = 0; s < nsrc; s++) {
             const int32_t v = src[s];
             dist[(size_t)v * 32 * SPL + s] = 0;
-            if (act[v] == 0) queue[q++] = v;
+            if (act[v] == 0) {
+                queue[q++] = v;
+                qe += (unsigned long long)(index[v + 1] - index[v]);
+            }
             act[v] |= 1u << (s / SPL);
         }
-        *qlen = q;
+        MsspCtl c{};
+        c.qlen[0] = q;
+        c.qedges[0] = qe;
+        c.pull_alpha = pull_alpha;
+        c.m = m;
+        c.max_epochs = max_epochs;
+        c.t0 = globaltimer_ns();
+        *ctl = c;
     }
 }
 
 // Relax edges [e0, e1) of row u for the active lanes in `m`; du = this lane's
 // distances of u.
 template <int SPL>
-__device__ __forceinline__ void relax_range(const int32_t *nbr, const int32_t *w, int32_t *dist, uint32_t m,
-                                            const int32_t (&du)[SPL], int64_t e0, int64_t e1, uint32_t *act_next,
-                                            int32_t *qnext, int *qlen, unsigned long long &relaxed) {
+__device__ __forceinline__ void relax_range(const int64_t *index, const int32_t *nbr, const int32_t *w,
+                                            int32_t *dist, uint32_t m, const int32_t (&du)[SPL], int64_t e0,
+                                            int64_t e1, uint32_t *act_next, int32_t *qnext, int *qlen,
+                                            unsigned long long &relaxed, unsigned long long &qe) {
     constexpr int K = 32 * SPL;
     const int lane = threadIdx.x & 31;
     const bool on = (m >> lane) & 1u;
@@ -143,7 +182,10 @@ __device__ __forceinline__ void relax_range(const int32_t *nbr, const int32_t *w
                 const int leader = __ffs(ap) - 1;
                 if (lane == leader) base_q = atomicAdd(qlen, __popc(ap));
                 base_q = __shfl_sync(kFull, base_q, leader);
-                if (app) qnext[base_q + __popc(ap & ((1u << lane) - 1u))] = myv;
+                if (app) {
+                    qnext[base_q + __popc(ap & ((1u << lane) - 1u))] = myv;
+                    qe += (unsigned long long)(index[myv + 1] - index[myv]);
+                }
             }
         }
         if (lane == 0) relaxed += (unsigned long long)cnt * __popc(m) * SPL;
@@ -152,13 +194,17 @@ __device__ __forceinline__ void relax_range(const int32_t *nbr, const int32_t *w
 
 template <int SPL>
 __global__ void __launch_bounds__(256) mssp_epoch(const int64_t *index, const int32_t *nbr, const int32_t *w,
-                                                  int32_t *dist, const int32_t *qcur, int nq, const uint32_t *act_cur,
-                                                  uint32_t *act_next, int32_t *qnext, int *qnext_len, int2 *tasks,
-                                                  int *ntasks, unsigned long long *relaxed) {
+                                                  int32_t *dist, const int32_t *qcur, const uint32_t *act_cur,
+                                                  uint32_t *act_next, int32_t *qnext, int2 *tasks, MsspCtl *ctl, int c,
+                                                  unsigned long long *relaxed) {
+    const int nq = ctl_queue(ctl, c);
+    if (nq == 0 || ctl_pull(ctl, c)) return;
+    int *qnext_len = &ctl->qlen[c ^ 1];
+    int *ntasks = &ctl->ntasks;
     const int lane = threadIdx.x & 31;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    unsigned long long rel = 0;
+    unsigned long long rel = 0, qe = 0;
     for (int qi = gwarp; qi < nq; qi += nwarps) {
         const int32_t u = qcur[qi];
         const uint32_t m = act_cur[u];
@@ -173,22 +219,27 @@ __global__ void __launch_bounds__(256) mssp_epoch(const int64_t *index, const in
         }
         int32_t du[SPL];
         load_row<SPL>(dist + (size_t)u * 32 * SPL + lane * SPL, du);
-        relax_range<SPL>(nbr, w, dist, m, du, b, e, act_next, qnext, qnext_len, rel);
+        relax_range<SPL>(index, nbr, w, dist, m, du, b, e, act_next, qnext, qnext_len, rel, qe);
     }
     rel = warp_sum(rel);
+    qe = warp_sum(qe);
     if (lane == 0 && rel) atomicAdd(relaxed, rel);
+    if (lane == 0 && qe) atomicAdd(&ctl->qedges[c ^ 1], qe);
 }
 
 template <int SPL>
 __global__ void __launch_bounds__(256) mssp_tasks(const int64_t *index, const int32_t *nbr, const int32_t *w,
-                                                  int32_t *dist, const int2 *tasks, const int *ntasks,
-                                                  const uint32_t *act_cur, uint32_t *act_next, int32_t *qnext,
-                                                  int *qnext_len, unsigned long long *relaxed) {
+                                                  int32_t *dist, const int2 *tasks, const uint32_t *act_cur,
+                                                  uint32_t *act_next, int32_t *qnext, MsspCtl *ctl, int c,
+                                                  unsigned long long *relaxed) {
+    const int nq = ctl_queue(ctl, c);
+    if (nq == 0 || ctl_pull(ctl, c)) return;
+    int *qnext_len = &ctl->qlen[c ^ 1];
     const int lane = threadIdx.x & 31;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const int nt = *ntasks;
-    unsigned long long rel = 0;
+    const int nt = ctl->ntasks;
+    unsigned long long rel = 0, qe = 0;
     for (int t = gwarp; t < nt; t += nwarps) {
         const int2 tk = tasks[t];
         const int32_t u = tk.x;
@@ -198,10 +249,12 @@ __global__ void __launch_bounds__(256) mssp_tasks(const int64_t *index, const in
         const int64_t e = (re < b + kLongRow) ? re : b + kLongRow;
         int32_t du[SPL];
         load_row<SPL>(dist + (size_t)u * 32 * SPL + lane * SPL, du);
-        relax_range<SPL>(nbr, w, dist, m, du, b, e, act_next, qnext, qnext_len, rel);
+        relax_range<SPL>(index, nbr, w, dist, m, du, b, e, act_next, qnext, qnext_len, rel, qe);
     }
     rel = warp_sum(rel);
+    qe = warp_sum(qe);
     if (lane == 0 && rel) atomicAdd(relaxed, rel);
+    if (lane == 0 && qe) atomicAdd(&ctl->qedges[c ^ 1], qe);
 }
 
 // Pull epoch, used while the queue covers a large part of the graph (weights
@@ -214,8 +267,10 @@ __global__ void __launch_bounds__(256) mssp_tasks(const int64_t *index, const in
 template <int SPL>
 __global__ void __launch_bounds__(256) mssp_pull(const int64_t *index, const int32_t *nbr, const int32_t *w,
                                                  int32_t *dist, int32_t n_rows, const int2 *tasks, int ntasks,
-                                                 const uint32_t *act_cur, uint32_t *act_next,
-                                                 unsigned long long *relaxed) {
+                                                 const uint32_t *act_cur, uint32_t *act_next, const MsspCtl *ctl,
+                                                 int c, unsigned long long *relaxed) {
+    const int nq = ctl_queue(ctl, c);
+    if (nq == 0 || !ctl_pull(ctl, c)) return;
     constexpr int K = 32 * SPL;
     const int lane = threadIdx.x & 31;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -308,8 +363,13 @@ __global__ void __launch_bounds__(256) mssp_pull(const int64_t *index, const int
     if (lane == 0 && rel) atomicAdd(relaxed, rel);
 }
 
-// Queue of the vertices with a non-zero activity mask, in vertex order.
-__global__ void mssp_compact(const uint32_t *act, int32_t n, int32_t *q, int *qlen) {
+// Queue of the vertices with a non-zero activity mask, in vertex order (after
+// a pull epoch).
+__global__ void mssp_compact(const int64_t *index, const uint32_t *act, int32_t n, int32_t *q, MsspCtl *ctl, int c) {
+    const int nq = ctl_queue(ctl, c);
+    if (nq == 0 || !ctl_pull(ctl, c)) return;
+    int *qlen = &ctl->qlen[c ^ 1];
+    unsigned long long qe = 0;
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -321,8 +381,13 @@ __global__ void mssp_compact(const uint32_t *act, int32_t n, int32_t *q, int *ql
         int q0 = 0;
         if (lane == 0) q0 = atomicAdd(qlen, __popc(bal));
         q0 = __shfl_sync(kFull, q0, 0);
-        if (on) q[q0 + __popc(bal & ((1u << lane) - 1u))] = (int32_t)v;
+        if (on) {
+            q[q0 + __popc(bal & ((1u << lane) - 1u))] = (int32_t)v;
+            qe += (unsigned long long)(index[v + 1] - index[v]);
+        }
     }
+    qe = warp_sum(qe);
+    if (lane == 0 && qe) atomicAdd(&ctl->qedges[c ^ 1], qe);
 }
 
 // (row, chunk) tasks for the rows longer than kLongRow.
@@ -351,8 +416,37 @@ hc_status ensure_pull_plan(hc_graph *g) {
     return HC_OK;
 }
 
-__global__ void mssp_clear(const int32_t *q, int nq, uint32_t *act) {
+// Clears the activity masks of the epoch's queue (they become the next-next
+// epoch's output).
+__global__ void mssp_clear(const int32_t *q, uint32_t *act, const MsspCtl *ctl, int c) {
+    const int nq = ctl_queue(ctl, c);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) act[q[i]] = 0;
+}
+
+// Closes epoch parity c: counts it, resets its counters for reuse, and decides
+// whether another epoch runs (queue non-empty, under the epoch cap and the
+// time bound); inside a graph it sets the while node's condition.
+__global__ void mssp_end(MsspCtl *ctl, int c, cudaGraphConditionalHandle cond, int use_cond) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    bool go = false;
+    if (!ctl->stop && ctl->qlen[c] > 0) {
+        ctl->epochs++;
+        ctl->qlen[c] = 0;
+        ctl->qedges[c] = 0;
+        ctl->ntasks = 0;
+        go = ctl->qlen[c ^ 1] > 0;
+        if (go && ctl->epochs >= ctl->max_epochs) {
+            ctl->stop = 1;
+            ctl->status = HC_ERR_NOT_CONVERGED;
+            go = false;
+        }
+        if (go && globaltimer_ns() - ctl->t0 > kGroupLimitNs) {
+            ctl->stop = 1;
+            ctl->status = HC_ERR_TIMEOUT;
+            go = false;
+        }
+    }
+    if (use_cond) cudaGraphSetConditional(cond, go ? 1u : 0u);
 }
 
 // dist[v][K] -> out[s][v] for the group's sources, 32-vertex tiles through
@@ -376,86 +470,113 @@ __global__ void mssp_transpose(const int32_t *dist, int32_t n, int nsrc, int32_t
     }
 }
 
+struct MsspBufs {
+    int32_t *dist;
+    uint32_t *act[2];
+    int32_t *q[2];
+    int2 *tasks;
+    MsspCtl *ctl;
+    int32_t *src;
+};
+
+// One epoch of parity c: the push kernels, the pull kernels (each returns at
+// once when the epoch is of the other kind), the activity clear and the end
+// kernel.  Six launches.
 template <int SPL>
-hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int max_epochs, int pull_div,
-                    int *epochs_out, unsigned long long *relaxed) {
+void launch_epoch(const hc_graph *g, cudaStream_t st, const MsspBufs &b, int c, unsigned long long *relaxed,
+                  cudaGraphConditionalHandle cond, int use_cond) {
+    const int grid = g->sm_count * 8;
+    const int64_t *index = g->index.as<int64_t>();
+    const int32_t *nbr = g->nbr.as<int32_t>(), *w = g->wgt.as<int32_t>();
+    mssp_epoch<SPL><<<grid, 256, 0, st>>>(index, nbr, w, b.dist, b.q[c], b.act[c], b.act[c ^ 1], b.q[c ^ 1], b.tasks,
+                                          b.ctl, c, relaxed);
+    mssp_tasks<SPL><<<grid, 256, 0, st>>>(index, nbr, w, b.dist, b.tasks, b.act[c], b.act[c ^ 1], b.q[c ^ 1], b.ctl, c,
+                                          relaxed);
+    mssp_pull<SPL><<<grid, 256, 0, st>>>(index, nbr, w, b.dist, g->n_active, g->ws_plan_mssp.as<int2>(),
+                                         g->mssp_tasks < 0 ? 0 : g->mssp_tasks, b.act[c], b.act[c ^ 1], b.ctl, c,
+                                         relaxed);
+    mssp_clear<<<grid, 256, 0, st>>>(b.q[c], b.act[c], b.ctl, c);
+    mssp_compact<<<grid, 256, 0, st>>>(index, b.act[c ^ 1], g->N, b.q[c ^ 1], b.ctl, c);
+    mssp_end<<<1, 32, 0, st>>>(b.ctl, c, cond, use_cond);
+}
+constexpr int kEpochLaunches = 6;
+
+template <int SPL>
+hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int max_epochs, int pull_alpha,
+                    bool use_graph, WhileGraph &eg, int *epochs_out, unsigned long long *relaxed) {
     constexpr int K = 32 * SPL;
     const int64_t n = g->N;
     const int64_t max_tasks = 2 * (g->M / kLongRow) + n / kLongRow + 64;
     HC_TRY(g->ws_batch.ensure((size_t)n * K * 4 + (size_t)n * 4 * 4 + sizeof(int2) * max_tasks + 8192));
     char *p = g->ws_batch.as<char>();
-    auto take = [&](size_t b) {
+    auto take = [&](size_t bytes) {
         char *r = p;
-        p += (b + 255) / 256 * 256;
+        p += (bytes + 255) / 256 * 256;
         return r;
     };
-    int32_t *dist = (int32_t *)take((size_t)n * K * 4);
-    uint32_t *act[2] = {(uint32_t *)take((size_t)n * 4), (uint32_t *)take((size_t)n * 4)};
-    int32_t *q[2] = {(int32_t *)take((size_t)n * 4), (int32_t *)take((size_t)n * 4)};
-    int2 *tasks = (int2 *)take(sizeof(int2) * max_tasks);
-    int *ctr = (int *)take(256);  // [0],[1] queue lengths, [2] tasks
-    int32_t *d_src = (int32_t *)take(sizeof(int32_t) * K);
+    MsspBufs b;
+    b.dist = (int32_t *)take((size_t)n * K * 4);
+    b.act[0] = (uint32_t *)take((size_t)n * 4);
+    b.act[1] = (uint32_t *)take((size_t)n * 4);
+    b.q[0] = (int32_t *)take((size_t)n * 4);
+    b.q[1] = (int32_t *)take((size_t)n * 4);
+    b.tasks = (int2 *)take(sizeof(int2) * max_tasks);
+    b.ctl = (MsspCtl *)take(sizeof(MsspCtl));
+    b.src = (int32_t *)take(sizeof(int32_t) * K);
     const int grid = g->sm_count * 8;
-    HC_TRY(g->pinned.ensure(64));
-    volatile int *hq = g->pinned.as<int>();
-    HC_CUDA_TRY(cudaMemcpyAsync(d_src, h_src, sizeof(int32_t) * k, cudaMemcpyHostToDevice, g->stream));
-    { mssp_init<SPL><<<grid, 256, 0, g->stream>>>(g->N, dist, act[0], act[1]); ::hc::count_launch(); }
-    { mssp_seed<SPL><<<1, 32, 0, g->stream>>>(k, d_src, dist, act[0], q[0], &ctr[0]); ::hc::count_launch(); }
-    HC_CUDA_TRY(cudaGetLastError());
-    HC_CUDA_TRY(cudaMemcpyAsync((void *)hq, &ctr[0], 4, cudaMemcpyDeviceToHost, g->stream));
-    HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    int nq = *hq;
-    int ep = 0;
-    const bool trace = std::getenv("HC_TRACE") != nullptr;
-    for (; nq > 0; ep++) {
-        const auto t0 = std::chrono::steady_clock::now();
-        if (ep >= max_epochs) return fail(HC_ERR_NOT_CONVERGED, "hc_sssp_batched: epoch cap reached");
-        const int c = ep & 1;
-        HC_CUDA_TRY(cudaMemsetAsync(&ctr[c ^ 1], 0, 4, g->stream));
-        HC_CUDA_TRY(cudaMemsetAsync(&ctr[2], 0, 4, g->stream));
-        // Pull while the queue holds more than n_active / pull_div vertices.
-        const bool pull = pull_div > 0 && (int64_t)nq * pull_div > g->n_active;
-        if (pull) {
-            {
-                mssp_pull<SPL><<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
-                                                            g->wgt.as<int32_t>(), dist, g->n_active,
-                                                            g->ws_plan_mssp.as<int2>(), g->mssp_tasks, act[c],
-                                                            act[c ^ 1], relaxed);
-                ::hc::count_launch();
-            }
-            { mssp_clear<<<(nq + 255) / 256, 256, 0, g->stream>>>(q[c], nq, act[c]); ::hc::count_launch(); }
-            { mssp_compact<<<grid, 256, 0, g->stream>>>(act[c ^ 1], g->N, q[c ^ 1], &ctr[c ^ 1]); ::hc::count_launch(); }
-        } else {
-        {
-            mssp_epoch<SPL><<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
-                                                         g->wgt.as<int32_t>(), dist, q[c], nq, act[c], act[c ^ 1],
-                                                         q[c ^ 1], &ctr[c ^ 1], tasks, &ctr[2], relaxed);
-            ::hc::count_launch();
-        }
-        {
-            mssp_tasks<SPL><<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
-                                                         g->wgt.as<int32_t>(), dist, tasks, &ctr[2], act[c],
-                                                         act[c ^ 1], q[c ^ 1], &ctr[c ^ 1], relaxed);
-            ::hc::count_launch();
-        }
-        { mssp_clear<<<(nq + 255) / 256, 256, 0, g->stream>>>(q[c], nq, act[c]); ::hc::count_launch(); }
-        }
-        HC_CUDA_TRY(cudaGetLastError());
-        HC_CUDA_TRY(cudaMemcpyAsync((void *)hq, &ctr[c ^ 1], 4, cudaMemcpyDeviceToHost, g->stream));
-        if (trace) HC_CUDA_TRY(cudaMemcpyAsync((void *)(hq + 2), relaxed, 8, cudaMemcpyDeviceToHost, g->stream));
-        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        if (trace) {
-            const double us = std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
-            unsigned long long r = 0;
-            std::memcpy(&r, (const void *)(hq + 2), 8);
-            std::fprintf(stderr, "mssp K=%d epoch %d %s queue %d next %d relaxed(total) %llu  %.1f us\n", K, ep,
-                         pull ? "pull" : "push", nq, *hq, r, us);
-        }
-        nq = *hq;
+    HC_TRY(g->pinned.ensure(sizeof(MsspCtl) + 64));
+    MsspCtl *hctl = g->pinned.as<MsspCtl>();
+    HC_CUDA_TRY(cudaMemcpyAsync(b.src, h_src, sizeof(int32_t) * k, cudaMemcpyHostToDevice, g->stream));
+    { mssp_init<SPL><<<grid, 256, 0, g->stream>>>(g->N, b.dist, b.act[0], b.act[1]); ::hc::count_launch(); }
+    {
+        mssp_seed<SPL><<<1, 32, 0, g->stream>>>(k, b.src, g->index.as<int64_t>(), b.dist, b.act[0], b.q[0], b.ctl,
+                                                pull_alpha, (long long)g->M, max_epochs);
+        ::hc::count_launch();
     }
-    *epochs_out = ep;
+    HC_CUDA_TRY(cudaGetLastError());
+    const bool trace = std::getenv("HC_TRACE") != nullptr;
+    if (use_graph && !trace) {
+        // The graph's body is two epochs (parity 0 then 1); kernels of an
+        // epoch whose queue is empty return at once.
+        if (!eg.exec) {
+            auto body = [&](cudaStream_t cs, cudaGraphConditionalHandle cond) {
+                launch_epoch<SPL>(g, cs, b, 0, relaxed, cond, 1);
+                launch_epoch<SPL>(g, cs, b, 1, relaxed, cond, 1);
+            };
+            HC_TRY(eg.build(body, "hc_sssp_batched"));
+        }
+        HC_CUDA_TRY(cudaGraphLaunch(eg.exec, g->stream));
+        HC_CUDA_TRY(cudaMemcpyAsync(hctl, b.ctl, sizeof(MsspCtl), cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        ::hc::count_launch(2 * kEpochLaunches * ((hctl->epochs + 1) / 2));
+    } else {
+        for (int ep = 0;; ep++) {
+            const auto t0 = std::chrono::steady_clock::now();
+            const int c = ep & 1;
+            launch_epoch<SPL>(g, g->stream, b, c, relaxed, 0, 0);
+            ::hc::count_launch(kEpochLaunches);
+            HC_CUDA_TRY(cudaGetLastError());
+            HC_CUDA_TRY(cudaMemcpyAsync(hctl, b.ctl, sizeof(MsspCtl), cudaMemcpyDeviceToHost, g->stream));
+            if (trace) HC_CUDA_TRY(cudaMemcpyAsync(hctl + 1, relaxed, 8, cudaMemcpyDeviceToHost, g->stream));
+            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            if (trace) {
+                const double us =
+                    std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+                unsigned long long r = 0;
+                std::memcpy(&r, hctl + 1, 8);
+                std::fprintf(stderr, "mssp K=%d epoch %d next %d (%llu edges) relaxed(total) %llu  %.1f us\n", K, ep,
+                             hctl->qlen[c ^ 1], hctl->qedges[c ^ 1], r, us);
+            }
+            if (hctl->stop || hctl->qlen[c ^ 1] == 0) break;
+        }
+    }
+    if (hctl->stop) {
+        if (hctl->status == HC_ERR_TIMEOUT) return fail(HC_ERR_TIMEOUT, "hc_sssp_batched: group time limit reached");
+        return fail(HC_ERR_NOT_CONVERGED, "hc_sssp_batched: epoch cap reached");
+    }
+    *epochs_out = hctl->epochs;
     if (dst) {
-        { mssp_transpose<SPL><<<grid, 256, 0, g->stream>>>(dist, g->N, k, dst); ::hc::count_launch(); }
+        { mssp_transpose<SPL><<<grid, 256, 0, g->stream>>>(b.dist, g->N, k, dst); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
     }
     return HC_OK;
@@ -488,35 +609,37 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
         size_t free_b = 0, total_b = 0;
         HC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
         free_b += g->ws_batch.bytes + g->ws_out0.bytes;  // workspaces are reused
-        // Host outputs also stage each group's rows in a device buffer.
-        const double copies = (dist_out && !is_device_pointer(dist_out)) ? 2.0 : 1.0;
         group = 256;
-        while (group > 32 && (double)g->N * group * 4.0 * copies > 0.4 * copies * (double)free_b) group /= 2;
+        while (group > 32 && (double)g->N * group * 4.0 > 0.4 * (double)free_b) group /= 2;
     }
     // Weights must be non-negative; pull epochs need symmetric weights.
     HC_TRY(ensure_weight_stats(g));
     if (g->w_negative) return fail(HC_ERR_INVALID_ARG, "hc_sssp_batched: negative edge weight");
-    int pull_div = g->w_symmetric ? kPullDiv : 0;
-    if (const char *e = std::getenv("HC_MSSP_PULL_DIV")) pull_div = g->w_symmetric ? std::atoi(e) : 0;
-    if (pull_div > 0) HC_TRY(ensure_pull_plan(g));
+    int pull_alpha = g->w_symmetric ? kPullAlpha : 0;
+    if (const char *e = std::getenv("HC_MSSP_PULL_ALPHA")) pull_alpha = g->w_symmetric ? std::atoi(e) : 0;
+    if (pull_alpha > 0) HC_TRY(ensure_pull_plan(g));
     const int64_t n = g->N;
     const bool dev_out = is_device_pointer(dist_out);
     if (dist_out && !dev_out) HC_TRY(g->ws_out0.ensure(sizeof(int32_t) * (size_t)group * n));
-    const int max_epochs = o.max_epochs > 0 ? o.max_epochs : 0x7fffffff;
+    // Chaotic relaxation finalises at least one more hop per epoch: N + 1 bounds the loop.
+    const int max_epochs = o.max_epochs > 0 ? o.max_epochs : g->N + 1;
     HC_TRY(g->ws_src.ensure(64));
     unsigned long long *relaxed = g->ws_src.as<unsigned long long>();
     HC_CUDA_TRY(cudaMemsetAsync(relaxed, 0, 8, g->stream));
     HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     int epochs_max = 0, groups = 0;
+    // The epoch loop runs as a CUDA graph unless use_graph asks otherwise.
+    const bool use_graph = o.use_graph != HC_GRAPH_OFF;
+    WhileGraph eg;  // built by the first group, reused by the others
     for (int s0 = 0; s0 < num_sources; s0 += group, groups++) {
         const int k = std::min(group, num_sources - s0);
         int32_t *dst = nullptr;
         if (dist_out) dst = dev_out ? dist_out + (size_t)s0 * n : g->ws_out0.as<int32_t>();
         int ep = 0;
-        if (group == 32) HC_TRY(run_group<1>(g, src.data() + s0, k, dst, max_epochs, pull_div, &ep, relaxed));
-        else if (group == 64) HC_TRY(run_group<2>(g, src.data() + s0, k, dst, max_epochs, pull_div, &ep, relaxed));
-        else if (group == 128) HC_TRY(run_group<4>(g, src.data() + s0, k, dst, max_epochs, pull_div, &ep, relaxed));
-        else HC_TRY(run_group<8>(g, src.data() + s0, k, dst, max_epochs, pull_div, &ep, relaxed));
+        if (group == 32) HC_TRY(run_group<1>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
+        else if (group == 64) HC_TRY(run_group<2>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
+        else if (group == 128) HC_TRY(run_group<4>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
+        else HC_TRY(run_group<8>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
         if (dist_out && !dev_out)
             HC_TRY(copy_out(dist_out + (size_t)s0 * n, dst, sizeof(int32_t) * (size_t)k * n, g->stream));
         epochs_max = std::max(epochs_max, ep);
@@ -531,9 +654,9 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
         stats->epochs = epochs_max;
         stats->groups = groups;
         stats->ms = ms;
-        // 8 B (neighbour + weight) per edge visit of a row, amortised over the
-        // group's 32 lanes, plus the 4 B distance read per source relaxed.
-        stats->bytes_model = (double)rel / (32.0 * (group / 32)) * 8.0 + (double)rel * 4.0;
+        // 8 B (neighbour + weight) per edge visit of a row, shared by the
+        // group's sources, plus the 4 B distance read per source relaxed.
+        stats->bytes_model = (double)rel / (double)group * 8.0 + (double)rel * 4.0;
     }
     return HC_OK;
 }

@@ -177,4 +177,52 @@ struct PinnedBuf {
 hc_status copy_in(void *dst_dev, const void *src_any, size_t bytes, cudaStream_t s);
 hc_status copy_out(void *dst_any, const void *src_dev, size_t bytes, cudaStream_t s);
 
+// An epoch loop as a CUDA graph: one conditional while node whose body is
+// captured from `body(stream, handle)`.  The body's last kernel sets the
+// condition with cudaGraphSetConditional; the handle starts at 1 on every
+// launch, so the body runs at least once.
+struct WhileGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    WhileGraph() = default;
+    WhileGraph(const WhileGraph &) = delete;
+    WhileGraph &operator=(const WhileGraph &) = delete;
+    ~WhileGraph() { reset(); }
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    template <class Body>
+    hc_status build(Body &&body, const char *who) {
+        reset();
+        HC_CUDA_TRY(cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle cond;
+        HC_CUDA_TRY(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = cond;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        HC_CUDA_TRY(cudaGraphAddNode(&node, graph, nullptr, 0, &np));
+        // Captured on a private stream, so the caller's stream may be any kind.
+        cudaStream_t cs;
+        HC_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t e =
+            cudaStreamBeginCaptureToGraph(cs, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            body(cs, cond);
+            cudaGraph_t captured = nullptr;
+            e = cudaStreamEndCapture(cs, &captured);
+        }
+        cudaStreamDestroy(cs);
+        if (e != cudaSuccess) return fail(HC_ERR_CUDA, "%s: epoch graph capture: %s", who, cudaGetErrorString(e));
+        HC_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
+        return HC_OK;
+    }
+};
+
 }  // namespace hc

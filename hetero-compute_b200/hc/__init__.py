@@ -76,6 +76,9 @@ class PrStats(C.Structure):
                 ("changed", C.c_int32), ("bytes_model", C.c_double), ("ms", C.c_double)]
 
 
+GRAPH_AUTO, GRAPH_ON, GRAPH_OFF = 0, 1, 2  # hc_batch_opts.use_graph
+
+
 class BatchOpts(C.Structure):
     _fields_ = [("group", C.c_int32), ("max_epochs", C.c_int32), ("use_graph", C.c_int32)]
 
@@ -358,21 +361,21 @@ class Graph:
                "hc_ppr_batched")
         return scores, st
 
-    def bfs_batched(self, sources, depth=None, *, group=0):
+    def bfs_batched(self, sources, depth=None, *, group=0, max_epochs=0, use_graph=GRAPH_AUTO):
         src = np.ascontiguousarray(sources, dtype=np.int32)
         if depth is None:
             depth = np.empty((len(src), self.num_nodes), dtype=np.int32)
-        o = BatchOpts(group, 0, 0)
+        o = BatchOpts(group, max_epochs, use_graph)
         st = BatchStats()
         _check(lib().hc_bfs_batched(self._h, _ptr(src), len(src), _ptr(depth), C.byref(o), C.byref(st)),
                "hc_bfs_batched")
         return depth, st
 
-    def sssp_batched(self, sources, dist=None, *, group=0):
+    def sssp_batched(self, sources, dist=None, *, group=0, max_epochs=0, use_graph=GRAPH_AUTO):
         src = np.ascontiguousarray(sources, dtype=np.int32)
         if dist is None:
             dist = np.empty((len(src), self.num_nodes), dtype=np.int32)
-        o = BatchOpts(group, 0, 0)
+        o = BatchOpts(group, max_epochs, use_graph)
         st = BatchStats()
         _check(lib().hc_sssp_batched(self._h, _ptr(src), len(src), _ptr(dist), C.byref(o), C.byref(st)),
                "hc_sssp_batched")

@@ -259,10 +259,15 @@ hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, const int32_t
 
 /* --------------------------------------------------------------- batched */
 
+/* hc_batch_opts.use_graph */
+#define HC_GRAPH_AUTO 0   /* the library's choice (a graph where the loop has one) */
+#define HC_GRAPH_ON 1     /* run the epoch loop as a CUDA graph (while node) */
+#define HC_GRAPH_OFF 2    /* host loop: one launch sequence and one sync per epoch */
+
 typedef struct hc_batch_opts {
-    int32_t group;        /* sources per group (0 = autotuned) */
+    int32_t group;        /* sources per group (0 = autotuned / sized to free memory) */
     int32_t max_epochs;   /* 0 = unlimited */
-    int32_t use_graph;    /* capture the epoch loop in a CUDA graph */
+    int32_t use_graph;    /* HC_GRAPH_AUTO / _ON / _OFF */
 } hc_batch_opts;
 
 typedef struct hc_batch_stats {

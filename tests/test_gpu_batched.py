@@ -29,13 +29,21 @@ def test_bfs_batched_groups_and_duplicates():
         assert np.array_equal(depth[i], oracle.bfs_depth(host.index, host.neighbors, s))
 
 
-def test_bfs_batched_grid():
+@pytest.mark.parametrize("use_graph", [hc.GRAPH_ON, hc.GRAPH_OFF])
+def test_bfs_batched_grid(use_graph):
+    """~90 levels: the level loop as a CUDA graph (while node) and as a host loop."""
     host = hc.gen_grid(40, 50, 1)
     g = hc.Graph.from_host(host)
     src = np.array([0, 1999, 1000, 7], dtype=np.int32)
-    depth, st = g.bfs_batched(src)
+    depth, st = g.bfs_batched(src, use_graph=use_graph)
+    assert st.epochs > 40
     for i, s in enumerate(src):
         assert np.array_equal(depth[i], oracle.bfs_depth(host.index, host.neighbors, s))
+    with pytest.raises(hc.HCError) as e:
+        g.bfs_batched(src, max_epochs=10, use_graph=use_graph)
+    assert e.value.status == hc.NOT_CONVERGED
+    depth2, _ = g.bfs_batched(src, use_graph=use_graph)  # handle still usable
+    assert np.array_equal(depth2, depth)
 
 
 @pytest.mark.parametrize("scale,k", [(12, 40), (10, 32), (13, 5)])
@@ -63,16 +71,42 @@ def test_sssp_batched_group_widths(group):
     assert np.array_equal(dd.cpu().numpy(), dist)
 
 
-@pytest.mark.parametrize("pull_div", ["0", "8", "1000000"])
-def test_sssp_batched_push_and_pull_epochs(monkeypatch, pull_div):
+@pytest.mark.parametrize("pull_alpha", ["0", "2", "1000000"])
+def test_sssp_batched_push_and_pull_epochs(monkeypatch, pull_alpha):
     """Push only, the default switch, and pull for every epoch."""
-    monkeypatch.setenv("HC_MSSP_PULL_DIV", pull_div)
+    monkeypatch.setenv("HC_MSSP_PULL_ALPHA", pull_alpha)
     big = hc.gen_kronecker(16, 16, 3, wtype=hc.W_I32)  # rows above the chunk size
     g = hc.Graph.from_host(big)
     src = hc.pick_sources(big, 70)
     dist, _ = g.sssp_batched(src, group=64)
     for i in range(0, 70, 9):
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(big.index, big.neighbors, big.weights, src[i])), i
+
+
+@pytest.mark.parametrize("use_graph", [hc.GRAPH_ON, hc.GRAPH_OFF])
+def test_sssp_batched_graph_and_host_loop(use_graph):
+    """The epoch loop as a CUDA graph (while node) and as a host loop give the same distances."""
+    host = hc.gen_grid(50, 40, 4, wtype=hc.W_I32)  # ~100 epochs
+    g = hc.Graph.from_host(host)
+    src = np.array([0, 1999, 1000, 7, 7, 1234], dtype=np.int32)
+    dist, st = g.sssp_batched(src, group=32, use_graph=use_graph)
+    assert st.epochs > 40
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s)), i
+    before = hc.kernel_launches()
+    g.sssp_batched(src, group=32, use_graph=use_graph)
+    assert hc.kernel_launches() - before >= 6 * st.epochs  # launches inside the graph are counted too
+
+
+@pytest.mark.parametrize("use_graph", [hc.GRAPH_ON, hc.GRAPH_OFF])
+def test_sssp_batched_epoch_cap(use_graph):
+    host = hc.gen_grid(50, 40, 4, wtype=hc.W_I32)
+    g = hc.Graph.from_host(host)
+    with pytest.raises(hc.HCError) as e:
+        g.sssp_batched(np.array([0], dtype=np.int32), max_epochs=5, use_graph=use_graph)
+    assert e.value.status == hc.NOT_CONVERGED
+    dist, st = g.sssp_batched(np.array([0], dtype=np.int32), use_graph=use_graph)  # handle still usable
+    assert np.array_equal(dist[0], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, 0))
 
 
 def test_sssp_batched_asymmetric_weights():
