@@ -54,18 +54,21 @@ struct MsCtl {
     int stop;                   // ended early; status says why
     int status;
     int max_levels;
-    int pad;
+    int push_alpha;             // push while fedges * push_alpha < m (0: pull only)
     long long m;
     double bytes;               // bytes model, summed over levels
     unsigned long long t0;
 };
-// Push while the frontier's edges times kMsPushAlpha stay below M.
-constexpr double kMsPushAlpha = 10.0;
+// Default direction switch: push while the frontier's edges times
+// kMsPushAlpha stay below M.
+constexpr int kMsPushAlpha = 10;
 // Wall-clock bound of one group's level loop (checked between levels).
 constexpr unsigned long long kMsLimitNs = 60ull * 1000000000ull;
 
 __device__ __forceinline__ bool ms_live(const MsCtl *c) { return !c->stop && !c->fin; }
-__device__ __forceinline__ bool ms_push(const MsCtl *c) { return (double)c->fedges * kMsPushAlpha < (double)c->m; }
+__device__ __forceinline__ bool ms_push(const MsCtl *c) {
+    return c->push_alpha > 0 && (double)c->fedges * c->push_alpha < (double)c->m;
+}
 
 template <int K64>
 __device__ __forceinline__ uint64_t full_mask(int word, int nsrc) {
@@ -393,10 +396,11 @@ __global__ void msbfs_push_finalize(const int32_t *tlist, int nsrc, uint64_t *se
     if ((threadIdx.x & 31) == 0 && my_found) atomicAdd(found, my_found);
 }
 
-__global__ void msbfs_ctl_init(MsCtl *ctl, int max_levels, long long m) {
+__global__ void msbfs_ctl_init(MsCtl *ctl, int max_levels, int push_alpha, long long m) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         MsCtl c{};
         c.max_levels = max_levels;
+        c.push_alpha = push_alpha;
         c.m = m;
         c.t0 = globaltimer_ns();
         *ctl = c;
@@ -524,7 +528,8 @@ hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int n
     if (depth) HC_CUDA_TRY(cudaMemsetAsync(depth, 0xff, sizeof(int32_t) * (size_t)nsrc * n, g->stream));
     { msbfs_seed<K64><<<(nsrc + 255) / 256, 256, 0, g->stream>>>(nsrc, d_src, seen, fr[0], act[0], depth, n); ::hc::count_launch(); }
     const int max_levels = o.max_epochs > 0 ? o.max_epochs : g->N + 1;
-    { msbfs_ctl_init<<<1, 32, 0, g->stream>>>(ctl, max_levels, (long long)g->M); ::hc::count_launch(); }
+    const int push_alpha = o.switch_alpha == 0 ? kMsPushAlpha : std::max(o.switch_alpha, 0);
+    { msbfs_ctl_init<<<1, 32, 0, g->stream>>>(ctl, max_levels, push_alpha, (long long)g->M); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     const int grid = g->sm_count * 8;
     // Offsets + neighbours once per pull level, plus seen / frontier words per vertex.
@@ -573,7 +578,8 @@ hc_status run_msbfs(hc_graph *g, const MsPlan &plan, const int32_t *d_src, int n
             HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
             if (trace)
                 std::fprintf(stderr, "[hc msbfs] L%-3d %s fedges=%-11llu found=%-9llu %8.1f us\n", level,
-                             (double)hctl->fedges * kMsPushAlpha < (double)g->M ? "push" : "pull", hctl->fedges,
+                             push_alpha > 0 && (double)hctl->fedges * push_alpha < (double)g->M ? "push" : "pull",
+                             hctl->fedges,
                              hctl->found,
                              std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count());
             if (hctl->stop || hctl->fin) break;
@@ -604,6 +610,9 @@ extern "C" hc_status hc_bfs_batched(hc_graph *g, const int32_t *sources, int32_t
     HC_CUDA_TRY(cudaMemcpy(src.data(), sources, sizeof(int32_t) * num_sources, cudaMemcpyDefault));
     for (int32_t s : src)
         if (s < 0 || s >= g->N) return fail(HC_ERR_INVALID_ARG, "hc_bfs_batched: source %d out of range", s);
+    // Zero fields: the handle's tuned values, else 512-source groups.
+    if (o.group <= 0) o.group = g->tune.mbfs_group;
+    if (o.switch_alpha == 0) o.switch_alpha = g->tune.mbfs_switch_alpha;
     const int group = o.group > 0 ? std::min(o.group, 512) : 512;
     const int64_t n = g->N;
     const bool dev_out = is_device_pointer(depth_out);

@@ -604,6 +604,8 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
     // whose distance matrix (N x width x 4 bytes) takes at most 40% of the
     // free device memory, 80% with the staging buffer of host outputs (wider
     // groups share each row read among more sources).
+    if (o.group <= 0) o.group = g->tune.mssp_group;
+    if (o.switch_alpha == 0) o.switch_alpha = g->tune.mssp_switch_alpha;
     int group = o.group <= 32 ? 32 : o.group <= 64 ? 64 : o.group <= 128 ? 128 : 256;
     if (o.group <= 0) {
         size_t free_b = 0, total_b = 0;
@@ -615,8 +617,7 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
     // Weights must be non-negative; pull epochs need symmetric weights.
     HC_TRY(ensure_weight_stats(g));
     if (g->w_negative) return fail(HC_ERR_INVALID_ARG, "hc_sssp_batched: negative edge weight");
-    int pull_alpha = g->w_symmetric ? kPullAlpha : 0;
-    if (const char *e = std::getenv("HC_MSSP_PULL_ALPHA")) pull_alpha = g->w_symmetric ? std::atoi(e) : 0;
+    const int pull_alpha = !g->w_symmetric ? 0 : o.switch_alpha == 0 ? kPullAlpha : std::max(o.switch_alpha, 0);
     if (pull_alpha > 0) HC_TRY(ensure_pull_plan(g));
     const int64_t n = g->N;
     const bool dev_out = is_device_pointer(dist_out);

@@ -380,8 +380,10 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
     if (!sources || num_sources < 0) return fail(HC_ERR_INVALID_ARG, "hc_bfs: bad source list");
     hc_bfs_opts o{};
     if (opts) o = *opts;
-    if (o.alpha <= 0) o.alpha = 15;
-    if (o.beta <= 0) o.beta = 18;
+    // Zero fields: the handle's tuned values, else Beamer's alpha = 15, beta = 18.
+    if (o.alpha <= 0) o.alpha = g->tune.bfs_alpha > 0 ? g->tune.bfs_alpha : 15;
+    if (o.beta <= 0) o.beta = g->tune.bfs_beta > 0 ? g->tune.bfs_beta : 18;
+    if (o.bu_variant == HC_VARIANT_AUTO) o.bu_variant = (hc_variant)g->tune.bfs_bu_variant;
     if (o.direction < 0 || o.direction > 2) return fail(HC_ERR_INVALID_ARG, "hc_bfs: direction must be 0, 1 or 2");
     if (stats) std::memset(stats, 0, sizeof(*stats));
 

@@ -77,6 +77,9 @@ struct hc_graph {
     hc::DevBuf ws_plan_mssp;
     int32_t mssp_tasks = -1;
 
+    // autotuned launch parameters (zero fields: built-in defaults)
+    hc_tuning tune{};
+
     // workspaces
     hc::DevBuf ws_bfs, ws_sssp, ws_pr, ws_batch, ws_out0, ws_out1, ws_ctl, ws_src;
     hc::PinnedBuf pinned;

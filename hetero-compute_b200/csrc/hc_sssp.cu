@@ -549,6 +549,9 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
     a.plan = g->pr_view;
     a.max_epochs = o.max_epochs > 0 ? o.max_epochs : 0x7fffffff;
     // The pull sweep reads w(u->v) from v's row: only valid when weights are symmetric.
+    // Zero fields: the handle's tuned values, else the defaults.
+    if (o.pull_alpha == 0) o.pull_alpha = g->tune.sssp_pull_alpha;
+    if (o.delta == 0) o.delta = g->tune.sssp_delta;
     a.pull_alpha = !g->w_symmetric ? 0 : (o.pull_alpha == 0 ? kDefaultPullAlpha : std::max(o.pull_alpha, 0));
     if (o.delta == 0) {
         const double davg = g->n_active ? (double)g->M / (double)g->n_active : 1.0;

@@ -80,7 +80,22 @@ GRAPH_AUTO, GRAPH_ON, GRAPH_OFF = 0, 1, 2  # hc_batch_opts.use_graph
 
 
 class BatchOpts(C.Structure):
-    _fields_ = [("group", C.c_int32), ("max_epochs", C.c_int32), ("use_graph", C.c_int32)]
+    _fields_ = [("group", C.c_int32), ("max_epochs", C.c_int32), ("use_graph", C.c_int32),
+                ("switch_alpha", C.c_int32)]
+
+
+class Tuning(C.Structure):
+    """hc_tuning: launch parameters picked by hc_autotune (0 = untuned)."""
+    _fields_ = [("bfs_alpha", C.c_int32), ("bfs_beta", C.c_int32), ("bfs_bu_variant", C.c_int32),
+                ("sssp_delta", C.c_int32), ("sssp_pull_alpha", C.c_int32), ("mbfs_group", C.c_int32),
+                ("mbfs_switch_alpha", C.c_int32), ("mssp_group", C.c_int32), ("mssp_switch_alpha", C.c_int32),
+                ("trials", C.c_int32), ("tune_ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+TUNE_BFS, TUNE_SSSP, TUNE_BFS_BATCHED, TUNE_SSSP_BATCHED, TUNE_ALL = 1, 2, 4, 8, 15
 
 
 class BatchStats(C.Structure):
@@ -116,6 +131,9 @@ _SIGS = {
     "hc_dev_memset": (C.c_int, [_P, C.c_int32, C.c_size_t]),
     "hc_device_synchronize": (C.c_int, []),
     "hc_kernel_launches": (C.c_int64, []),
+    "hc_autotune": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.POINTER(Tuning)]),
+    "hc_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "hc_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "hc_bfs_noalloc": (C.c_int, [_P, _P, C.c_int32, C.c_int64, C.c_int32, _P, _P, _P]),
     "hc_epoch_sssp_pull": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, _P, C.c_int, C.c_int32, C.c_int32, _P]),
     "hc_epoch_pr_pull": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, _P, C.c_int32, _P, C.c_int, C.c_int32,
@@ -361,25 +379,42 @@ class Graph:
                "hc_ppr_batched")
         return scores, st
 
-    def bfs_batched(self, sources, depth=None, *, group=0, max_epochs=0, use_graph=GRAPH_AUTO):
+    def bfs_batched(self, sources, depth=None, *, group=0, max_epochs=0, use_graph=GRAPH_AUTO, switch_alpha=0):
         src = np.ascontiguousarray(sources, dtype=np.int32)
         if depth is None:
             depth = np.empty((len(src), self.num_nodes), dtype=np.int32)
-        o = BatchOpts(group, max_epochs, use_graph)
+        o = BatchOpts(group, max_epochs, use_graph, switch_alpha)
         st = BatchStats()
         _check(lib().hc_bfs_batched(self._h, _ptr(src), len(src), _ptr(depth), C.byref(o), C.byref(st)),
                "hc_bfs_batched")
         return depth, st
 
-    def sssp_batched(self, sources, dist=None, *, group=0, max_epochs=0, use_graph=GRAPH_AUTO):
+    def sssp_batched(self, sources, dist=None, *, group=0, max_epochs=0, use_graph=GRAPH_AUTO, switch_alpha=0):
         src = np.ascontiguousarray(sources, dtype=np.int32)
         if dist is None:
             dist = np.empty((len(src), self.num_nodes), dtype=np.int32)
-        o = BatchOpts(group, max_epochs, use_graph)
+        o = BatchOpts(group, max_epochs, use_graph, switch_alpha)
         st = BatchStats()
         _check(lib().hc_sssp_batched(self._h, _ptr(src), len(src), _ptr(dist), C.byref(o), C.byref(st)),
                "hc_sssp_batched")
         return dist, st
+
+    def autotune(self, sample_sources, what=TUNE_ALL) -> dict:
+        """Times candidate launch parameters on the sample sources and keeps the fastest on the handle."""
+        src = np.ascontiguousarray(sample_sources, dtype=np.int32)
+        t = Tuning()
+        _check(lib().hc_autotune(self._h, _ptr(src), len(src), what, C.byref(t)), "hc_autotune")
+        return t.as_dict()
+
+    @property
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(lib().hc_get_tuning(self._h, C.byref(t)), "hc_get_tuning")
+        return t.as_dict()
+
+    def set_tuning(self, values: dict):
+        t = Tuning(**{k: v for k, v in values.items() if k in dict(Tuning._fields_)})
+        _check(lib().hc_set_tuning(self._h, C.byref(t)), "hc_set_tuning")
 
 
 # --------------------------------------------- reference-shaped entry points

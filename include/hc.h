@@ -265,9 +265,13 @@ hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, const int32_t
 #define HC_GRAPH_OFF 2    /* host loop: one launch sequence and one sync per epoch */
 
 typedef struct hc_batch_opts {
-    int32_t group;        /* sources per group (0 = autotuned / sized to free memory) */
+    int32_t group;        /* sources per group (0 = tuned, else sized to free memory) */
     int32_t max_epochs;   /* 0 = unlimited */
     int32_t use_graph;    /* HC_GRAPH_AUTO / _ON / _OFF */
+    int32_t switch_alpha; /* direction switch (0 = tuned / default, < 0 = never switch):
+                             BFS pushes while frontier edges * alpha < M (default 10),
+                             else pulls; < 0 pulls every level.  SSSP pulls when the
+                             queue's edges * alpha > M (default 2); < 0 pushes only. */
 } hc_batch_opts;
 
 typedef struct hc_batch_stats {
@@ -289,6 +293,43 @@ hc_status hc_bfs_batched(hc_graph *g, const int32_t *sources, int32_t num_source
 hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_t num_sources,
                           int32_t *dist_out, const hc_batch_opts *opts,
                           hc_batch_stats *stats);
+
+/* ------------------------------------------------------------- autotuner */
+
+/* Launch parameters of one graph, picked by hc_autotune.  A zero field in an
+ * opts struct (hc_bfs_opts.alpha, hc_sssp_opts.delta, hc_batch_opts.group ...)
+ * means "the tuned value", or the built-in default while a field is untuned
+ * (zero here).  No counterpart in the reference, whose variant and launch
+ * shape are chosen by hand per call (src/kernels/gpu/bfs.cuh:352-360). */
+typedef struct hc_tuning {
+    int32_t bfs_alpha;          /* hc_bfs_opts.alpha */
+    int32_t bfs_beta;           /* hc_bfs_opts.beta */
+    int32_t bfs_bu_variant;     /* hc_bfs_opts.bu_variant (HC_VARIANT_AUTO = untuned) */
+    int32_t sssp_delta;         /* hc_sssp_opts.delta */
+    int32_t sssp_pull_alpha;    /* hc_sssp_opts.pull_alpha */
+    int32_t mbfs_group;         /* hc_bfs_batched group */
+    int32_t mbfs_switch_alpha;  /* hc_bfs_batched switch_alpha */
+    int32_t mssp_group;         /* hc_sssp_batched group */
+    int32_t mssp_switch_alpha;  /* hc_sssp_batched switch_alpha */
+    int32_t trials;             /* candidates timed by the last hc_autotune */
+    double tune_ms;             /* device time spent on them */
+} hc_tuning;
+
+#define HC_TUNE_BFS 1u
+#define HC_TUNE_SSSP 2u
+#define HC_TUNE_BFS_BATCHED 4u
+#define HC_TUNE_SSSP_BATCHED 8u
+#define HC_TUNE_ALL 15u
+
+/* Times candidate parameters on the sample sources (CUDA events, outputs
+ * discarded) by coordinate descent, one parameter at a time from the current
+ * values, and stores the fastest on the handle; `out` (optional) receives the
+ * result.  The batched searches run on up to 256 / 512 of the samples. */
+hc_status hc_autotune(hc_graph *g, const int32_t *sample_sources, int32_t num_samples,
+                      uint32_t what, hc_tuning *out);
+/* Reads / replaces the handle's tuning (e.g. one saved from an earlier run). */
+hc_status hc_get_tuning(const hc_graph *g, hc_tuning *out);
+hc_status hc_set_tuning(hc_graph *g, const hc_tuning *t);
 
 /* ------------------------------------------------------ device memory */
 /* Plain device-memory helpers so hosts that drive the epoch kernels below

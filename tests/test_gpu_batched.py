@@ -19,6 +19,16 @@ def test_bfs_batched_depths(scale, k):
         assert np.array_equal(depth[i], oracle.bfs_depth(host.index, host.neighbors, s)), i
 
 
+@pytest.mark.parametrize("switch_alpha", [-1, 1000000])
+def test_bfs_batched_pull_only_and_push_mostly(switch_alpha):
+    host = hc.gen_kronecker(13, 16, 33)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, 70)
+    depth, _ = g.bfs_batched(src, group=128, switch_alpha=switch_alpha)
+    for i in range(0, 70, 7):
+        assert np.array_equal(depth[i], oracle.bfs_depth(host.index, host.neighbors, src[i])), i
+
+
 def test_bfs_batched_groups_and_duplicates():
     host = hc.gen_kronecker(11, 8, 2)
     g = hc.Graph.from_host(host)
@@ -71,14 +81,13 @@ def test_sssp_batched_group_widths(group):
     assert np.array_equal(dd.cpu().numpy(), dist)
 
 
-@pytest.mark.parametrize("pull_alpha", ["0", "2", "1000000"])
-def test_sssp_batched_push_and_pull_epochs(monkeypatch, pull_alpha):
+@pytest.mark.parametrize("switch_alpha", [-1, 0, 1000000])
+def test_sssp_batched_push_and_pull_epochs(switch_alpha):
     """Push only, the default switch, and pull for every epoch."""
-    monkeypatch.setenv("HC_MSSP_PULL_ALPHA", pull_alpha)
     big = hc.gen_kronecker(16, 16, 3, wtype=hc.W_I32)  # rows above the chunk size
     g = hc.Graph.from_host(big)
     src = hc.pick_sources(big, 70)
-    dist, _ = g.sssp_batched(src, group=64)
+    dist, _ = g.sssp_batched(src, group=64, switch_alpha=switch_alpha)
     for i in range(0, 70, 9):
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(big.index, big.neighbors, big.weights, src[i])), i
 
