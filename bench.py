@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--cpu-budget-s", type=float, default=20.0)
     p.add_argument("--mode", choices=["bench", "profile"], default="bench",
                    help="profile: one BFS, one SSSP and one PageRank solve, untimed (for ncu captures)")
-    p.add_argument("--suite", choices=["plain", "batched", "adjoint", "grid"], default="plain",
+    p.add_argument("--suite", choices=["plain", "batched", "adjoint", "grid", "roofline"], default="plain",
                    help="batched: 512 BFS / 512 SSSP sources and 256 PPR columns in batched launches vs "
                         "sequential plain launches (Kronecker scale 24); adjoint: PageRank forward vs "
                         "forward + adjoint (scale 24, fp32 weights, and an Erdos-Renyi 2^24 graph); "
@@ -83,7 +83,7 @@ def run_suite(a):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    scale = a.scale if a.scale != 22 else 24
+    scale = a.scale if a.scale != 22 else (25 if a.suite == "roofline" else 24)
     out = {"suite": a.suite, "metric": METRIC, "unit": "GTEPS", "data": "synthetic", "warmup": a.warmup,
            "steps": a.steps}
     t0 = time.time()
@@ -183,6 +183,46 @@ def run_suite(a):
         out["adjoint"] = res
         out["value"] = res["kronecker"]["ratio"]
         out["unit"] = "forward+adjoint / forward"
+    elif a.suite == "roofline":
+        # Plain BFS / SSSP / PageRank on one large Kronecker graph: GTEPS and
+        # the bytes model of each call against the measured HBM peak.
+        host = hc.gen_kronecker(scale, a.edge_factor, a.seed, hc.W_I32)
+        gen_s = time.time() - t0
+        g = hc.Graph.from_host(host)
+        g.set_stream(stream.cuda_stream)
+        n, m = host.num_nodes, host.num_edges
+        src = hc.pick_sources(host, 16)
+        del host
+        tuning = g.autotune(src, hc.TUNE_BFS | hc.TUNE_SSSP) if a.tune else None
+        depth = torch.empty((16, n), dtype=torch.int32, device=dev)
+        parent = torch.empty((16, n), dtype=torch.int32, device=dev)
+        scores = torch.empty(n, dtype=torch.float32, device=dev)
+        hbm, peak_kind = peaks()
+        res = {}
+        for name, call, runs in [
+                ("bfs", lambda st=False: g.bfs(src, depth, parent, stats=st)[2], 16),
+                ("sssp", lambda st=False: g.sssp(src[:8], depth[:8], stats=st)[2], 8),
+                ("pagerank", lambda st=False: g.pagerank(None, scores, tol_l1=1e-4, max_iters=50)[1], 1)]:
+            for _ in range(max(1, a.warmup)):
+                call()
+            ms = _time_cuda(call, torch, dev, max(1, a.steps))
+            st = call(True)  # instrumented pass: bytes model and device time of the launches
+            res[name] = {"ms": ms, "gteps": runs * (m / 2) / ms / 1e6, "runs": runs, "kernel_ms": st.ms,
+                         "bytes_model": st.bytes_model,
+                         "achieved_gbs": st.bytes_model / (st.ms / 1e3) / 1e9 if st.ms else None}
+            res[name]["frac"] = res[name]["achieved_gbs"] / hbm if res[name]["achieved_gbs"] else None
+        res["pagerank"]["iterations"] = int(st.iterations)
+        # One pass over the CSR (offsets + neighbours + weights), the floor of any full sweep.
+        one_pass = 8.0 * (n + 1) + 4.0 * m
+        res["pagerank"]["per_iteration_ms"] = res["pagerank"]["kernel_ms"] / max(1, int(st.iterations))
+        res["pagerank"]["one_pass_ms_at_peak"] = one_pass / (hbm * 1e9) * 1e3
+        out["config"] = {"workload": f"kronecker-s{scale}-ef{a.edge_factor}: bfs x16, sssp x8, pagerank "
+                                     f"(d=0.85, L1 tol 1e-4, max 50)", "num_nodes": n, "num_edges": m,
+                         "graph_gen_s": gen_s, "peak_gbs": hbm, "peak_kind": peak_kind}
+        out["tuning"] = tuning
+        out["roofline"] = res
+        out["value"] = res["pagerank"]["frac"]
+        out["unit"] = "fraction of measured HBM peak (pagerank)"
     else:
         host = hc.gen_grid(4096, 4096, a.seed, hc.W_I32)
         g = hc.Graph.from_host(host)

@@ -160,27 +160,41 @@ __global__ void __launch_bounds__(kPrThreads) pr_sweep(SweepArgs a, PrPlanDev pl
             const int32_t gend = (int32_t)(a.index[min(r0 + 32, a.n_active)] - s0);
             s_acc[wib][lane] = 0.f;
             __syncwarp();
-            for (int k0 = 0; k0 < gend; k0 += 32) {
-                const int k = k0 + lane;
-                const bool act = k < gend;
-                int lo = 0;
+            // Four 32-edge chunks per pass: their loads and gathers are issued
+            // together, then each chunk is summed by its segmented scan in the
+            // same order as one chunk at a time.
+            for (int k0 = 0; k0 < gend; k0 += 128) {
+                float vals[4];
 #pragma unroll
-                for (int st = 16; st > 0; st >>= 1) {
-                    const int c = __shfl_sync(kFull, rel, lo + st);
-                    if (c <= k) lo += st;
+                for (int j = 0; j < 4; j++) {
+                    const int k = k0 + 32 * j + lane;
+                    vals[j] = k < gend ? edge_val<kEW>(a, s0 + k) : 0.f;
                 }
-                int owner = act ? lo : 32;
-                float v = act ? edge_val<kEW>(a, s0 + k) : 0.f;
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const float y = __shfl_up_sync(kFull, v, o);
-                    const int ow = __shfl_up_sync(kFull, owner, o);
-                    if (lane >= o && ow == owner) v += y;
+                for (int j = 0; j < 4; j++) {
+                    const int kb = k0 + 32 * j;
+                    if (kb >= gend) break;
+                    const int k = kb + lane;
+                    const bool act = k < gend;
+                    int lo = 0;
+#pragma unroll
+                    for (int st = 16; st > 0; st >>= 1) {
+                        const int c = __shfl_sync(kFull, rel, lo + st);
+                        if (c <= k) lo += st;
+                    }
+                    int owner = act ? lo : 32;
+                    float v = vals[j];
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const float y = __shfl_up_sync(kFull, v, o);
+                        const int ow = __shfl_up_sync(kFull, owner, o);
+                        if (lane >= o && ow == owner) v += y;
+                    }
+                    const int next_owner = __shfl_down_sync(kFull, owner, 1);
+                    const bool tail = (lane == 31) || next_owner != owner;
+                    if (act && tail) s_acc[wib][owner] += v;
+                    __syncwarp();
                 }
-                const int next_owner = __shfl_down_sync(kFull, owner, 1);
-                const bool tail = (lane == 31) || next_owner != owner;
-                if (act && tail) s_acc[wib][owner] += v;
-                __syncwarp();
             }
             if (r < a.n_active) finish_row<kEW, kRS, kPS, kBaseVec>(a, r, s_acc[wib][lane], l1, chg);
             __syncwarp();

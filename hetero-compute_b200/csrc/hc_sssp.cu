@@ -20,6 +20,7 @@
 // changed bitmap uint32[N/32] (pull sweeps); tasks int2[] for long rows.
 #include <algorithm>
 #include <climits>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -31,11 +32,18 @@ namespace hc {
 namespace {
 
 constexpr int kSsspThreads = 512;
+constexpr int kPullThreads = 256;
 constexpr int kTraceEpochs = 96;
 constexpr int kDefaultPullAlpha = 4;
 
 struct SsspCtl {
     GridSync gs;
+    // Pull epochs run as a separate kernel (sssp_pull_kernel): the persistent
+    // kernel saves its loop state here and exits with need_pull set, and the
+    // next launch (resume set) folds the lowered rows into its queues.
+    int need_pull, resume;
+    int saved_E, saved_phase, saved_pulls, saved_T;
+    unsigned long long t_start;
     int qlen[3];
     int tasks[3];
     unsigned long long mf[3];  // degree sum of each near queue
@@ -121,8 +129,13 @@ struct RelaxVisit {
     }
 };
 
+// The gather goes through L1 (.ca): most edges point at a few thousand hub
+// rows, whose distances then stay on the SM.  A value cached earlier in the
+// same sweep can be stale, but distances only fall, so it is an upper bound,
+// and the row that lowered it is marked changed and relaxed again next epoch;
+// the grid barrier's fence invalidates L1 between epochs.
 __device__ __forceinline__ int32_t pull_val(const SsspArgs &a, int64_t e) {
-    const int32_t du = __ldcg(a.dist + a.nbr[e]);
+    const int32_t du = __ldca(a.dist + a.nbr[e]);
     return du == kInfDist ? kInfDist : du + a.w[e];
 }
 
@@ -176,26 +189,40 @@ __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwa
             const int32_t gend = (int32_t)(a.index[min(r0 + 32, a.n_active)] - s0);
             s_acc[wib][lane] = kInfDist;
             __syncwarp();
-            for (int k0 = 0; k0 < gend; k0 += 32) {
-                const int k = k0 + lane;
-                const bool act = k < gend;
-                int lo = 0;
+            // Four 32-edge chunks per pass: their loads and gathers are issued
+            // together, then each chunk is reduced by its segmented scan.
+            for (int k0 = 0; k0 < gend; k0 += 128) {
+                int32_t vals[4];
 #pragma unroll
-                for (int st = 16; st > 0; st >>= 1) {
-                    const int c = __shfl_sync(kFull, rel, lo + st);
-                    if (c <= k) lo += st;
+                for (int j = 0; j < 4; j++) {
+                    const int k = k0 + 32 * j + lane;
+                    vals[j] = k < gend ? pull_val(a, s0 + k) : kInfDist;
                 }
-                const int owner = act ? lo : 32;
-                int32_t v = act ? pull_val(a, s0 + k) : kInfDist;
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int32_t y = __shfl_up_sync(kFull, v, o);
-                    const int ow = __shfl_up_sync(kFull, owner, o);
-                    if (lane >= o && ow == owner) v = min(v, y);
+                for (int j = 0; j < 4; j++) {
+                    const int kb = k0 + 32 * j;
+                    if (kb >= gend) break;
+                    const int k = kb + lane;
+                    const bool act = k < gend;
+                    int lo = 0;
+#pragma unroll
+                    for (int st = 16; st > 0; st >>= 1) {
+                        const int c = __shfl_sync(kFull, rel, lo + st);
+                        if (c <= k) lo += st;
+                    }
+                    const int owner = act ? lo : 32;
+                    int32_t v = vals[j];
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int32_t y = __shfl_up_sync(kFull, v, o);
+                        const int ow = __shfl_up_sync(kFull, owner, o);
+                        if (lane >= o && ow == owner) v = min(v, y);
+                    }
+                    const int next_owner = __shfl_down_sync(kFull, owner, 1);
+                    if (act && (lane == 31 || next_owner != owner))
+                        s_acc[wib][owner] = min(s_acc[wib][owner], v);
+                    __syncwarp();
                 }
-                const int next_owner = __shfl_down_sync(kFull, owner, 1);
-                if (act && (lane == 31 || next_owner != owner)) s_acc[wib][owner] = min(s_acc[wib][owner], v);
-                __syncwarp();
             }
             const int32_t m = s_acc[wib][lane];
             bool ch = false;
@@ -214,10 +241,9 @@ __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwa
 }
 
 template <bool kStats>
-__global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
+__global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
     __shared__ unsigned long long s_red[32];
     __shared__ int s_min[32];
-    __shared__ int32_t s_acc[kSsspThreads / 32][32];
     SsspCtl *ctl = a.ctl;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthreads = gridDim.x * blockDim.x;
@@ -225,33 +251,82 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
     const int lane = threadIdx.x & 31;
     const int W_act = (a.n_active + 31) >> 5;
 
-    for (int i = gtid; i < a.n; i += nthreads) {
-        a.dist[i] = kInfDist;
-        a.stamp[i] = -1;
-        a.fstamp[i] = -1;
-    }
-    for (int i = gtid; i < W_act; i += nthreads) a.changed[i] = 0;
-    const unsigned long long t_start = globaltimer_ns();
-    if (!grid_barrier(&ctl->gs)) return;
-    if (gtid == 0) {
-        a.dist[a.src] = 0;
-        a.stamp[a.src] = 0;
-        a.q0[0] = a.src;
-        ctl->qlen[0] = 1;
-        ctl->mf[0] = (unsigned long long)(a.index[a.src + 1] - a.index[a.src]);
-        ctl->min_far = kInfDist;
-    }
-    if (!grid_barrier(&ctl->gs)) return;
-
     const bool use_far = a.delta > 0;
     int32_t T = use_far ? a.delta : kInfDist;
     int E = 0, phase = 0, pulls = 0;
     unsigned long long my_v = 0, my_e = 0;
+    // Every block reads the same control words (written before this launch).
+    const bool resumed = __ldcg(&ctl->resume) != 0;
+    unsigned long long t_start;
+    if (!resumed) {
+        for (int i = gtid; i < a.n; i += nthreads) {
+            a.dist[i] = kInfDist;
+            a.stamp[i] = -1;
+            a.fstamp[i] = -1;
+        }
+        for (int i = gtid; i < W_act; i += nthreads) a.changed[i] = 0;
+        t_start = globaltimer_ns();
+        if (gtid == 0) ctl->t_start = t_start;
+        if (!grid_barrier(&ctl->gs)) return;
+        if (gtid == 0) {
+            a.dist[a.src] = 0;
+            a.stamp[a.src] = 0;
+            a.q0[0] = a.src;
+            ctl->qlen[0] = 1;
+            ctl->mf[0] = (unsigned long long)(a.index[a.src + 1] - a.index[a.src]);
+            ctl->min_far = kInfDist;
+        }
+        if (!grid_barrier(&ctl->gs)) return;
+    } else {
+        E = __ldcg(&ctl->saved_E);
+        phase = __ldcg(&ctl->saved_phase);
+        pulls = __ldcg(&ctl->saved_pulls);
+        T = __ldcg(&ctl->saved_T);
+        t_start = __ldcg(&ctl->t_start);
+        if (!grid_barrier(&ctl->gs)) return;  // everyone has read the saved state
+        if (gtid == 0) ctl->need_pull = 0;
+    }
+    bool after_pull = resumed;  // epoch E's pull sweep ran in sssp_pull_kernel
 
     for (;;) {
         const int cur = E % 3, nxt = (E + 1) % 3, old = (E + 2) % 3;
         int32_t *qcur = (E & 1) ? a.q1 : a.q0;
         int32_t *qnext = (E & 1) ? a.q0 : a.q1;
+        const int next_e = E + 1;
+        if (after_pull) {
+            after_pull = false;
+            int32_t *fpile = (phase & 1) ? a.far1 : a.far0;
+            int *fpile_len = &ctl->far_len[phase & 1];
+            // Lowered vertices back into the near queue / far pile.
+            unsigned long long mf_next = 0;
+            for (int w0 = gwarp * 32; w0 < W_act; w0 += nwarps * 32) {
+                const int w = w0 + lane;
+                uint32_t bits = 0;
+                if (w < W_act) {
+                    bits = __ldcg(a.changed + w);
+                    if (bits) a.changed[w] = 0;
+                }
+                while (__any_sync(kFull, bits != 0)) {
+                    bool near = false, far = false;
+                    int32_t v = 0;
+                    if (bits) {
+                        v = w * 32 + __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        const int32_t d = __ldcg(a.dist + v);
+                        if (d < T) near = atomicMax(a.stamp + v, next_e) < next_e;
+                        else far = atomicMax(a.fstamp + v, phase + 1) < phase + 1;
+                        if (near) mf_next += (unsigned long long)(a.index[v + 1] - a.index[v]);
+                    }
+                    warp_append(near, v, qnext, &ctl->qlen[nxt]);
+                    if (use_far) warp_append(far, v, fpile, fpile_len);
+                }
+            }
+            mf_next = block_sum(mf_next, s_red);
+            if (threadIdx.x == 0 && mf_next) atomicAdd(&ctl->mf[nxt], mf_next);
+            if (!grid_barrier(&ctl->gs)) return;
+            E++;
+            continue;
+        }
         if (gtid == 0 && globaltimer_ns() - t_start > kRunLimitNs) atomicExch(&ctl->gs.err, (int)HC_ERR_TIMEOUT);
         int nq = __ldcg(&ctl->qlen[cur]);
         if (nq == 0) {
@@ -316,9 +391,9 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
             ctl->tasks[old] = 0;
             ctl->mf[old] = 0;
         }
+        // After the far split above: `phase` may have advanced.
         int32_t *fpile = (phase & 1) ? a.far1 : a.far0;
         int *fpile_len = &ctl->far_len[phase & 1];
-        const int next_e = E + 1;
         const unsigned long long mfc = __ldcg(&ctl->mf[cur]);
         const bool pull = a.pull_alpha > 0 && (double)mfc * (double)a.pull_alpha > (double)a.m;
         if (gtid == 0 && E < kTraceEpochs) {
@@ -328,36 +403,16 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
         }
         if (kStats && gtid == 0) my_v += nq;
         if (pull) {
-            pulls++;
-            pull_sweep<kStats>(a, gwarp, nwarps, s_acc, my_e);
-            if (!grid_barrier(&ctl->gs)) return;
-            // Lowered vertices back into the near queue / far pile.
-            unsigned long long mf_next = 0;
-            for (int w0 = gwarp * 32; w0 < W_act; w0 += nwarps * 32) {
-                const int w = w0 + lane;
-                uint32_t bits = 0;
-                if (w < W_act) {
-                    bits = __ldcg(a.changed + w);
-                    if (bits) a.changed[w] = 0;
-                }
-                while (__any_sync(kFull, bits != 0)) {
-                    bool near = false, far = false;
-                    int32_t v = 0;
-                    if (bits) {
-                        v = w * 32 + __ffs(bits) - 1;
-                        bits &= bits - 1;
-                        const int32_t d = __ldcg(a.dist + v);
-                        if (d < T) near = atomicMax(a.stamp + v, next_e) < next_e;
-                        else far = atomicMax(a.fstamp + v, phase + 1) < phase + 1;
-                        if (near) mf_next += (unsigned long long)(a.index[v + 1] - a.index[v]);
-                    }
-                    warp_append(near, v, qnext, &ctl->qlen[nxt]);
-                    if (use_far) warp_append(far, v, fpile, fpile_len);
-                }
+            // Hand the epoch to sssp_pull_kernel and resume after it.
+            if (gtid == 0) {
+                ctl->saved_E = E;
+                ctl->saved_phase = phase;
+                ctl->saved_pulls = pulls + 1;
+                ctl->saved_T = T;
+                ctl->resume = 1;
+                ctl->need_pull = 1;
             }
-            mf_next = block_sum(mf_next, s_red);
-            if (threadIdx.x == 0 && mf_next) atomicAdd(&ctl->mf[nxt], mf_next);
-            if (!grid_barrier(&ctl->gs)) return;
+            break;
         } else {
             RelaxVisit relax{a.index, a.nbr, a.w, a.dist, a.stamp, a.fstamp, qnext, &ctl->qlen[nxt], fpile,
                              fpile_len, T, next_e, phase + 1, use_far, 0ull, 0ull};
@@ -383,11 +438,27 @@ __global__ void __launch_bounds__(kSsspThreads) sssp_persistent(SsspArgs a) {
         unsigned long long e = block_sum(my_e, s_red);
         if (threadIdx.x == 0 && e) atomicAdd(&ctl->erelax, e);
     }
-    if (gtid == 0) {
+    if (gtid == 0 && !__ldcg(&ctl->need_pull)) {
         ctl->epochs = E;
         ctl->phases = phase;
         ctl->pulls = pulls;
         ctl->trace[E < kTraceEpochs ? E : kTraceEpochs].t_ns = globaltimer_ns();
+    }
+}
+
+// One pull epoch (the reference's Bellman-Ford epoch) as its own launch, so
+// that it runs at the occupancy of a small kernel instead of the persistent
+// kernel's; lowered rows are marked in `changed`.
+template <bool kStats>
+__global__ void __launch_bounds__(kPullThreads) sssp_pull_kernel(SsspArgs a) {
+    __shared__ int32_t s_acc[kPullThreads / 32][32];
+    __shared__ unsigned long long s_red[32];
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long my_e = 0;
+    pull_sweep<kStats>(a, gtid >> 5, (gridDim.x * blockDim.x) >> 5, s_acc, my_e);
+    if (kStats) {
+        const unsigned long long e = block_sum(my_e, s_red);
+        if (threadIdx.x == 0 && e) atomicAdd(&a.ctl->erelax, e);
     }
 }
 
@@ -466,6 +537,38 @@ hc_status launch_sssp(hc_graph *g, const SsspArgs &args) {
     ::hc::count_launch();
     HC_CUDA_TRY(cudaLaunchCooperativeKernel((void *)sssp_persistent<kStats>, grid, block, params, 0, g->stream));
     return HC_OK;
+}
+
+template <bool kStats>
+hc_status launch_pull(hc_graph *g, const SsspArgs &a) {
+    static int blocks_per_sm[2] = {0, 0};
+    int &bps = blocks_per_sm[kStats ? 1 : 0];
+    if (bps == 0) {
+        HC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sssp_pull_kernel<kStats>, kPullThreads, 0));
+        if (bps < 1) return fail(HC_ERR_CUDA, "SSSP pull kernel cannot be resident");
+    }
+    ::hc::count_launch();
+    sssp_pull_kernel<kStats><<<g->sm_count * bps, kPullThreads, 0, g->stream>>>(a);
+    HC_CUDA_TRY(cudaGetLastError());
+    return HC_OK;
+}
+
+// One source: the persistent kernel, and for each pull epoch it hands back,
+// the pull kernel and another persistent launch that resumes the loop.
+template <bool kStats>
+hc_status run_source(hc_graph *g, const SsspArgs &a, volatile int *h_flags) {
+    for (int round = 0;; round++) {
+        HC_TRY(launch_sssp<kStats>(g, a));
+        if (a.pull_alpha <= 0) return HC_OK;  // no pull epochs: one launch
+        // gs.err and need_pull, adjacent at the head of SsspCtl.
+        HC_CUDA_TRY(cudaMemcpyAsync((void *)h_flags, a.ctl, offsetof(SsspCtl, resume), cudaMemcpyDeviceToHost,
+                                    g->stream));
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        const SsspCtl *hc = (const SsspCtl *)h_flags;
+        if (hc->gs.err || !hc->need_pull) return HC_OK;
+        if (round > a.max_epochs) return fail(HC_ERR_NOT_CONVERGED, "hc_sssp: pull rounds exceed the epoch cap");
+        HC_TRY(launch_pull<kStats>(g, a));
+    }
 }
 
 }  // namespace
@@ -565,13 +668,15 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
     if (!dev_dist) HC_TRY(g->ws_out0.ensure(4 * n));
     if (parent_out && !dev_parent) HC_TRY(g->ws_out1.ensure(4 * n));
 
+    HC_TRY(g->pinned.ensure(sizeof(SsspCtl)));
+    volatile int *h_flags = g->pinned.as<int>();
     double total_ms = 0;
     for (int32_t i = 0; i < num_sources; i++) {
         a.src = src[i];
         a.dist = dev_dist ? dist_out + (size_t)i * n : g->ws_out0.as<int32_t>();
         HC_CUDA_TRY(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), g->stream));
         HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
-        HC_TRY(o.collect_stats ? launch_sssp<true>(g, a) : launch_sssp<false>(g, a));
+        HC_TRY(o.collect_stats ? run_source<true>(g, a, h_flags) : run_source<false>(g, a, h_flags));
         HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
         if (parent_out) {
             int32_t *par = dev_parent ? parent_out + (size_t)i * n : g->ws_out1.as<int32_t>();
