@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--cpu-budget-s", type=float, default=20.0)
     p.add_argument("--mode", choices=["bench", "profile"], default="bench",
                    help="profile: one BFS, one SSSP and one PageRank solve, untimed (for ncu captures)")
-    p.add_argument("--suite", choices=["plain", "batched", "adjoint", "grid", "roofline"], default="plain",
+    p.add_argument("--suite", choices=["plain", "batched", "adjoint", "grid", "roofline", "large"], default="plain",
                    help="batched: 512 BFS / 512 SSSP sources and 256 PPR columns in batched launches vs "
                         "sequential plain launches (Kronecker scale 24); adjoint: PageRank forward vs "
                         "forward + adjoint (scale 24, fp32 weights, and an Erdos-Renyi 2^24 graph); "
@@ -83,7 +83,7 @@ def run_suite(a):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    scale = a.scale if a.scale != 22 else (25 if a.suite == "roofline" else 24)
+    scale = a.scale if a.scale != 22 else {"roofline": 25, "large": 27}.get(a.suite, 24)
     out = {"suite": a.suite, "metric": METRIC, "unit": "GTEPS", "data": "synthetic", "warmup": a.warmup,
            "steps": a.steps}
     t0 = time.time()
@@ -183,6 +183,69 @@ def run_suite(a):
         out["adjoint"] = res
         out["value"] = res["kronecker"]["ratio"]
         out["unit"] = "forward+adjoint / forward"
+    elif a.suite == "large":
+        # One graph resident in HBM (int32 weights [1,255]): BFS and SSSP from
+        # 64 sources, one batched 128-source BFS, PageRank forward + adjoint
+        # (the int32 weights as fp32), each as GTEPS and the bytes model
+        # against the measured HBM peak.
+        host = hc.gen_kronecker(scale, a.edge_factor, a.seed, hc.W_I32)
+        gen_s = time.time() - t0
+        g = hc.Graph.from_host(host)
+        g.set_stream(stream.cuda_stream)
+        n, m = host.num_nodes, host.num_edges
+        src = hc.pick_sources(host, 128)
+        del host
+        hbm, peak_kind = peaks()
+        tuning = g.autotune(src[:64], hc.TUNE_BFS | hc.TUNE_SSSP) if a.tune else None
+        res = {}
+
+        def record(name, ms, runs, st=None):
+            r = {"ms": ms, "runs": runs, "gteps": runs * (m / 2) / ms / 1e6}
+            if st is not None and st.ms:
+                r["bytes_model"] = st.bytes_model
+                r["achieved_gbs"] = st.bytes_model / (st.ms / 1e3) / 1e9
+                r["frac"] = r["achieved_gbs"] / hbm
+            res[name] = r
+        out4 = torch.empty((4, n), dtype=torch.int32, device=dev)
+        par4 = torch.empty((4, n), dtype=torch.int32, device=dev)
+        out_i, par = out4[:1], par4[:1]
+        s64 = src[:64]
+        g.bfs(s64[:2], out4[:2], par4[:2])
+        ms = _time_cuda(lambda: [g.bfs(s64[i:i + 1], out_i, par) for i in range(64)], torch, dev, 1)
+        record("bfs_x64", ms, 64, g.bfs(s64[:4], out4, par4, stats=True)[2])
+        g.sssp(s64[:1], out_i)
+        ms = _time_cuda(lambda: [g.sssp(s64[i:i + 1], out_i) for i in range(64)], torch, dev, 1)
+        record("sssp_x64", ms, 64, g.sssp(s64[:4], out4, stats=True)[2])
+        depth = torch.empty((128, n), dtype=torch.int32, device=dev)
+        g.bfs_batched(src[:64], depth[:64])
+        ms = _time_cuda(lambda: g.bfs_batched(src, depth), torch, dev, 1)
+        _, bst = g.bfs_batched(src, depth)
+        record("bfs_batched_x128", ms, 128, bst)
+        del depth, out_i, par, out4, par4
+        x = torch.empty(n, dtype=torch.float32, device=dev)
+        rng = np.random.default_rng(a.seed)
+        c = torch.from_numpy(rng.standard_normal(n).astype(np.float32)).to(dev)
+        dt = torch.empty(n, dtype=torch.float32, device=dev)
+        dw = torch.empty(m, dtype=torch.float32, device=dev)
+        popts = dict(tol_l1=1e-6, max_iters=200, weighted=True)
+        g.pagerank(None, x, **popts)
+        tf = _time_cuda(lambda: g.pagerank(None, x, **popts), torch, dev, 1)
+        _, fst = g.pagerank(None, x, **popts)
+        tb = _time_cuda(lambda: g.pagerank_backward(x, c, dteleport=dt, dweights=dw, **popts), torch, dev, 1)
+        _, _, bst2 = g.pagerank_backward(x, c, dteleport=dt, dweights=dw, **popts)
+        record("pagerank_forward", tf, 1, fst)
+        res["pagerank_forward"]["iterations"] = int(fst.iterations)
+        record("pagerank_adjoint", tb, 1, bst2)
+        res["pagerank_adjoint"]["iterations"] = int(bst2.iterations)
+        res["pagerank_forward_plus_adjoint_over_forward"] = (tf + tb) / tf
+        out["config"] = {"workload": f"kronecker-s{scale}-ef{a.edge_factor} int32 weights [1,255] resident in HBM: "
+                                     f"bfs x64, sssp x64, batched bfs x128, weighted pagerank forward + adjoint "
+                                     f"(L1 tol 1e-6, max 200)", "num_nodes": n, "num_edges": m,
+                         "graph_gen_s": gen_s, "device_bytes_held": int(g.info().device_bytes),
+                         "peak_gbs": hbm, "peak_kind": peak_kind}
+        out["tuning"] = tuning
+        out["large"] = res
+        out["value"] = res["bfs_batched_x128"]["gteps"]
     elif a.suite == "roofline":
         # Plain BFS / SSSP / PageRank on one large Kronecker graph: GTEPS and
         # the bytes model of each call against the measured HBM peak.

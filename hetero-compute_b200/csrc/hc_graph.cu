@@ -146,6 +146,11 @@ __global__ void build_inv_wsum(const int64_t *index, const float *w, int32_t n, 
     }
 }
 
+__global__ void weights_to_f32(const int32_t *w, size_t n, float *out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (float)w[i];
+}
+
 // wtn[slot (v,i)] = w[u -> v] / sum_k w[u -> k] with u = nbr[v][i]: the weight
 // the forward pull at v needs, stored in v's own row so the pull streams it.
 // Rows are sorted, so the reverse slot is found by binary search in row u.
@@ -174,6 +179,56 @@ __global__ void build_wtn(const int64_t *index, const int32_t *nbr, const float 
 
 }  // namespace
 
+// Flags an edge without its reverse (missing) or whose reverse carries a
+// different weight (wdiff).  Rows are sorted, so the reverse slot is found by
+// binary search in row u.
+__global__ void check_symmetry(const int64_t *index, const int32_t *nbr, const float *w, int32_t n, int *missing,
+                               int *wdiff) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const int64_t b = index[v], e = index[v + 1];
+        for (int64_t i = b + lane; i < e; i += 32) {
+            const int32_t u = nbr[i];
+            int64_t lo = index[u], hi = index[u + 1];
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (nbr[mid] < v) lo = mid + 1; else hi = mid;
+            }
+            if (lo >= index[u + 1] || nbr[lo] != v) *missing = 1;
+            else if (w && w[lo] != w[i]) *wdiff = 1;
+        }
+    }
+}
+
+hc_status ensure_pr_symmetry(hc_graph *g, bool weighted, bool *symmetric) {
+    if (g->pr_sym_struct < 0 || (weighted && g->pr_sym_w < 0)) {
+        if (!g->rows_sorted) {
+            g->pr_sym_struct = 0;
+            g->pr_sym_w = 0;
+        } else {
+            const float *w = weighted ? pr_weights(g) : nullptr;
+            DevBuf flags;
+            HC_TRY(flags.ensure(2 * sizeof(int)));
+            HC_CUDA_TRY(cudaMemsetAsync(flags.ptr, 0, 2 * sizeof(int), g->stream));
+            { check_symmetry<<<g->sm_count * 8, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), w,
+                                                                     g->N, flags.as<int>(), flags.as<int>() + 1); ::hc::count_launch(); }
+            HC_CUDA_TRY(cudaGetLastError());
+            int h[2] = {0, 0};
+            HC_CUDA_TRY(cudaMemcpyAsync(h, flags.ptr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            g->pr_sym_struct = !h[0];
+            if (weighted) g->pr_sym_w = !h[0] && !h[1];
+        }
+    }
+    *symmetric = weighted ? g->pr_sym_w == 1 : g->pr_sym_struct == 1;
+    return HC_OK;
+}
+
+const float *pr_weights(const hc_graph *g) {
+    return g->wtype == HC_W_I32 ? g->wf32.as<float>() : g->wgt.as<float>();
+}
+
 hc_status ensure_pr_derived(hc_graph *g, bool weighted) {
     const int grid = g->sm_count * 8, block = 256;
     if (!g->inv_deg.ptr) {
@@ -182,18 +237,24 @@ hc_status ensure_pr_derived(hc_graph *g, bool weighted) {
         HC_CUDA_TRY(cudaGetLastError());
     }
     if (weighted && !g->wtn.ptr) {
-        if (g->wtype != HC_W_F32)
-            return fail(HC_ERR_UNSUPPORTED, "weighted PageRank needs fp32 edge weights");
+        if (g->wtype == HC_W_NONE) return fail(HC_ERR_UNSUPPORTED, "weighted PageRank needs edge weights");
+        if (g->wtype == HC_W_I32 && !g->wf32.ptr) {
+            // Exact for |w| < 2^24 (the generators' int32 weights are in [1, 255]).
+            HC_TRY(g->wf32.ensure(sizeof(float) * (size_t)(g->M + kNbrPad)));
+            { weights_to_f32<<<grid, block, 0, g->stream>>>(g->wgt.as<int32_t>(), (size_t)(g->M + kNbrPad),
+                                                            g->wf32.as<float>()); ::hc::count_launch(); }
+            HC_CUDA_TRY(cudaGetLastError());
+        }
         HC_TRY(g->inv_wsum.ensure(sizeof(float) * std::max<int32_t>(g->N, 1)));
         HC_TRY(g->wtn.ensure(sizeof(float) * (size_t)(g->M + kNbrPad)));
-        { build_inv_wsum<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->wgt.as<float>(), g->N,
+        { build_inv_wsum<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), pr_weights(g), g->N,
                                                         g->inv_wsum.as<float>()); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         DevBuf flag;
         HC_TRY(flag.ensure(sizeof(int)));
         HC_CUDA_TRY(cudaMemsetAsync(flag.ptr, 0, sizeof(int), g->stream));
         { build_wtn<<<grid, block, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
-                                                   g->wgt.as<float>(), g->inv_wsum.as<float>(), g->N,
+                                                   pr_weights(g), g->inv_wsum.as<float>(), g->N,
                                                    g->wtn.as<float>(), flag.as<int>()); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         int missing = 0;
@@ -213,9 +274,9 @@ hc_status ensure_pr_derived(hc_graph *g, bool weighted) {
 }  // namespace hc
 
 int64_t hc_graph::bytes_held() const {
-    const hc::DevBuf *bufs[] = {&index, &nbr, &wgt, &inv_deg, &inv_wsum, &wtn, &pr_plan,
+    const hc::DevBuf *bufs[] = {&index, &nbr, &wgt, &inv_deg, &inv_wsum, &wtn, &wf32, &pr_plan,
                                 &pr_plan_huge_rows, &ws_bfs, &ws_sssp, &ws_pr, &ws_batch,
-                                &ws_out0, &ws_out1, &ws_ctl, &ws_plan_ms, &ws_src};
+                                &ws_out0, &ws_out1, &ws_ctl, &ws_plan_ms, &ws_plan_mssp, &ws_src};
     int64_t t = 0;
     for (auto *b : bufs) t += (int64_t)b->bytes;
     return t;
@@ -326,9 +387,9 @@ hc_status hc_graph_destroy(hc_graph *g) {
     cudaSetDevice(g->device);
     if (g->own_stream) cudaStreamSynchronize(g->own_stream);
     if (g->stream && g->stream != g->own_stream) cudaStreamSynchronize(g->stream);
-    DevBuf *bufs[] = {&g->index, &g->nbr, &g->wgt, &g->inv_deg, &g->inv_wsum, &g->wtn, &g->pr_plan,
+    DevBuf *bufs[] = {&g->index, &g->nbr, &g->wgt, &g->inv_deg, &g->inv_wsum, &g->wtn, &g->wf32, &g->pr_plan,
                       &g->pr_plan_huge_rows, &g->ws_bfs, &g->ws_sssp, &g->ws_pr, &g->ws_batch,
-                      &g->ws_out0, &g->ws_out1, &g->ws_ctl, &g->ws_plan_ms, &g->ws_src};
+                      &g->ws_out0, &g->ws_out1, &g->ws_ctl, &g->ws_plan_ms, &g->ws_plan_mssp, &g->ws_src};
     for (auto *b : bufs) b->release();
     g->pinned.release();
     if (g->ev_start) cudaEventDestroy(g->ev_start);

@@ -59,10 +59,15 @@ struct hc_graph {
     hc::DevBuf inv_deg;        // f32[N]: 1/deg (0 for isolated)
     hc::DevBuf inv_wsum;       // f32[N]: 1/sum_k w_uk (weighted PageRank)
     hc::DevBuf wtn;            // f32[M]: slot (v,i) holds w_{u v}/sum_k w_uk, u = nbr[v][i]
+    hc::DevBuf wf32;           // f32[M]: int32 weights as floats (weighted PageRank on int32 graphs)
     hc::DevBuf pr_plan;        // row plan (device arrays)
     hc::PrPlanDev pr_view{};   // host copy of its pointers and counts
     int32_t pr_partial_slots = 0;
     hc::DevBuf pr_plan_huge_rows;
+
+    // symmetry of the PageRank transition (-1: not checked yet)
+    int pr_sym_struct = -1;    // every edge u->v has v->u (rows sorted)
+    int pr_sym_w = -1;         // ... with the same weight
 
     // weight statistics, computed once
     int wstats_done = 0;
@@ -93,6 +98,12 @@ namespace hc {
 hc_status activate(hc_graph *g);
 // Builds inv_deg (and, for weighted graphs, inv_wsum / wtn) if missing.
 hc_status ensure_pr_derived(hc_graph *g, bool weighted);
+// Whether the PageRank transition is a reversible walk (symmetric structure,
+// and symmetric weights when `weighted`), checked once per graph.
+hc_status ensure_pr_symmetry(hc_graph *g, bool weighted, bool *symmetric);
+// The edge weights as fp32 for weighted PageRank: the weight array itself
+// (fp32 graphs) or its converted copy (int32 graphs, built by ensure_pr_derived).
+const float *pr_weights(const hc_graph *g);
 // Builds the row plan if missing (g->pr_view, g->pr_partial_slots).
 hc_status ensure_plan(hc_graph *g);
 // Computes w_negative, w_mean and w_symmetric once (int32 weights).

@@ -55,6 +55,7 @@ struct SweepArgs {
     unsigned *hub_count;
     IterState *st;
     int it;
+    float omega;            // Chebyshev weight of this iteration (1: plain Jacobi)
     float tol_l1, eps;
     int max_iters;
     int32_t n_active;
@@ -64,11 +65,19 @@ template <bool kEW, bool kRS, bool kPS, bool kBaseVec>
 __device__ __forceinline__ void finish_row(const SweepArgs &a, int32_t r, float sum, float &l1, int &chg) {
     const float base = kBaseVec ? a.basev[r] : a.base_scalar;
     const float scale = kRS ? a.rs[r] : 1.0f;
-    const float nv = base + a.d * (scale * sum);
+    float nv = base + a.d * (scale * sum);
     const float ov = a.xin[r];
+    // The residual |J(x_k) - x_k| of the fixed-point equation: the change of
+    // a plain Jacobi sweep, and the stopping rule of both iterations.
+    const float dl = fabsf(nv - ov);
+    // Chebyshev semi-iteration: x_{k+1} = omega (J(x_k) - x_{k-1}) + x_{k-1};
+    // x_{k-1} is what the output buffer still holds.
+    if (a.omega != 1.0f) {
+        const float prev = a.xout[r];
+        nv = a.omega * (nv - prev) + prev;
+    }
     a.xout[r] = nv;
     if (kPS) a.gout[r] = nv * a.ps[r];
-    const float dl = fabsf(nv - ov);
     l1 += dl;
     chg += dl > a.eps;
 }
@@ -241,13 +250,14 @@ __global__ void __launch_bounds__(kPrThreads) pr_sweep(SweepArgs a, PrPlanDev pl
 }
 
 // x <- (1-d) t (or (1-d)/N) for every vertex; gather vector g <- x * ps.
+// Rows that may have edges start from x0_scale * (x0v or x0_scalar).
 __global__ void pr_init(int32_t n, const float *basev, float base_scalar, float x0_scalar, const float *x0v,
-                        const float *ps, float *x, float *g, float *x2, float *g2, int32_t n_active) {
+                        float x0_scale, const float *ps, float *x, float *g, float *x2, float *g2, int32_t n_active) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         const float base = basev ? basev[v] : base_scalar;
         // Vertices without edges sit at their base from the start; the rest
         // start from the initial guess.
-        const float x0 = v >= n_active ? base : (x0v ? x0v[v] : x0_scalar);
+        const float x0 = v >= n_active ? base : x0_scale * (x0v ? x0v[v] : x0_scalar);
         x[v] = x0;
         x2[v] = x0;
         if (g) {
@@ -579,8 +589,12 @@ struct SolveResult {
     float ms;
 };
 
+// Sweeps until converged.  cheb_rho > 0: Chebyshev semi-iteration for a
+// Jacobi operator whose spectrum lies in [-cheb_rho, cheb_rho] (a reversible
+// walk scaled by d): weights omega_1 = 1, omega_2 = 1 / (1 - rho^2 / 2),
+// omega_{k+1} = 1 / (1 - rho^2 omega_k / 4) (Golub and Varga, 1961).
 hc_status run_solve(hc_graph *g, SweepArgs a, const PrPlanDev &plan, SweepFn fn, float *x[2], float *gv[2],
-                    bool separate_g, SolveResult *res) {
+                    bool separate_g, SolveResult *res, float cheb_rho = 0.f) {
     IterState *st = reinterpret_cast<IterState *>(g->ws_ctl.ptr);
     HC_CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(IterState), g->stream));
     HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
@@ -591,9 +605,13 @@ hc_status run_solve(hc_graph *g, SweepArgs a, const PrPlanDev &plan, SweepFn fn,
     };
     HC_TRY(g->pinned.ensure(64));
     volatile Tail *pt = g->pinned.as<Tail>();
+    const double rho2 = (double)cheb_rho * cheb_rho;
+    double omega = 1.0;
     for (int it = 0; it < a.max_iters && !host_done;) {
         for (int k = 0; k < kRound && it < a.max_iters; k++, it++) {
             a.it = it;
+            if (cheb_rho > 0.f) omega = it == 0 ? 1.0 : it == 1 ? 1.0 / (1.0 - rho2 / 2.0) : 1.0 / (1.0 - rho2 * omega / 4.0);
+            a.omega = (float)omega;
             a.gin = separate_g ? gv[it & 1] : x[it & 1];
             a.xin = x[it & 1];
             a.xout = x[(it + 1) & 1];
@@ -751,6 +769,8 @@ extern "C" hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t n
     float *partials = (float *)take((size_t)(partial_slots + 1) * 4);
     unsigned *hub_count = (unsigned *)take((size_t)(plan.n_hub + 1) * 4);
     HC_CUDA_TRY(cudaMemsetAsync(hub_count, 0, (size_t)(plan.n_hub + 1) * 4, g->stream));
+    bool cheb = false;
+    if (o.accel > 0) HC_TRY(ensure_pr_symmetry(g, weighted, &cheb));
     const bool basevec = teleport != nullptr;
     if (basevec) {
         HC_TRY(copy_in(basev, teleport, n * 4, g->stream));
@@ -758,11 +778,13 @@ extern "C" hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t n
     }
     // Uniform teleport: base (1-d)/N as the reference computes it
     // (src/kernels/gpu/pr.cuh:152), start from 1/N (src/kernels/cpu/pr.cuh:39).
+    // A teleport vector t starts from t itself (base / (1-d)), which has the
+    // fixed point's mass, so the error has no part in the slowest mode.
     const float base_scalar = (1.0f - o.damping) / (float)g->N;
     const float *ps = weighted ? nullptr : g->inv_deg.as<float>();
     { pr_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, basevec ? basev : nullptr, base_scalar,
                                                     basevec ? 0.f : 1.0f / (float)g->N, basevec ? basev : nullptr,
-                                                    ps, x[0], weighted ? nullptr : gv[0], x[1],
+                                                    basevec ? 1.0f / (1.0f - o.damping) : 1.0f, ps, x[0], weighted ? nullptr : gv[0], x[1],
                                                     weighted ? nullptr : gv[1], g->n_active); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     SweepArgs a{};
@@ -785,7 +807,7 @@ extern "C" hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t n
     if (!fn) return fail(HC_ERR_UNSUPPORTED, "hc_pr_forward: no sweep for this option set");
     if (o.eps_vertex <= 0.f) a.eps = 3.4e38f;
     SolveResult r;
-    HC_TRY(run_solve(g, a, plan, fn, x, gv, !weighted, &r));
+    HC_TRY(run_solve(g, a, plan, fn, x, gv, !weighted, &r, cheb ? o.damping : 0.f));
     HC_TRY(copy_out(scores_out, x[r.iters & 1], n * 4, g->stream));
     HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
     if (stats) {
@@ -832,14 +854,19 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
     HC_CUDA_TRY(cudaMemsetAsync(hub_count, 0, (size_t)(plan.n_hub + 1) * 4, g->stream));
     HC_TRY(copy_in(cvec, dL_dscores, n * 4, g->stream));
     HC_TRY(copy_in(xs, scores, n * 4, g->stream));
-    // lambda_0 = c; isolated vertices keep lambda = c.
-    { pr_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, cvec, 0.f, 0.f, cvec, nullptr, lam[0], nullptr, lam[1],
-                                                    nullptr, g->n_active); ::hc::count_launch(); }
+    // lambda_0 = c / (1-d); isolated vertices keep lambda = c.  With
+    // symmetric weights the walk's stationary vector is the weighted degree
+    // s, and the fixed point has s.lambda = s.c / (1-d) on every connected
+    // component: this start already carries that, so the mode that decays
+    // only at rate d (eigenvalue 1 of the walk) is absent from the start.
+    // Any start converges to the same fixed point; this one converges fastest.
+    { pr_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, cvec, 0.f, 0.f, cvec, 1.0f / (1.0f - o.damping), nullptr,
+                                                    lam[0], nullptr, lam[1], nullptr, g->n_active); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     SweepArgs a{};
     a.index = g->index.as<int64_t>();
     a.nbr = g->nbr.as<int32_t>();
-    a.ew = weighted ? g->wgt.as<float>() : nullptr;
+    a.ew = weighted ? pr_weights(g) : nullptr;
     a.basev = cvec;
     a.d = o.damping;
     a.rs = weighted ? g->inv_wsum.as<float>() : g->inv_deg.as<float>();
@@ -862,9 +889,14 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
     a.max_iters = o.max_iters;
     a.n_active = g->n_active;
     SweepFn fn = pick_sweep(weighted, true, false, true);
+    // lambda = c + d A^T lambda: for a reversible walk A^T = D^-1 S is similar
+    // to a symmetric matrix with spectrum in [-1, 1], so the Jacobi operator's
+    // spectrum lies in [-d, d] and Chebyshev weights apply.
+    bool cheb = false;
+    if (o.accel >= 0) HC_TRY(ensure_pr_symmetry(g, weighted, &cheb));
     SolveResult r;
     float *gdummy[2] = {spare, spare};
-    HC_TRY(run_solve(g, a, plan, fn, lam, gdummy, false, &r));
+    HC_TRY(run_solve(g, a, plan, fn, lam, gdummy, false, &r, cheb ? o.damping : 0.f));
     float *lfin = lam[r.iters & 1];
     HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     if (dL_dteleport) {
@@ -883,7 +915,7 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
         }
         const float *rsv = weighted ? g->inv_wsum.as<float>() : g->inv_deg.as<float>();
         if (weighted)
-            { pr_edge_grad<true><<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, g->wgt.as<float>(), rsv, xs,
+            { pr_edge_grad<true><<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, pr_weights(g), rsv, xs,
                                                                        lfin, o.damping, g->N, dst); ::hc::count_launch(); }
         else
             { pr_edge_grad<false><<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, nullptr, rsv, xs, lfin,

@@ -68,7 +68,7 @@ class SsspStats(C.Structure):
 
 class PrOpts(C.Structure):
     _fields_ = [("damping", C.c_float), ("tol_l1", C.c_float), ("eps_vertex", C.c_float), ("max_iters", C.c_int32),
-                ("weighted", C.c_int32), ("variant", C.c_int)]
+                ("weighted", C.c_int32), ("variant", C.c_int), ("accel", C.c_int32)]
 
 
 class PrStats(C.Structure):
@@ -344,23 +344,23 @@ class Graph:
         return dist, parent, st
 
     def pagerank(self, teleport=None, scores=None, *, damping=0.85, tol_l1=1e-4, eps_vertex=0.0, max_iters=50,
-                 weighted=False):
+                 weighted=False, accel=0):
         ncols = 1 if teleport is None or teleport.ndim == 1 else teleport.shape[1]
         if scores is None:
             scores = np.empty((self.num_nodes,) if ncols == 1 else (self.num_nodes, ncols), dtype=np.float32)
-        o = PrOpts(damping, tol_l1, eps_vertex, max_iters, 1 if weighted else 0, VARIANT_AUTO)
+        o = PrOpts(damping, tol_l1, eps_vertex, max_iters, 1 if weighted else 0, VARIANT_AUTO, accel)
         st = PrStats()
         _check(lib().hc_pr_forward(self._h, _ptr(teleport), ncols, _ptr(scores), C.byref(o), C.byref(st)),
                "hc_pr_forward")
         return scores, st
 
     def pagerank_backward(self, scores, dL_dscores, *, damping=0.85, tol_l1=1e-7, eps_vertex=0.0, max_iters=500,
-                          weighted=False, want_dw=True, dteleport=None, dweights=None):
+                          weighted=False, want_dw=True, dteleport=None, dweights=None, accel=0):
         if dteleport is None:
             dteleport = np.empty(self.num_nodes, dtype=np.float32)
         if dweights is None and want_dw:
             dweights = np.empty(self.num_edges, dtype=np.float32)
-        o = PrOpts(damping, tol_l1, eps_vertex, max_iters, 1 if weighted else 0, VARIANT_AUTO)
+        o = PrOpts(damping, tol_l1, eps_vertex, max_iters, 1 if weighted else 0, VARIANT_AUTO, accel)
         st = PrStats()
         _check(lib().hc_pr_backward(self._h, _ptr(scores), _ptr(dL_dscores), _ptr(dteleport), _ptr(dweights),
                                     C.byref(o), C.byref(st)), "hc_pr_backward")

@@ -94,8 +94,74 @@ def test_backward_requires_inputs(ugraph):
     host, g = ugraph
     st = hc.lib().hc_pr_backward(g.handle, None, None, None, None, None, None)
     assert st == hc.INVALID_ARG
-    fg = hc.Graph.from_host(hc.gen_kronecker(8, 4, 1, wtype=hc.W_I32))  # int weights: no weighted PageRank
-    x, _ = fg.pagerank()
+    ug = hc.Graph.from_host(hc.gen_kronecker(8, 4, 1))  # no weights: no weighted PageRank
+    x, _ = ug.pagerank()
     with pytest.raises(hc.HCError) as e:
-        fg.pagerank_backward(x, np.ones_like(x), weighted=True)
+        ug.pagerank_backward(x, np.ones_like(x), weighted=True)
     assert e.value.status == hc.UNSUPPORTED
+
+
+def test_int32_weights_match_their_fp32_values():
+    """Weighted PageRank and its adjoint on int32 weights equal the same run on the weights as fp32."""
+    host = hc.gen_kronecker(11, 16, 23, wtype=hc.W_I32)
+    gi = hc.Graph.from_host(host)
+    gf = hc.Graph(host.index, host.neighbors, host.weights.astype(np.float32))
+    rng = np.random.default_rng(3)
+    c = rng.standard_normal(host.num_nodes).astype(np.float32)
+    xi, _ = gi.pagerank(weighted=True, tol_l1=1e-8, max_iters=300)
+    xf, _ = gf.pagerank(weighted=True, tol_l1=1e-8, max_iters=300)
+    assert np.array_equal(xi, xf)
+    dti, dwi, _ = gi.pagerank_backward(xi, c, weighted=True, tol_l1=1e-8, max_iters=300)
+    dtf, dwf, _ = gf.pagerank_backward(xf, c, weighted=True, tol_l1=1e-8, max_iters=300)
+    assert np.array_equal(dti, dtf) and np.array_equal(dwi, dwf)
+    x64, dt64, dw64 = oracle.pr_dense_grad(host.index, host.neighbors, c.astype(np.float64),
+                                           host.weights.astype(np.float64),
+                                           np.full(host.num_nodes, 1.0 / host.num_nodes), D)
+    assert np.abs(xi - x64).max() < 1e-7
+    assert np.abs(dti - dt64).max() < 1e-5 * np.abs(dt64).max()
+
+
+@pytest.mark.parametrize("weighted", [True, False])
+def test_chebyshev_and_jacobi_reach_the_same_gradient(wgraph, ugraph, weighted):
+    """accel=0 (Chebyshev semi-iteration on the symmetric walk) and accel=-1 (plain Jacobi) both match the
+    FP64 dense gradient; the accelerated solve needs fewer sweeps."""
+    host, g = wgraph if weighted else ugraph
+    c, t, x64, dt64, dw64 = _case(host, weighted, 8)
+    x, _ = g.pagerank(t.astype(np.float32), weighted=weighted, tol_l1=1e-10, max_iters=400)
+    runs = {}
+    for accel in (0, -1):
+        dt, dw, st = g.pagerank_backward(x, c.astype(np.float32), weighted=weighted, tol_l1=1e-9, max_iters=500,
+                                         accel=accel)
+        assert np.abs(dt - dt64).max() < 1e-5 * np.abs(dt64).max(), accel
+        assert np.abs(dw - dw64).max() < 1e-4 * np.abs(dw64).max(), accel
+        # Sweeps to a tolerance above the fp32 rounding floor (1e-9 never stops before the cap).
+        dt, _, st = g.pagerank_backward(x, c.astype(np.float32), weighted=weighted, tol_l1=1e-5, max_iters=500,
+                                        accel=accel, want_dw=False)
+        assert st.converged and np.abs(dt - dt64).max() < 1e-2 * np.abs(dt64).max(), accel
+        runs[accel] = st.iterations
+    assert runs[0] <= 2 * runs[-1], runs  # no blow-up; the gain shows on large graphs
+
+
+def test_chebyshev_forward(wgraph):
+    host, g = wgraph
+    _, t, x64, _, _ = _case(host, True, 9)
+    x1, s1 = g.pagerank(t.astype(np.float32), weighted=True, tol_l1=1e-7, max_iters=400, accel=1)
+    x0, s0 = g.pagerank(t.astype(np.float32), weighted=True, tol_l1=1e-7, max_iters=400, accel=-1)
+    assert s1.converged and s0.converged
+    assert np.abs(x1 - x64).max() < 1e-7 and np.abs(x0 - x64).max() < 1e-7
+    assert s1.iterations <= s0.iterations
+
+
+def test_asymmetric_weights_fall_back_to_jacobi():
+    """w(u->v) != w(v->u): no Chebyshev weights (the walk is not reversible); the result still matches."""
+    host = hc.gen_kronecker(11, 8, 7)
+    w = np.random.default_rng(1).random(host.num_edges).astype(np.float32) + 0.01
+    g = hc.Graph(host.index, host.neighbors, w)
+    rng = np.random.default_rng(2)
+    c = rng.standard_normal(host.num_nodes)
+    t = np.full(host.num_nodes, 1.0 / host.num_nodes)
+    x64, dt64, dw64 = oracle.pr_dense_grad(host.index, host.neighbors, c, w.astype(np.float64), t, D)
+    x, _ = g.pagerank(t.astype(np.float32), weighted=True, tol_l1=1e-10, max_iters=400)
+    dt, dw, _ = g.pagerank_backward(x, c.astype(np.float32), weighted=True, tol_l1=1e-9, max_iters=500)
+    assert np.abs(dt - dt64).max() < 1e-5 * np.abs(dt64).max()
+    assert np.abs(dw - dw64).max() < 1e-4 * np.abs(dw64).max()
