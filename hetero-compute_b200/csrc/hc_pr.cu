@@ -61,8 +61,18 @@ struct SweepArgs {
     int32_t n_active;
 };
 
-template <bool kEW, bool kRS, bool kPS, bool kBaseVec>
+template <bool kEW, bool kRS, bool kPS, bool kBaseVec, bool kCG = false>
 __device__ __forceinline__ void finish_row(const SweepArgs &a, int32_t r, float sum, float &l1, int &chg) {
+    if constexpr (kCG) {
+        // Conjugate-gradient product (gin = p): xout = (S p)_r, and
+        // p_r q_r with q = s p - d S p summed where the residual goes.
+        const float pr = a.gin[r];
+        const float rsr = a.rs[r];
+        const float sr = rsr > 0.f ? 1.0f / rsr : 0.f;
+        a.xout[r] = sum;
+        l1 += pr * (sr * pr - a.d * sum);
+        return;
+    }
     const float base = kBaseVec ? a.basev[r] : a.base_scalar;
     const float scale = kRS ? a.rs[r] : 1.0f;
     float nv = base + a.d * (scale * sum);
@@ -88,7 +98,7 @@ __device__ __forceinline__ float edge_val(const SweepArgs &a, int64_t e) {
     return kEW ? g * a.ew[e] : g;
 }
 
-template <bool kEW, bool kRS, bool kPS, bool kBaseVec>
+template <bool kEW, bool kRS, bool kPS, bool kBaseVec, bool kCG = false>
 __global__ void __launch_bounds__(kPrThreads) pr_sweep(SweepArgs a, PrPlanDev plan) {
     __shared__ float s_acc[kPrThreads / 32][32];
     __shared__ double s_l1[32];
@@ -135,7 +145,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_sweep(SweepArgs a, PrPlanDev pl
                 t = warp_sum(t);
                 if (lane == 0) {
                     a.hub_count[tk.x] = 0;
-                    finish_row<kEW, kRS, kPS, kBaseVec>(a, h.row, t, l1, chg);
+                    finish_row<kEW, kRS, kPS, kBaseVec, kCG>(a, h.row, t, l1, chg);
                 }
             }
         } else if (item < plan.n_tasks + plan.n_long) {
@@ -158,7 +168,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_sweep(SweepArgs a, PrPlanDev pl
             const int64_t tail = ab + ((e - ab) & ~(int64_t)3);
             if (tail + lane < e) s += edge_val<kEW>(a, tail + lane);
             s = warp_sum(s);
-            if (lane == 0) finish_row<kEW, kRS, kPS, kBaseVec>(a, r, s, l1, chg);
+            if (lane == 0) finish_row<kEW, kRS, kPS, kBaseVec, kCG>(a, r, s, l1, chg);
         } else {
             // Stream group: rows r0 .. r0+31 (clipped to n_active).
             const int32_t r0 = plan.stream[item - plan.n_tasks - plan.n_long] * 32;
@@ -205,7 +215,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_sweep(SweepArgs a, PrPlanDev pl
                     __syncwarp();
                 }
             }
-            if (r < a.n_active) finish_row<kEW, kRS, kPS, kBaseVec>(a, r, s_acc[wib][lane], l1, chg);
+            if (r < a.n_active) finish_row<kEW, kRS, kPS, kBaseVec, kCG>(a, r, s_acc[wib][lane], l1, chg);
             __syncwarp();
         }
     }
@@ -281,24 +291,59 @@ __global__ void scale_vec(const float *in, float s, float *out, size_t n) {
         out[v] = s * in[v];
 }
 
-// dL/dw_uk = (d x_u / s_u) (lambda_k - sum_j W_uj lambda_j), slot order of row u.
-template <bool kEW>
-__global__ void pr_edge_grad(const int64_t *index, const int32_t *nbr, const float *w, const float *rs,
-                             const float *x, const float *lam, float d, int32_t n, float *grad) {
+// dL/dw_uk = (d x_u / s_u) (lambda_k - sum_j W_uj lambda_j), slot order of
+// row u, and at the fixed point sum_j W_uj lambda_j = (lambda_u - c_u) / d, so one pass:
+// dL/dw_uk = (x_u / s_u) (d lambda_k - lambda_u + c_u).
+// Work items are the row plan's: hub chunks and long rows (one warp, one row)
+// and stream groups (32 rows, one warp walks their edges 32 at a time and
+// each lane finds its edge's row among the group's offsets).
+__global__ void __launch_bounds__(kPrThreads) pr_edge_grad(PrPlanDev plan, const int64_t *index, const int32_t *nbr,
+                                                           const float *rs, const float *x, const float *lam,
+                                                           const float *c, float d, int32_t n_active, float *grad) {
     const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += nw) {
-        const int64_t b = index[u], e = index[u + 1];
-        if (b == e) continue;
-        float s = 0.f;
-        for (int64_t i = b + lane; i < e; i += 32) {
-            const float l = __ldg(lam + nbr[i]);
-            s += kEW ? w[i] * l : l;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int total = plan.n_tasks + plan.n_long + plan.n_stream;
+    for (int item = gwarp; item < total; item += nwarps) {
+        if (item < plan.n_tasks + plan.n_long) {
+            int32_t u;
+            int64_t b, e;
+            if (item < plan.n_tasks) {
+                const int2 tk = plan.tasks[item];
+                u = plan.hubs[tk.x].row;
+                const int64_t rb = index[u], re = index[u + 1];
+                b = rb + (int64_t)tk.y * kHubChunk;
+                e = min(re, b + (int64_t)kHubChunk);
+            } else {
+                u = plan.longrows[item - plan.n_tasks];
+                b = index[u];
+                e = index[u + 1];
+            }
+            const float coef = x[u] * rs[u];
+            const float off = lam[u] - c[u];
+            for (int64_t i = b + lane; i < e; i += 32) grad[i] = coef * (d * __ldg(lam + nbr[i]) - off);
+        } else {
+            const int32_t r0 = plan.stream[item - plan.n_tasks - plan.n_long] * 32;
+            const int32_t r = r0 + lane;
+            const int32_t rc = min(r, n_active);
+            const int64_t s0 = index[r0];
+            const int32_t rel = (int32_t)(index[rc] - s0);
+            const int32_t gend = (int32_t)(index[min(r0 + 32, n_active)] - s0);
+            const float coef = r < n_active ? x[r] * rs[r] : 0.f;
+            const float off = r < n_active ? lam[r] - c[r] : 0.f;
+            for (int k0 = 0; k0 < gend; k0 += 32) {
+                const int k = k0 + lane;
+                int lo = 0;
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const int cc = __shfl_sync(kFull, rel, lo + st);
+                    if (cc <= k) lo += st;
+                }
+                const float cf = __shfl_sync(kFull, coef, lo);
+                const float of = __shfl_sync(kFull, off, lo);
+                if (k < gend) grad[s0 + k] = cf * (d * __ldg(lam + nbr[s0 + k]) - of);
+            }
         }
-        s = warp_sum(s);
-        const float mean = s * rs[u];
-        const float coef = d * x[u] * rs[u];
-        for (int64_t i = b + lane; i < e; i += 32) grad[i] = coef * (__ldg(lam + nbr[i]) - mean);
     }
 }
 
@@ -547,14 +592,15 @@ PrPlanDev plan_view(hc_graph *g, int *partial_slots) {
     return g->pr_view;
 }
 
-template <bool kEW, bool kRS, bool kPS, bool kBaseVec>
+template <bool kEW, bool kRS, bool kPS, bool kBaseVec, bool kCG = false>
 hc_status launch_sweep(hc_graph *g, const SweepArgs &a, const PrPlanDev &plan) {
     static int bps = 0;
     if (bps == 0) {
-        HC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pr_sweep<kEW, kRS, kPS, kBaseVec>, kPrThreads, 0));
+        HC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pr_sweep<kEW, kRS, kPS, kBaseVec, kCG>,
+                                                                  kPrThreads, 0));
         bps = std::max(bps, 1);
     }
-    { pr_sweep<kEW, kRS, kPS, kBaseVec><<<g->sm_count * bps, kPrThreads, 0, g->stream>>>(a, plan); ::hc::count_launch(); }
+    { pr_sweep<kEW, kRS, kPS, kBaseVec, kCG><<<g->sm_count * bps, kPrThreads, 0, g->stream>>>(a, plan); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     return HC_OK;
 }
@@ -637,6 +683,198 @@ hc_status run_solve(hc_graph *g, SweepArgs a, const PrPlanDev &plan, SweepFn fn,
     }
     res->l1 = l1;
     res->changed = chg;
+    HC_CUDA_TRY(cudaEventElapsedTime(&res->ms, g->ev_start, g->ev_stop));
+    return HC_OK;
+}
+
+// ------------------------------------------------- adjoint by conjugate gradients
+// For a reversible walk (symmetric weights S, weighted degrees s, D = diag(s))
+// the adjoint equation lambda = c + d D^-1 S lambda is, multiplied by D, the
+// symmetric positive definite system (D - d S) lambda = D c, solved here by
+// conjugate gradients with the diagonal preconditioner D (Hestenes and
+// Stiefel, 1952).  The preconditioned residual z = D^-1 r equals the Jacobi
+// residual c + d A^T lambda - lambda, so the stopping rule is the same as the
+// sweeps'.  Rows without weight (s = 0) keep lambda = c.  Vectors are fp32,
+// dot products fp64; alpha, beta and the stop decision stay on the device.
+struct CgState {
+    double acc0, acc1;       // block partial sums of the running kernel
+    double rz, alpha, beta, z1;
+    double tol;
+    unsigned blocks;
+    int iters, max_iters, converged;
+};
+
+__device__ __forceinline__ float row_weight(const float *rs, int32_t v) {
+    const float r = rs[v];
+    return r > 0.f ? 1.0f / r : 0.f;
+}
+
+// Accumulates (a0, a1) over the grid; the last block to finish returns true
+// in thread 0 with the totals in *t0, *t1 and the accumulators cleared.
+__device__ __forceinline__ bool grid_sum2(CgState *cg, double a0, double a1, double *t0, double *t1) {
+    __shared__ double s0[32], s1[32];
+    __shared__ int s_last;
+    a0 = block_sum(a0, s0);
+    a1 = block_sum(a1, s1);
+    if (threadIdx.x == 0) {
+        if (a0 != 0.0) atomicAdd(&cg->acc0, a0);
+        if (a1 != 0.0) atomicAdd(&cg->acc1, a1);
+        __threadfence();
+        s_last = atomicAdd(&cg->blocks, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return false;
+    __threadfence();
+    *t0 = *(volatile double *)&cg->acc0;
+    *t1 = *(volatile double *)&cg->acc1;
+    cg->acc0 = 0.0;
+    cg->acc1 = 0.0;
+    cg->blocks = 0;
+    return true;
+}
+
+// r = s (c - lambda) + d S lambda, z = r / s, p = z; rz = r.z, stop if |z|_1 < tol.
+__global__ void cg_start(int32_t n, const float *c, float *lam, const float *slam, const float *rs, float d, float *r,
+                         float *p, CgState *cg, IterState *st) {
+    double rz = 0.0, z1 = 0.0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const float sv = row_weight(rs, v);
+        if (sv == 0.f) {
+            lam[v] = c[v];
+            r[v] = 0.f;
+            p[v] = 0.f;
+            continue;
+        }
+        const float rv = sv * (c[v] - lam[v]) + d * slam[v];
+        const float zv = rv * rs[v];
+        r[v] = rv;
+        p[v] = zv;
+        rz += (double)rv * zv;
+        z1 += fabs((double)zv);
+    }
+    double trz, tz1;
+    if (grid_sum2(cg, rz, z1, &trz, &tz1)) {
+        cg->rz = trz;
+        cg->z1 = tz1;
+        if (tz1 < cg->tol || trz <= 0.0) {
+            cg->converged = 1;
+            st->done = 1;
+        }
+    }
+}
+
+// alpha = rz / (p . q), p . q from the sweep's residual slot; lambda += alpha
+// p, r -= alpha q; beta = r.z / rz; stop on |z|_1 < tol or the cap.
+__global__ void cg_update(int32_t n, const float *p, const float *sp, const float *rs, float d, float *lam, float *r,
+                          CgState *cg, IterState *st, int slot) {
+    if (*(volatile int *)&st->done) return;
+    const double pq = *(volatile double *)&st->l1[slot];
+    if (!(pq > 0.0)) {  // p = 0 (already exact) or a breakdown: stop
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->done = 1;
+        return;
+    }
+    const float alpha = (float)(cg->rz / pq);
+    double rz = 0.0, z1 = 0.0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const float pv = p[v];
+        const float q = row_weight(rs, v) * pv - d * sp[v];
+        lam[v] += alpha * pv;
+        const float rv = r[v] - alpha * q;
+        r[v] = rv;
+        const float zv = rv * rs[v];
+        rz += (double)rv * zv;
+        z1 += fabs((double)zv);
+    }
+    double trz, tz1;
+    if (grid_sum2(cg, rz, z1, &trz, &tz1)) {
+        cg->beta = cg->rz > 0.0 ? trz / cg->rz : 0.0;
+        cg->rz = trz;
+        cg->z1 = tz1;
+        cg->iters++;
+        if (tz1 < cg->tol) cg->converged = 1;
+        if (cg->converged || cg->iters >= cg->max_iters) st->done = 1;
+    }
+}
+
+// p = z + beta p.
+__global__ void cg_direction(int32_t n, const float *r, const float *rs, float *p, const CgState *cg,
+                             const IterState *st) {
+    if (*(volatile const int *)&st->done) return;
+    const float beta = (float)cg->beta;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        p[v] = r[v] * rs[v] + beta * p[v];
+}
+
+// Solves the adjoint into lam (which holds the start) with the row plan's
+// sweep for S x.  `work` holds 3 vectors of n floats.
+hc_status run_cg(hc_graph *g, const PrPlanDev &plan, bool weighted, const float *c, float *lam, float d, double tol,
+                 int max_iters, float *work, float *partials, unsigned *hub_count, SolveResult *res) {
+    const int64_t n = g->N;
+    float *r = work, *pv = work + n, *sp = work + 2 * n;
+    IterState *st = reinterpret_cast<IterState *>(g->ws_ctl.ptr);
+    CgState *cg = reinterpret_cast<CgState *>(g->ws_ctl.as<char>() + (sizeof(IterState) + 255) / 256 * 256);
+    const float *rs = weighted ? g->inv_wsum.as<float>() : g->inv_deg.as<float>();
+    HC_CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(IterState), g->stream));
+    CgState h{};
+    h.tol = tol;
+    h.max_iters = max_iters;
+    HC_CUDA_TRY(cudaMemcpyAsync(cg, &h, sizeof(h), cudaMemcpyHostToDevice, g->stream));
+    // y = S x through the pull sweep (own-row weights, no stopping rule of
+    // its own: it returns at once once st->done is set); in the iterations
+    // its epilogue also sums p . q (kCG).
+    SweepArgs a{};
+    a.index = g->index.as<int64_t>();
+    a.nbr = g->nbr.as<int32_t>();
+    a.ew = weighted ? pr_weights(g) : nullptr;
+    a.base_scalar = 0.f;
+    a.d = 1.0f;
+    a.rs = rs;
+    a.omega = 1.0f;
+    a.partials = partials;
+    a.hub_count = hub_count;
+    a.st = st;
+    a.tol_l1 = 0.f;
+    a.eps = 3.4e38f;
+    a.max_iters = max_iters;
+    a.n_active = g->n_active;
+    SweepFn sweep = pick_sweep(weighted, false, false, false);
+    SweepFn cg_sweep = weighted ? launch_sweep<true, false, false, false, true> : launch_sweep<false, false, false, false, true>;
+    const int grid = g->sm_count * 4;
+    HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
+    a.it = 0;
+    a.gin = lam;
+    a.xin = sp;
+    a.xout = sp;
+    a.gout = sp;
+    HC_TRY(sweep(g, a, plan));
+    { cg_start<<<grid, 256, 0, g->stream>>>((int32_t)n, c, lam, sp, rs, d, r, pv, cg, st); ::hc::count_launch(); }
+    HC_CUDA_TRY(cudaGetLastError());
+    constexpr int kRound = 4;
+    HC_TRY(g->pinned.ensure(64));
+    volatile int *hdone = g->pinned.as<int>();
+    int it = 0;
+    for (bool done = false; !done && it < max_iters;) {
+        for (int k = 0; k < kRound && it < max_iters; k++, it++) {
+            a.it = it + 1;
+            a.gin = pv;
+            a.d = d;
+            HC_TRY(cg_sweep(g, a, plan));
+            const int slot = a.it % kMaxIterSlots;
+            { cg_update<<<grid, 256, 0, g->stream>>>((int32_t)n, pv, sp, rs, d, lam, r, cg, st, slot); ::hc::count_launch(); }
+            { cg_direction<<<grid, 256, 0, g->stream>>>((int32_t)n, r, rs, pv, cg, st); ::hc::count_launch(); }
+            HC_CUDA_TRY(cudaGetLastError());
+        }
+        HC_CUDA_TRY(cudaMemcpyAsync((void *)hdone, &st->done, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        done = *hdone != 0;
+    }
+    HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
+    HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    HC_CUDA_TRY(cudaMemcpy(&h, cg, sizeof(h), cudaMemcpyDeviceToHost));
+    res->iters = h.iters;
+    res->done = h.converged;
+    res->l1 = h.z1;
+    res->changed = 0;
     HC_CUDA_TRY(cudaEventElapsedTime(&res->ms, g->ev_start, g->ev_stop));
     return HC_OK;
 }
@@ -770,7 +1008,7 @@ extern "C" hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t n
     unsigned *hub_count = (unsigned *)take((size_t)(plan.n_hub + 1) * 4);
     HC_CUDA_TRY(cudaMemsetAsync(hub_count, 0, (size_t)(plan.n_hub + 1) * 4, g->stream));
     bool cheb = false;
-    if (o.accel > 0) HC_TRY(ensure_pr_symmetry(g, weighted, &cheb));
+    if (o.accel == 1) HC_TRY(ensure_pr_symmetry(g, weighted, &cheb));
     const bool basevec = teleport != nullptr;
     if (basevec) {
         HC_TRY(copy_in(basev, teleport, n * 4, g->stream));
@@ -836,8 +1074,9 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
     int partial_slots = 0;
     PrPlanDev plan = plan_view(g, &partial_slots);
     const int64_t n = g->N;
-    HC_TRY(g->ws_ctl.ensure(sizeof(IterState) + 4096));
-    const size_t bytes = 5 * (size_t)n * 4 + (size_t)(partial_slots + 1) * 4 + (size_t)(plan.n_hub + 1) * 4 + 4096;
+    HC_TRY(g->ws_ctl.ensure(sizeof(IterState) + sizeof(CgState) + 4096));
+    // cvec, lam[2], xs, spare and the three vectors of the CG solve.
+    const size_t bytes = 8 * (size_t)n * 4 + (size_t)(partial_slots + 1) * 4 + (size_t)(plan.n_hub + 1) * 4 + 8192;
     HC_TRY(g->ws_pr.ensure(bytes));
     char *p = g->ws_pr.as<char>();
     auto take = [&](size_t b) {
@@ -849,6 +1088,7 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
     float *lam[2] = {(float *)take(n * 4), (float *)take(n * 4)};
     float *xs = (float *)take(n * 4);
     float *spare = (float *)take(n * 4);
+    float *cg_work = (float *)take(3 * n * 4);  // r, p and S p of the conjugate-gradient solve
     float *partials = (float *)take((size_t)(partial_slots + 1) * 4);
     unsigned *hub_count = (unsigned *)take((size_t)(plan.n_hub + 1) * 4);
     HC_CUDA_TRY(cudaMemsetAsync(hub_count, 0, (size_t)(plan.n_hub + 1) * 4, g->stream));
@@ -889,15 +1129,25 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
     a.max_iters = o.max_iters;
     a.n_active = g->n_active;
     SweepFn fn = pick_sweep(weighted, true, false, true);
-    // lambda = c + d A^T lambda: for a reversible walk A^T = D^-1 S is similar
-    // to a symmetric matrix with spectrum in [-1, 1], so the Jacobi operator's
-    // spectrum lies in [-d, d] and Chebyshev weights apply.
-    bool cheb = false;
-    if (o.accel >= 0) HC_TRY(ensure_pr_symmetry(g, weighted, &cheb));
+    // lambda = c + d A^T lambda.  For a reversible walk (symmetric weights)
+    // A^T = D^-1 S is similar to a symmetric matrix with spectrum in [-1, 1]:
+    // conjugate gradients on (D - d S) lambda = D c (accel 0 / 1), or Chebyshev
+    // weights on the Jacobi sweeps, whose operator's spectrum lies in [-d, d]
+    // (accel 2).  Otherwise, and with accel -1, plain Jacobi sweeps.
+    bool sym = false;
+    if (o.accel >= 0) HC_TRY(ensure_pr_symmetry(g, weighted, &sym));
     SolveResult r;
-    float *gdummy[2] = {spare, spare};
-    HC_TRY(run_solve(g, a, plan, fn, lam, gdummy, false, &r, cheb ? o.damping : 0.f));
-    float *lfin = lam[r.iters & 1];
+    float *lfin;
+    if (sym && o.accel != 2) {
+        HC_CUDA_TRY(cudaMemsetAsync(cg_work + 2 * n, 0, n * 4, g->stream));  // S p rows without edges stay 0
+        HC_TRY(run_cg(g, plan, weighted, cvec, lam[0], o.damping, (double)a.tol_l1, o.max_iters, cg_work, partials,
+                      hub_count, &r));
+        lfin = lam[0];
+    } else {
+        float *gdummy[2] = {spare, spare};
+        HC_TRY(run_solve(g, a, plan, fn, lam, gdummy, false, &r, sym ? o.damping : 0.f));
+        lfin = lam[r.iters & 1];
+    }
     HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
     if (dL_dteleport) {
         const bool dev = is_device_pointer(dL_dteleport);
@@ -914,12 +1164,8 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
             dst = g->ws_out0.as<float>();
         }
         const float *rsv = weighted ? g->inv_wsum.as<float>() : g->inv_deg.as<float>();
-        if (weighted)
-            { pr_edge_grad<true><<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, pr_weights(g), rsv, xs,
-                                                                       lfin, o.damping, g->N, dst); ::hc::count_launch(); }
-        else
-            { pr_edge_grad<false><<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, nullptr, rsv, xs, lfin,
-                                                                        o.damping, g->N, dst); ::hc::count_launch(); }
+        { pr_edge_grad<<<g->sm_count * 8, kPrThreads, 0, g->stream>>>(plan, a.index, a.nbr, rsv, xs, lfin, cvec,
+                                                                      o.damping, g->n_active, dst); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         if (!dev) HC_TRY(copy_out(dL_dweights, dst, sizeof(float) * (size_t)g->M, g->stream));
     }

@@ -216,10 +216,11 @@ typedef struct hc_pr_opts {
     int32_t max_iters;    /* 0 -> 50 */
     int32_t weighted;     /* 1: transition weight w_uv / sum_k w_uk; 0: 1/deg(u) */
     hc_variant variant;
-    int32_t accel;        /* 0: Chebyshev semi-iteration for the adjoint solve when the
-                             weights (or, unweighted, the structure) are symmetric, plain
-                             Jacobi sweeps for the forward; 1: Chebyshev for the forward
-                             too (same condition); -1: Jacobi everywhere */
+    int32_t accel;        /* when the walk is reversible (symmetric weights, or symmetric
+                             structure unweighted): 0: adjoint by preconditioned conjugate
+                             gradients, forward by Jacobi sweeps; 1: as 0, and Chebyshev
+                             semi-iteration for the forward; 2: Chebyshev for the adjoint;
+                             -1: Jacobi sweeps everywhere.  Other graphs: Jacobi sweeps. */
 } hc_pr_opts;
 
 typedef struct hc_pr_stats {

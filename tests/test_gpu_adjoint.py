@@ -122,14 +122,14 @@ def test_int32_weights_match_their_fp32_values():
 
 
 @pytest.mark.parametrize("weighted", [True, False])
-def test_chebyshev_and_jacobi_reach_the_same_gradient(wgraph, ugraph, weighted):
-    """accel=0 (Chebyshev semi-iteration on the symmetric walk) and accel=-1 (plain Jacobi) both match the
-    FP64 dense gradient; the accelerated solve needs fewer sweeps."""
+def test_cg_chebyshev_and_jacobi_reach_the_same_gradient(wgraph, ugraph, weighted):
+    """accel=0 (conjugate gradients on the symmetric system), 2 (Chebyshev semi-iteration) and -1 (plain
+    Jacobi) all match the FP64 dense gradient; conjugate gradients need the fewest sweeps."""
     host, g = wgraph if weighted else ugraph
     c, t, x64, dt64, dw64 = _case(host, weighted, 8)
     x, _ = g.pagerank(t.astype(np.float32), weighted=weighted, tol_l1=1e-10, max_iters=400)
     runs = {}
-    for accel in (0, -1):
+    for accel in (0, 2, -1):
         dt, dw, st = g.pagerank_backward(x, c.astype(np.float32), weighted=weighted, tol_l1=1e-9, max_iters=500,
                                          accel=accel)
         assert np.abs(dt - dt64).max() < 1e-5 * np.abs(dt64).max(), accel
@@ -139,17 +139,18 @@ def test_chebyshev_and_jacobi_reach_the_same_gradient(wgraph, ugraph, weighted):
                                         accel=accel, want_dw=False)
         assert st.converged and np.abs(dt - dt64).max() < 1e-2 * np.abs(dt64).max(), accel
         runs[accel] = st.iterations
-    assert runs[0] <= 2 * runs[-1], runs  # no blow-up; the gain shows on large graphs
+    assert runs[0] < runs[-1] and runs[2] <= 2 * runs[-1], runs
 
 
 def test_chebyshev_forward(wgraph):
+    """accel=1: Chebyshev weights on the forward sweeps reach the same fixed point (opt-in: from the
+    uniform start the forward's error is already in fast modes, where plain sweeps do as well)."""
     host, g = wgraph
     _, t, x64, _, _ = _case(host, True, 9)
     x1, s1 = g.pagerank(t.astype(np.float32), weighted=True, tol_l1=1e-7, max_iters=400, accel=1)
     x0, s0 = g.pagerank(t.astype(np.float32), weighted=True, tol_l1=1e-7, max_iters=400, accel=-1)
     assert s1.converged and s0.converged
     assert np.abs(x1 - x64).max() < 1e-7 and np.abs(x0 - x64).max() < 1e-7
-    assert s1.iterations <= s0.iterations
 
 
 def test_asymmetric_weights_fall_back_to_jacobi():
