@@ -217,7 +217,7 @@ def run_suite(a):
         ms = _time_cuda(lambda: [g.sssp(s64[i:i + 1], out_i) for i in range(64)], torch, dev, 1)
         record("sssp_x64", ms, 64, g.sssp(s64[:4], out4, stats=True)[2])
         depth = torch.empty((128, n), dtype=torch.int32, device=dev)
-        g.bfs_batched(src[:64], depth[:64])
+        g.bfs_batched(src, depth)  # warm-up with the timed call's shape (workspace sized once)
         ms = _time_cuda(lambda: g.bfs_batched(src, depth), torch, dev, 1)
         _, bst = g.bfs_batched(src, depth)
         record("bfs_batched_x128", ms, 128, bst)
@@ -228,7 +228,10 @@ def run_suite(a):
         dt = torch.empty(n, dtype=torch.float32, device=dev)
         dw = torch.empty(m, dtype=torch.float32, device=dev)
         popts = dict(tol_l1=1e-6, max_iters=200, weighted=True)
+        # Warm-ups: the one-time setup (fp32 weights, transposed weights, the
+        # symmetry check, workspaces) stays out of the timed calls.
         g.pagerank(None, x, **popts)
+        g.pagerank_backward(x, c, dteleport=dt, dweights=dw, **popts)
         tf = _time_cuda(lambda: g.pagerank(None, x, **popts), torch, dev, 1)
         _, fst = g.pagerank(None, x, **popts)
         tb = _time_cuda(lambda: g.pagerank_backward(x, c, dteleport=dt, dweights=dw, **popts), torch, dev, 1)

@@ -179,47 +179,72 @@ __global__ void build_wtn(const int64_t *index, const int32_t *nbr, const float 
 
 }  // namespace
 
-// Flags an edge without its reverse (missing) or whose reverse carries a
-// different weight (wdiff).  Rows are sorted, so the reverse slot is found by
-// binary search in row u.
-__global__ void check_symmetry(const int64_t *index, const int32_t *nbr, const float *w, int32_t n, int *missing,
-                               int *wdiff) {
+// Edge-multiset hashing: each edge v->u (v != u) hashes its unordered key
+// (min, max) -- and, for the weighted sums, its weight bits -- and adds the
+// hash to the "lo" sum when v < u, else to the "hi" sum.  The edge multiset
+// equals its reverse exactly when every lo sum equals its hi sum, up to a
+// collision of two independent 64-bit hashes (SplitMix64 finaliser, Steele et
+// al. 2014) of wrapping sums.  One streaming pass, no searches, any row order.
+__device__ __forceinline__ uint64_t mix_u64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__global__ void edge_hash_sums(const int64_t *index, const int32_t *nbr, const uint32_t *wbits, int32_t n,
+                               unsigned long long *acc) {
+    __shared__ unsigned long long s_red[32];
+    unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // {struct, weight} x {hash a, hash b} x {lo, hi}
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
         const int64_t b = index[v], e = index[v + 1];
         for (int64_t i = b + lane; i < e; i += 32) {
             const int32_t u = nbr[i];
-            int64_t lo = index[u], hi = index[u + 1];
-            while (lo < hi) {
-                const int64_t mid = (lo + hi) >> 1;
-                if (nbr[mid] < v) lo = mid + 1; else hi = mid;
+            if (u == v) continue;
+            const uint64_t lo = (uint64_t)(uint32_t)min(u, v), hi = (uint64_t)(uint32_t)max(u, v);
+            const uint64_t key = (lo << 32) | hi;
+            const int side = v < u ? 0 : 1;
+            const uint64_t ha = mix_u64(key + 0x9e3779b97f4a7c15ull);
+            const uint64_t hb = mix_u64(key ^ 0xd1b54a32d192ed03ull);
+            h[0 + side] += ha;
+            h[2 + side] += hb;
+            if (wbits) {
+                const uint64_t wk = mix_u64((uint64_t)wbits[i] + 0x632be59bd9b4e019ull);
+                h[4 + side] += mix_u64(ha ^ wk);
+                h[6 + side] += mix_u64(hb + wk);
             }
-            if (lo >= index[u + 1] || nbr[lo] != v) *missing = 1;
-            else if (w && w[lo] != w[i]) *wdiff = 1;
         }
     }
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const unsigned long long t = block_sum(h[j], s_red);
+        if (threadIdx.x == 0 && t) atomicAdd(acc + j, t);
+    }
+}
+
+hc_status edge_symmetry(hc_graph *g, const uint32_t *wbits, bool *structure, bool *weights) {
+    DevBuf acc;
+    HC_TRY(acc.ensure(8 * sizeof(unsigned long long)));
+    HC_CUDA_TRY(cudaMemsetAsync(acc.ptr, 0, 8 * sizeof(unsigned long long), g->stream));
+    { edge_hash_sums<<<g->sm_count * 8, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), wbits, g->N,
+                                                             acc.as<unsigned long long>()); ::hc::count_launch(); }
+    HC_CUDA_TRY(cudaGetLastError());
+    unsigned long long h[8];
+    HC_CUDA_TRY(cudaMemcpyAsync(h, acc.ptr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    *structure = h[0] == h[1] && h[2] == h[3];
+    *weights = *structure && (!wbits || (h[4] == h[5] && h[6] == h[7]));
+    return HC_OK;
 }
 
 hc_status ensure_pr_symmetry(hc_graph *g, bool weighted, bool *symmetric) {
     if (g->pr_sym_struct < 0 || (weighted && g->pr_sym_w < 0)) {
-        if (!g->rows_sorted) {
-            g->pr_sym_struct = 0;
-            g->pr_sym_w = 0;
-        } else {
-            const float *w = weighted ? pr_weights(g) : nullptr;
-            DevBuf flags;
-            HC_TRY(flags.ensure(2 * sizeof(int)));
-            HC_CUDA_TRY(cudaMemsetAsync(flags.ptr, 0, 2 * sizeof(int), g->stream));
-            { check_symmetry<<<g->sm_count * 8, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), w,
-                                                                     g->N, flags.as<int>(), flags.as<int>() + 1); ::hc::count_launch(); }
-            HC_CUDA_TRY(cudaGetLastError());
-            int h[2] = {0, 0};
-            HC_CUDA_TRY(cudaMemcpyAsync(h, flags.ptr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
-            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-            g->pr_sym_struct = !h[0];
-            if (weighted) g->pr_sym_w = !h[0] && !h[1];
-        }
+        const uint32_t *w = weighted ? reinterpret_cast<const uint32_t *>(pr_weights(g)) : nullptr;
+        bool st = false, ws = false;
+        HC_TRY(edge_symmetry(g, w, &st, &ws));
+        g->pr_sym_struct = st;
+        if (weighted) g->pr_sym_w = ws;
     }
     *symmetric = weighted ? g->pr_sym_w == 1 : g->pr_sym_struct == 1;
     return HC_OK;

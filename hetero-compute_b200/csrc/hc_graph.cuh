@@ -101,6 +101,9 @@ hc_status ensure_pr_derived(hc_graph *g, bool weighted);
 // Whether the PageRank transition is a reversible walk (symmetric structure,
 // and symmetric weights when `weighted`), checked once per graph.
 hc_status ensure_pr_symmetry(hc_graph *g, bool weighted, bool *symmetric);
+// Whether every edge u->v has a reverse v->u (as multisets), and whether the
+// reverse carries the same weight bits (`wbits` may be null).
+hc_status edge_symmetry(hc_graph *g, const uint32_t *wbits, bool *structure, bool *weights);
 // The edge weights as fp32 for weighted PageRank: the weight array itself
 // (fp32 graphs) or its converted copy (int32 graphs, built by ensure_pr_derived).
 const float *pr_weights(const hc_graph *g);

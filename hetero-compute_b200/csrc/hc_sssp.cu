@@ -494,10 +494,8 @@ __global__ void count_finite(const int32_t *dist, int32_t n, unsigned long long 
     if (threadIdx.x == 0 && c) atomicAdd(out, c);
 }
 
-// Negative weights, their sum, and whether w(u->v) == w(v->u) everywhere
-// (binary search of the reverse slot; rows must be sorted).
-__global__ void weight_stats(const int64_t *index, const int32_t *nbr, const int32_t *w, int32_t n, int check_sym,
-                             int *neg, int *asym, unsigned long long *sum) {
+// Whether any weight is negative, and the weights' sum.
+__global__ void weight_stats(const int64_t *index, const int32_t *w, int32_t n, int *neg, unsigned long long *sum) {
     __shared__ unsigned long long s_red[32];
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -508,15 +506,6 @@ __global__ void weight_stats(const int64_t *index, const int32_t *nbr, const int
             const int32_t x = w[i];
             if (x < 0) *neg = 1;
             s += (unsigned long long)max(x, 0);
-            if (check_sym) {
-                const int32_t u = nbr[i];
-                int64_t lo = index[u], hi = index[u + 1];
-                while (lo < hi) {
-                    const int64_t mid = (lo + hi) >> 1;
-                    if (nbr[mid] < v) lo = mid + 1; else hi = mid;
-                }
-                if (lo >= index[u + 1] || nbr[lo] != v || w[lo] != x) *asym = 1;
-            }
         }
     }
     s = block_sum(s, s_red);
@@ -581,9 +570,8 @@ hc_status ensure_weight_stats(hc_graph *g) {
     int *flags = buf.as<int>();
     unsigned long long *sum = reinterpret_cast<unsigned long long *>(buf.as<char>() + 16);
     {
-        weight_stats<<<g->sm_count * 8, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(),
-                                                             g->wgt.as<int32_t>(), g->N, g->rows_sorted, flags,
-                                                             flags + 1, sum);
+        weight_stats<<<g->sm_count * 8, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->wgt.as<int32_t>(), g->N,
+                                                             flags, sum);
         ::hc::count_launch();
     }
     HC_CUDA_TRY(cudaGetLastError());
@@ -593,7 +581,10 @@ hc_status ensure_weight_stats(hc_graph *g) {
     HC_CUDA_TRY(cudaMemcpyAsync(&hsum, sum, 8, cudaMemcpyDeviceToHost, g->stream));
     HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
     g->w_negative = hf[0];
-    g->w_symmetric = g->rows_sorted && !hf[1];
+    // Symmetric weights (w(u->v) == w(v->u) for every edge): one hashing pass.
+    bool st = false, ws = false;
+    HC_TRY(edge_symmetry(g, reinterpret_cast<const uint32_t *>(g->wgt.ptr), &st, &ws));
+    g->w_symmetric = ws;
     g->w_mean = g->M ? (double)hsum / (double)g->M : 1.0;
     g->wstats_done = 1;
     return HC_OK;

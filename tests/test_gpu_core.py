@@ -161,6 +161,38 @@ def test_sssp_asymmetric_weights_use_push():
         assert oracle.verify_sp_tree(host.index, host.neighbors, w, d, parent[i], s) == 0
 
 
+def test_sssp_one_asymmetric_weight_disables_pull():
+    """A single edge whose reverse has another weight: the symmetry hash must see it (pull sweeps would read
+    the reverse weight), and every epoch stays push."""
+    host = hc.gen_kronecker(12, 8, 4, wtype=hc.W_I32)
+    w = host.weights.copy()
+    src = hc.pick_sources(host, 4)
+    u = int(src[0])
+    e = int(host.index[u])  # the first edge of a source row: on every shortest-path tree from it
+    w[e] = 1 if w[e] != 1 else 2
+    g = hc.Graph(host.index, host.neighbors, w)
+    dist, _, _ = g.sssp(src, pull_alpha=1000000)
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, w, s)), i
+
+
+def test_sssp_pull_on_unsorted_rows():
+    """Rows in shuffled order (symmetric weights): pull sweeps stay enabled and exact."""
+    host = hc.gen_kronecker(12, 8, 5, wtype=hc.W_I32)
+    rng = np.random.default_rng(3)
+    nbr, w = host.neighbors.copy(), host.weights.copy()
+    for v in range(host.num_nodes):
+        b, e = host.index[v], host.index[v + 1]
+        if e - b > 1:
+            p = rng.permutation(e - b) + b
+            nbr[b:e], w[b:e] = nbr[p], w[p]
+    g = hc.Graph(host.index, nbr, w)
+    src = hc.pick_sources(host, 4)
+    dist, _, st = g.sssp(src, pull_alpha=1000000, stats=True)
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, nbr, w, s)), i
+
+
 def test_sssp_grid_against_dijkstra():
     host = hc.gen_grid(200, 300, 3, wtype=hc.W_I32)
     g = hc.Graph.from_host(host)
