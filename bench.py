@@ -311,8 +311,23 @@ def run_suite(a):
 
 def profile_case(a):
     """One source of BFS and SSSP, then one PageRank solve: the launches an ncu
-    capture of bfs_persistent / sssp_persistent / pr_sweep selects."""
+    capture of bfs_persistent / sssp_persistent / sssp_pull_kernel / pr_sweep
+    selects.  With --suite batched: one 512-source batched BFS and one
+    256-source batched SSSP (device outputs)."""
     import hc
+    if a.suite == "batched":
+        import torch
+        host = hc.gen_kronecker(a.scale, a.edge_factor, a.seed, hc.W_I32)
+        g = hc.Graph.from_host(host)
+        src = hc.pick_sources(host, 512)
+        out = torch.empty((512, host.num_nodes), dtype=torch.int32, device="cuda")
+        # Host-driven epoch loops, so that each kernel is a plain launch for the profiler.
+        g.bfs_batched(src, out, use_graph=hc.GRAPH_OFF)
+        g.sssp_batched(src[:256], out[:256], group=256, use_graph=hc.GRAPH_OFF)
+        torch.cuda.synchronize()
+        g.close()
+        print(json.dumps({"mode": "profile", "suite": "batched", "scale": a.scale, "num_edges": host.num_edges}))
+        return
     host = hc.gen_kronecker(a.scale, a.edge_factor, a.seed, hc.W_I32)
     g = hc.Graph.from_host(host)
     src = hc.pick_sources(host, 1)

@@ -59,18 +59,25 @@ __device__ __forceinline__ bool ctl_pull(const MsspCtl *ctl, int c) {
     return ctl->pull_alpha > 0 && (double)ctl->qedges[c] * ctl->pull_alpha > (double)ctl->m;
 }
 
-template <int SPL>
+// A lane's SPL distances of one vertex.  kL1: through L1 (neighbour rows,
+// which many warps of an SM read: most edges point at a few thousand hub
+// rows); a value cached earlier in the same launch may be stale, but
+// distances only fall, so it is an upper bound, and the vertex that lowered
+// it is active for the next epoch.  Otherwise L2 only (rows this warp owns).
+template <int SPL, bool kL1 = false>
 __device__ __forceinline__ void load_row(const int32_t *p, int32_t (&d)[SPL]) {
     if constexpr (SPL == 1) {
-        d[0] = __ldcg(p);
+        d[0] = kL1 ? __ldca(p) : __ldcg(p);
     } else if constexpr (SPL == 2) {
-        const int2 x = __ldcg(reinterpret_cast<const int2 *>(p));
+        const int2 *q = reinterpret_cast<const int2 *>(p);
+        const int2 x = kL1 ? __ldca(q) : __ldcg(q);
         d[0] = x.x;
         d[1] = x.y;
     } else {
 #pragma unroll
         for (int h = 0; h < SPL / 4; h++) {
-            const int4 x = __ldcg(reinterpret_cast<const int4 *>(p) + h);
+            const int4 *q = reinterpret_cast<const int4 *>(p) + h;
+            const int4 x = kL1 ? __ldca(q) : __ldcg(q);
             d[4 * h] = x.x;
             d[4 * h + 1] = x.y;
             d[4 * h + 2] = x.z;
@@ -118,6 +125,11 @@ __global__ void mssp_seed(int nsrc, const int32_t *src, const int64_t *index, in
 
 // Relax edges [e0, e1) of row u for the active lanes in `m`; du = this lane's
 // distances of u.
+// Edges (push) or neighbours (pull) a warp keeps in flight: four, or two
+// when a lane holds 16 distances per vertex (register budget).
+template <int SPL>
+constexpr int kInflight = SPL >= 16 ? 2 : 4;
+
 template <int SPL>
 __device__ __forceinline__ void relax_range(const int64_t *index, const int32_t *nbr, const int32_t *w,
                                             int32_t *dist, uint32_t m, const int32_t (&du)[SPL], int64_t e0,
@@ -134,20 +146,21 @@ __device__ __forceinline__ void relax_range(const int64_t *index, const int32_t 
             vv = nbr[my];
             ww = w[my];
         }
-        for (int j0 = 0; j0 < cnt; j0 += 4) {
-            int32_t v[4], wt[4], d[4][SPL];
-            bool ok[4], imp[4];
+        constexpr int F = kInflight<SPL>;
+        for (int j0 = 0; j0 < cnt; j0 += F) {
+            int32_t v[F], wt[F], d[F][SPL];
+            bool ok[F], imp[F];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < F; k++) {
                 const int idx = j0 + k;
                 v[k] = __shfl_sync(kFull, vv, idx & 31);
                 wt[k] = __shfl_sync(kFull, ww, idx & 31);
                 ok[k] = on && idx < cnt;
             }
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < F; k++) {
                 if (ok[k]) {
-                    load_row<SPL>(dist + (size_t)v[k] * K + lane * SPL, d[k]);
+                    load_row<SPL, true>(dist + (size_t)v[k] * K + lane * SPL, d[k]);
                 } else {
 #pragma unroll
                     for (int s = 0; s < SPL; s++) d[k][s] = kInfDist;
@@ -158,7 +171,7 @@ __device__ __forceinline__ void relax_range(const int64_t *index, const int32_t 
             // real improvement (values only fall between the load and the
             // atomic) at the price of an occasional redundant rescan.
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < F; k++) {
                 imp[k] = false;
 #pragma unroll
                 for (int s = 0; s < SPL; s++) {
@@ -169,11 +182,16 @@ __device__ __forceinline__ void relax_range(const int64_t *index, const int32_t 
                     }
                 }
             }
-            unsigned bal[4];
+            unsigned mybal = 0u;  // lane k < F: target k's new activity bits
+            int32_t myv = 0;
 #pragma unroll
-            for (int k = 0; k < 4; k++) bal[k] = __ballot_sync(kFull, imp[k]);
-            const unsigned mybal = lane == 0 ? bal[0] : lane == 1 ? bal[1] : lane == 2 ? bal[2] : lane == 3 ? bal[3] : 0u;
-            const int32_t myv = lane == 0 ? v[0] : lane == 1 ? v[1] : lane == 2 ? v[2] : v[3];
+            for (int k = 0; k < F; k++) {
+                const unsigned b = __ballot_sync(kFull, imp[k]);
+                if (lane == k) {
+                    mybal = b;
+                    myv = v[k];
+                }
+            }
             bool app = false;
             if (mybal) app = atomicOr(act_next + myv, mybal) == 0u;
             const unsigned ap = __ballot_sync(kFull, app);
@@ -312,10 +330,11 @@ __global__ void __launch_bounds__(256) mssp_pull(const int64_t *index, const int
             rel += (unsigned long long)__popc(aa) * SPL;
             unsigned live = __ballot_sync(kFull, aa != 0u);
             while (live) {
-                int32_t u[4], wt[4], d[4][SPL];
-                bool on[4];
+                constexpr int F = kInflight<SPL>;
+                int32_t u[F], wt[F], d[F][SPL];
+                bool on[F];
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
+                for (int k = 0; k < F; k++) {
                     const bool have = live != 0u;
                     const int idx = have ? __ffs(live) - 1 : 0;
                     if (have) live &= live - 1u;
@@ -325,16 +344,16 @@ __global__ void __launch_bounds__(256) mssp_pull(const int64_t *index, const int
                     on[k] = have && ((a >> lane) & 1u);
                 }
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
+                for (int k = 0; k < F; k++) {
                     if (on[k]) {
-                        load_row<SPL>(dist + (size_t)u[k] * K + lane * SPL, d[k]);
+                        load_row<SPL, true>(dist + (size_t)u[k] * K + lane * SPL, d[k]);
                     } else {
 #pragma unroll
                         for (int s = 0; s < SPL; s++) d[k][s] = kInfDist;
                     }
                 }
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
+                for (int k = 0; k < F; k++) {
 #pragma unroll
                     for (int s = 0; s < SPL; s++)
                         if (d[k][s] != kInfDist && d[k][s] + wt[k] < best[s]) best[s] = d[k][s] + wt[k];
@@ -454,17 +473,18 @@ __global__ void mssp_end(MsspCtl *ctl, int c, cudaGraphConditionalHandle cond, i
 template <int SPL>
 __global__ void mssp_transpose(const int32_t *dist, int32_t n, int nsrc, int32_t *out) {
     constexpr int K = 32 * SPL;
-    __shared__ int32_t tile[32][K + 1];
+    constexpr int TV = SPL >= 16 ? 16 : 32;  // vertices per tile (48 KB of static shared memory)
+    __shared__ int32_t tile[TV][K + 1];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-    for (int64_t vb = (int64_t)blockIdx.x * 32; vb < n; vb += (int64_t)gridDim.x * 32) {
-        for (int r = ty; r < 32; r += 8) {
+    for (int64_t vb = (int64_t)blockIdx.x * TV; vb < n; vb += (int64_t)gridDim.x * TV) {
+        for (int r = ty; r < TV; r += 8) {
             const int64_t v = vb + r;
             for (int c = tx; c < K; c += 32) tile[r][c] = v < n ? dist[(size_t)v * K + c] : 0;
         }
         __syncthreads();
         for (int s = ty; s < nsrc; s += 8) {
             const int64_t v = vb + tx;
-            if (v < n) out[(size_t)s * n + v] = tile[tx][s];
+            if (tx < TV && v < n) out[(size_t)s * n + v] = tile[tx][s];
         }
         __syncthreads();
     }
@@ -600,18 +620,18 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
     HC_CUDA_TRY(cudaMemcpy(src.data(), sources, sizeof(int32_t) * num_sources, cudaMemcpyDefault));
     for (int32_t s : src)
         if (s < 0 || s >= g->N) return fail(HC_ERR_INVALID_ARG, "hc_sssp_batched: source %d out of range", s);
-    // Group width: 32, 64, 128 or 256 sources.  The default is the widest
-    // whose distance matrix (N x width x 4 bytes) takes at most 40% of the
+    // Group width: 32, 64, 128, 256 or 512 sources.  The default is the widest
+    // up to 256 whose distance matrix (N x width x 4 bytes) takes at most 40% of the
     // free device memory, 80% with the staging buffer of host outputs (wider
     // groups share each row read among more sources).
     if (o.group <= 0) o.group = g->tune.mssp_group;
     if (o.switch_alpha == 0) o.switch_alpha = g->tune.mssp_switch_alpha;
-    int group = o.group <= 32 ? 32 : o.group <= 64 ? 64 : o.group <= 128 ? 128 : 256;
+    int group = o.group <= 32 ? 32 : o.group <= 64 ? 64 : o.group <= 128 ? 128 : o.group <= 256 ? 256 : 512;
     if (o.group <= 0) {
         size_t free_b = 0, total_b = 0;
         HC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
         free_b += g->ws_batch.bytes + g->ws_out0.bytes;  // workspaces are reused
-        group = 256;
+        group = 256;  // 512 reads twice the row bytes per edge for no gain per source
         while (group > 32 && (double)g->N * group * 4.0 > 0.4 * (double)free_b) group /= 2;
     }
     // Weights must be non-negative; pull epochs need symmetric weights.
@@ -640,7 +660,8 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
         if (group == 32) HC_TRY(run_group<1>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
         else if (group == 64) HC_TRY(run_group<2>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
         else if (group == 128) HC_TRY(run_group<4>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
-        else HC_TRY(run_group<8>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
+        else if (group == 256) HC_TRY(run_group<8>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
+        else HC_TRY(run_group<16>(g, src.data() + s0, k, dst, max_epochs, pull_alpha, use_graph, eg, &ep, relaxed));
         if (dist_out && !dev_out)
             HC_TRY(copy_out(dist_out + (size_t)s0 * n, dst, sizeof(int32_t) * (size_t)k * n, g->stream));
         epochs_max = std::max(epochs_max, ep);

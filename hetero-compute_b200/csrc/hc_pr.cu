@@ -479,23 +479,24 @@ __global__ void __launch_bounds__(kPrThreads) spmm_sweep(SpmmArgs a, PrPlanDev p
     }
 }
 
+// Start: each column's teleport t (base / (1-d)), which has the fixed
+// point's mass; vertices without edges sit at their base (1-d) t from the start.
 __global__ void spmm_init(int32_t n, int K, const float *basev, const int32_t *seed_off, const int32_t *seed_idx,
-                          float d, const float *ps, float *x, float *g, float *x2, float *g2, int32_t n_active) {
+                          const uint8_t *is_seed, float d, const float *ps, float *x, float *g, float *x2, float *g2,
+                          int32_t n_active) {
     const size_t total = (size_t)n * K;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const int32_t v = (int32_t)(i / K);
         const int c = (int)(i % K);
-        float t;
+        float base = 0.f;
         if (basev) {
-            t = basev[i];
-        } else {
-            t = 0.f;
+            base = basev[i];
+        } else if (is_seed[v]) {
             const int32_t b = seed_off[c], e = seed_off[c + 1];
             for (int32_t j = b; j < e; j++)
-                if (seed_idx[j] == v) t = (1.0f - d) / (float)(e - b);
+                if (seed_idx[j] == v) base = (1.0f - d) / (float)(e - b);
         }
-        // Start from the base; isolated vertices stay there.
-        (void)n_active;
+        const float t = v < n_active ? base / (1.0f - d) : base;
         x[i] = t;
         x2[i] = t;
         const float gv = ps ? t * ps[v] : t;
@@ -936,8 +937,8 @@ extern "C" hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t n
         { scale_vec<<<g->sm_count * 8, 256, 0, g->stream>>>(basev, 1.0f - o.damping, basev, nk); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaMemsetAsync(hub_count, 0, (size_t)(plan.n_hub + 1) * 4, g->stream));
         const float *ps = weighted ? nullptr : g->inv_deg.as<float>();
-        { spmm_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, K, basev, nullptr, nullptr, o.damping, ps, x[0],
-                                                          gv[0], x[1], gv[1], g->n_active); ::hc::count_launch(); }
+        { spmm_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, K, basev, nullptr, nullptr, nullptr, o.damping, ps,
+                                                          x[0], gv[0], x[1], gv[1], g->n_active); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
         SpmmArgs a{};
         a.index = g->index.as<int64_t>();
@@ -1235,8 +1236,8 @@ extern "C" hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, co
     HC_CUDA_TRY(cudaMemsetAsync(hub_count, 0, (size_t)(plan.n_hub + 1) * 4, g->stream));
     { mark_seeds<<<64, 256, 0, g->stream>>>(d_seeds, nseeds, is_seed); ::hc::count_launch(); }
     const float *ps = weighted ? nullptr : g->inv_deg.as<float>();
-    { spmm_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, K, nullptr, d_off, d_seeds, o.damping, ps, x[0], gv[0],
-                                                      x[1], gv[1], g->n_active); ::hc::count_launch(); }
+    { spmm_init<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, K, nullptr, d_off, d_seeds, is_seed, o.damping, ps,
+                                                      x[0], gv[0], x[1], gv[1], g->n_active); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     SpmmArgs a{};
     a.index = g->index.as<int64_t>();

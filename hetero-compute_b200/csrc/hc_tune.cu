@@ -153,13 +153,13 @@ hc_status tune_sssp_batched(Tuner &tu, hc_tuning &out) {
     if (g->wtype != HC_W_I32) return HC_OK;
     HC_TRY(ensure_weight_stats(g));
     if (g->w_negative) return HC_OK;
-    const int k = (int)std::min<size_t>(tu.src.size(), 256);
+    const int k = (int)std::min<size_t>(tu.src.size(), 512);
     // Widest group that fits, as hc_sssp_batched picks it untuned.
     size_t free_b = 0, total_b = 0;
     HC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     free_b += g->ws_batch.bytes + g->ws_out0.bytes;
     std::vector<int32_t> groups;
-    for (int32_t w : {64, 128, 256})
+    for (int32_t w : {64, 128, 256, 512})
         if ((double)g->N * w * 4.0 <= 0.4 * (double)free_b) groups.push_back(w);
     if (groups.empty()) groups.push_back(32);
     hc_batch_opts o{};

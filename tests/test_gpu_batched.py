@@ -66,7 +66,7 @@ def test_sssp_batched_distances(scale, k):
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s)), i
 
 
-@pytest.mark.parametrize("group", [32, 64, 128, 256])
+@pytest.mark.parametrize("group", [32, 64, 128, 256, 512])
 def test_sssp_batched_group_widths(group):
     host = hc.gen_kronecker(11, 16, 42, wtype=hc.W_I32)
     g = hc.Graph.from_host(host)
