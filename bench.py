@@ -611,10 +611,14 @@ def main():
             traffic = json.load(open(tpath)).get(f"s{a.scale}", {}).get(dom)
         except Exception:
             traffic = None
-    roof = {"bound": "hbm", "kernel": {"bfs": "bfs_persistent", "sssp": "sssp_persistent",
+    roof = {"bound": "hbm", "kernel": {"bfs": "bfs_persistent",
+                                       "sssp": "sssp_persistent + sssp_pull_kernel",
                                        "pagerank": "pr_sweep"}[dom],
             "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm if achieved else None, "peak_kind": peak_kind, "traffic": traffic}
+            "frac": achieved / hbm if achieved else None, "peak_kind": peak_kind, "traffic": traffic,
+            "traffic_unit": "DRAM bytes per source (per solve for pagerank), one ncu capture "
+                            "(profiles/traffic.json)" if traffic else None,
+            "bytes_model_per_unit": per_algo[dom]["bytes_model"] / (k if dom != "pagerank" else 1)}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
