@@ -365,14 +365,16 @@ struct SpmmArgs {
     float *partials;         // [chunks][K]
     unsigned *hub_count;
     double *col_l1;          // [K] accumulators for this sweep
-    int K;
+    const int32_t *col_map;  // packed column -> seed-list column (null: identity)
+    int K;                   // columns in the packed layout
     int32_t n_active;
 };
 
 __device__ __forceinline__ float spmm_base(const SpmmArgs &a, int32_t r, int c, float one_minus_d) {
     if (a.basev) return a.basev[(size_t)r * a.K + c];
     // Uniform over the seed set of column c.
-    const int32_t b = a.seed_off[c], e = a.seed_off[c + 1];
+    const int cc = a.col_map ? a.col_map[c] : c;
+    const int32_t b = a.seed_off[cc], e = a.seed_off[cc + 1];
     for (int32_t i = b; i < e; i++)
         if (a.seed_idx[i] == r) return one_minus_d / (float)(e - b);
     return 0.f;
@@ -503,6 +505,52 @@ __global__ void spmm_init(int32_t n, int K, const float *basev, const int32_t *s
         g[i] = gv;
         g2[i] = gv;
     }
+}
+
+// Repacks the live columns of x ([n][kw]) into xo ([n][nkw], gather copy go =
+// xo * ps when go is set); a column with newpos < 0 has converged and goes to
+// its place col_map[c] in out ([n][K0]).  Rows stay contiguous on both sides.
+__global__ void spmm_repack(int32_t n, int kw, const float *x, const int32_t *newpos, const int32_t *col_map,
+                            int K0, float *out, int nkw, float *xo, float *go, const float *ps) {
+    const size_t total = (size_t)n * kw;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int32_t v = (int32_t)(i / kw);
+        const int c = (int)(i % kw);
+        const float val = x[i];
+        const int np = newpos[c];
+        if (np < 0) {
+            out[(size_t)v * K0 + col_map[c]] = val;
+        } else {
+            xo[(size_t)v * nkw + np] = val;
+            if (go) go[(size_t)v * nkw + np] = ps ? val * ps[v] : val;
+        }
+    }
+}
+
+// One packed column c (width kw) as a plain vector (and its gather copy).
+__global__ void spmm_take_column(int32_t n, int kw, int c, const float *x, const float *ps, float *x0, float *x1,
+                                 float *g0, float *g1) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const float val = x[(size_t)v * kw + c];
+        x0[v] = val;
+        x1[v] = val;
+        if (g0) {
+            const float gv = ps ? val * ps[v] : val;
+            g0[v] = gv;
+            g1[v] = gv;
+        }
+    }
+}
+
+// base[v] = (1-d) / |seeds| on the seeds of one column (base zeroed before).
+__global__ void spmm_column_base(const int32_t *seed_idx, int32_t b, int32_t e, float one_minus_d, float *base) {
+    for (int i = b + blockIdx.x * blockDim.x + threadIdx.x; i < e; i += gridDim.x * blockDim.x)
+        base[seed_idx[i]] = one_minus_d / (float)(e - b);
+}
+
+__global__ void spmm_put_column(int32_t n, const float *x, int K0, int oc, float *out) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        out[(size_t)v * K0 + oc] = x[v];
 }
 
 __global__ void mark_seeds(const int32_t *seed_idx, int32_t nseeds, uint8_t *is_seed) {
@@ -1214,7 +1262,7 @@ extern "C" hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, co
     const int64_t n = g->N;
     const size_t nk = (size_t)n * K;
     const size_t bytes = 4 * nk * sizeof(float) + (size_t)(partial_slots + 1) * K * 4 + (size_t)(plan.n_hub + 1) * 4 +
-                         (size_t)K * 8 + (size_t)n + (size_t)(nseeds + ncols + 1) * 4 + 8192;
+                         (size_t)K * 8 + (size_t)n + (size_t)(nseeds + ncols + 1) * 4 + 5 * (size_t)n * 4 + 16384;
     HC_TRY(g->ws_pr.ensure(bytes));
     char *p = g->ws_pr.as<char>();
     auto take = [&](size_t b) {
@@ -1230,6 +1278,9 @@ extern "C" hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, co
     uint8_t *is_seed = (uint8_t *)take((size_t)n);
     int32_t *d_off = (int32_t *)take((size_t)(ncols + 1) * 4);
     int32_t *d_seeds = (int32_t *)take((size_t)nseeds * 4);
+    float *col_x[2] = {(float *)take((size_t)n * 4), (float *)take((size_t)n * 4)};
+    float *col_g[2] = {(float *)take((size_t)n * 4), (float *)take((size_t)n * 4)};
+    float *col_base = (float *)take((size_t)n * 4);
     HC_CUDA_TRY(cudaMemcpyAsync(d_off, off.data(), (ncols + 1) * 4, cudaMemcpyHostToDevice, g->stream));
     HC_CUDA_TRY(cudaMemcpyAsync(d_seeds, sd.data(), (size_t)nseeds * 4, cudaMemcpyHostToDevice, g->stream));
     HC_CUDA_TRY(cudaMemsetAsync(is_seed, 0, (size_t)n, g->stream));
@@ -1253,42 +1304,161 @@ extern "C" hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, co
     a.col_l1 = col_l1;
     a.K = K;
     a.n_active = g->n_active;
-    HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
-    int it = 0;
+    // Columns converge at their own pace (personalised teleports differ):
+    // a column whose L1 change falls below tol is final.  Whenever the live
+    // columns fit fewer 32-column chunks, one pass writes the final ones to
+    // the output and packs the live ones tighter, so later sweeps gather only
+    // live columns.
+    const bool dev_out = is_device_pointer(scores_out);
+    float *out = scores_out;
+    if (!dev_out) {
+        HC_TRY(g->ws_out0.ensure(nk * 4));
+        out = g->ws_out0.as<float>();
+    }
+    HC_TRY(g->ws_src.ensure((size_t)2 * K * 4));
+    int32_t *d_map = g->ws_src.as<int32_t>();
+    int32_t *d_newpos = d_map + K;
+    std::vector<int32_t> hmap(K), hpos(K);
+    for (int c = 0; c < K; c++) hmap[c] = c;
+    HC_CUDA_TRY(cudaMemcpyAsync(d_map, hmap.data(), (size_t)K * 4, cudaMemcpyHostToDevice, g->stream));
+    a.col_map = d_map;
+    auto repack = [&](int cur, int kw, int nkw) -> hc_status {
+        HC_CUDA_TRY(cudaMemcpyAsync(d_newpos, hpos.data(), (size_t)kw * 4, cudaMemcpyHostToDevice, g->stream));
+        {
+            spmm_repack<<<g->sm_count * 8, 256, 0, g->stream>>>(g->N, kw, x[cur], d_newpos, d_map, K, out, nkw,
+                                                                x[cur ^ 1], weighted ? nullptr : gv[cur ^ 1], ps);
+            ::hc::count_launch();
+        }
+        HC_CUDA_TRY(cudaGetLastError());
+        // Rows without edges (past n_active) are never written by a sweep:
+        // give the buffer the next sweep writes their values in the new layout.
+        if (nkw > 0 && g->n_active < g->N)
+            HC_CUDA_TRY(cudaMemcpyAsync(x[cur] + (size_t)g->n_active * nkw, x[cur ^ 1] + (size_t)g->n_active * nkw,
+                                        (size_t)(g->N - g->n_active) * nkw * 4, cudaMemcpyDeviceToDevice, g->stream));
+        return HC_OK;
+    };
+    // The single-column solver's run_solve records g's events: this call
+    // times itself with its own pair.
+    cudaEvent_t ev0, ev1;
+    HC_CUDA_TRY(cudaEventCreate(&ev0));
+    HC_CUDA_TRY(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } ev_guard{ev0, ev1};
+    HC_CUDA_TRY(cudaEventRecord(ev0, g->stream));
+    int it = 0, cur = 0, kw = K;
     std::vector<double> hl1(K);
+    double bytes_model = 0, mx = 0;
     bool conv = false;
-    for (; it < o.max_iters && !conv; it++) {
-        a.gin = weighted ? x[it & 1] : gv[it & 1];
-        a.xin = x[it & 1];
-        a.xout = x[(it + 1) & 1];
-        a.gout = weighted ? a.xout : gv[(it + 1) & 1];
-        HC_CUDA_TRY(cudaMemsetAsync(col_l1, 0, (size_t)K * 8, g->stream));
-        const int cols = (K + 31) / 32;
+    // A few slow columns (a seed set in a small bipartite component converges
+    // at rate d) finish on the single-column sweeps, which gather 4 bytes per
+    // edge instead of a 32-column row segment.
+    constexpr int kSingleCols = 4;
+    for (; it < o.max_iters && kw > (K > kSingleCols ? kSingleCols : 0); it++) {
+        a.K = kw;
+        a.gin = weighted ? x[cur] : gv[cur];
+        a.xin = x[cur];
+        a.xout = x[cur ^ 1];
+        a.gout = weighted ? a.xout : gv[cur ^ 1];
+        HC_CUDA_TRY(cudaMemsetAsync(col_l1, 0, (size_t)kw * 8, g->stream));
+        const int cols = (kw + 31) / 32;
         const int grid = g->sm_count * 8;
         if (cols <= 1) { spmm_sweep<1><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed); ::hc::count_launch(); }
         else if (cols <= 2) { spmm_sweep<2><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed); ::hc::count_launch(); }
         else if (cols <= 4) { spmm_sweep<4><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed); ::hc::count_launch(); }
         else { spmm_sweep<8><<<grid, kPrThreads, 0, g->stream>>>(a, plan, is_seed); ::hc::count_launch(); }
         HC_CUDA_TRY(cudaGetLastError());
-        HC_CUDA_TRY(cudaMemcpyAsync(hl1.data(), col_l1, (size_t)K * 8, cudaMemcpyDeviceToHost, g->stream));
+        bytes_model += 8.0 * (n + 1) + 4.0 * g->M * (weighted ? 2 : 1) + 12.0 * (double)n * kw;
+        cur ^= 1;
+        HC_CUDA_TRY(cudaMemcpyAsync(hl1.data(), col_l1, (size_t)kw * 8, cudaMemcpyDeviceToHost, g->stream));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        double mx = 0;
-        for (double v : hl1) mx = std::max(mx, v);
-        conv = o.tol_l1 > 0.f && mx < (double)o.tol_l1;
+        int live = 0;
+        mx = 0;
+        for (int c = 0; c < kw; c++) {
+            mx = std::max(mx, hl1[c]);
+            const bool done = o.tol_l1 > 0.f && hl1[c] < (double)o.tol_l1;
+            hpos[c] = done ? -1 : live++;
+        }
+        if (live == 0) {
+            conv = true;
+            HC_TRY(repack(cur, kw, 0));  // every column is final
+            kw = 0;
+        } else if ((live + 31) / 32 < (kw + 31) / 32 || (live <= kSingleCols && kw > kSingleCols)) {
+            HC_TRY(repack(cur, kw, live));
+            std::vector<int32_t> nmap(live);
+            for (int c = 0; c < kw; c++)
+                if (hpos[c] >= 0) nmap[hpos[c]] = hmap[c];
+            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));  // d_map is read by the repack
+            hmap = nmap;
+            HC_CUDA_TRY(cudaMemcpyAsync(d_map, hmap.data(), (size_t)live * 4, cudaMemcpyHostToDevice, g->stream));
+            cur ^= 1;
+            kw = live;
+        }
     }
-    HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
-    HC_TRY(copy_out(scores_out, x[it & 1], nk * 4, g->stream));
+    int tail_iters = 0;
+    if (kw > 0 && it < o.max_iters) {
+        // Each remaining column continues from its packed values on the
+        // single-column sweeps (teleport vector, same stopping rule).
+        SweepArgs sa{};
+        sa.index = g->index.as<int64_t>();
+        sa.nbr = g->nbr.as<int32_t>();
+        sa.ew = weighted ? g->wtn.as<float>() : nullptr;
+        sa.basev = col_base;
+        sa.d = o.damping;
+        sa.ps = ps;
+        sa.partials = partials;
+        sa.hub_count = hub_count;
+        sa.st = reinterpret_cast<IterState *>(g->ws_ctl.ptr);
+        sa.tol_l1 = o.tol_l1;
+        sa.eps = 3.4e38f;
+        sa.max_iters = o.max_iters - it;
+        sa.n_active = g->n_active;
+        SweepFn fn = pick_sweep(weighted, false, !weighted, true);
+        HC_TRY(g->ws_ctl.ensure(sizeof(IterState) + 4096));
+        sa.st = reinterpret_cast<IterState *>(g->ws_ctl.ptr);
+        bool all_conv = true;
+        for (int c = 0; c < kw; c++) {
+            const int oc = hmap[c];
+            HC_CUDA_TRY(cudaMemsetAsync(col_base, 0, (size_t)n * 4, g->stream));
+            { spmm_column_base<<<4, 256, 0, g->stream>>>(d_seeds, off[oc], off[oc + 1], 1.0f - o.damping, col_base); ::hc::count_launch(); }
+            {
+                spmm_take_column<<<g->sm_count * 4, 256, 0, g->stream>>>(g->N, kw, c, x[cur], ps, col_x[0], col_x[1],
+                                                                         weighted ? nullptr : col_g[0],
+                                                                         weighted ? nullptr : col_g[1]);
+                ::hc::count_launch();
+            }
+            HC_CUDA_TRY(cudaGetLastError());
+            SolveResult r;
+            HC_TRY(run_solve(g, sa, plan, fn, col_x, col_g, !weighted, &r));
+            { spmm_put_column<<<g->sm_count * 4, 256, 0, g->stream>>>(g->N, col_x[r.iters & 1], K, oc, out); ::hc::count_launch(); }
+            HC_CUDA_TRY(cudaGetLastError());
+            tail_iters = std::max(tail_iters, r.iters);
+            all_conv = all_conv && r.done == 1;
+            mx = std::max(mx, r.l1);
+            bytes_model += (double)r.iters * (8.0 * (n + 1) + 4.0 * g->M * (weighted ? 2 : 1) + 12.0 * (double)n);
+        }
+        conv = all_conv;
+        kw = 0;
+    }
+    if (kw > 0) {  // iteration cap: the live columns as they stand
+        for (int c = 0; c < kw; c++) hpos[c] = -1;
+        HC_TRY(repack(cur, kw, 0));
+    }
+    HC_CUDA_TRY(cudaEventRecord(ev1, g->stream));
+    if (!dev_out) HC_TRY(copy_out(scores_out, out, nk * 4, g->stream));
     HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
     float ms = 0;
-    HC_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_start, g->ev_stop));
+    HC_CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
     if (stats) {
-        double mx = 0;
-        for (double v : hl1) mx = std::max(mx, v);
-        stats->iterations = it;
+        stats->iterations = it + tail_iters;
         stats->converged = conv;
         stats->residual_l1 = (float)mx;
         stats->ms = ms;
-        stats->bytes_model = (double)it * (8.0 * (n + 1) + 4.0 * g->M * (weighted ? 2 : 1) + 12.0 * (double)n * K);
+        stats->bytes_model = bytes_model;
     }
     return HC_OK;
 }

@@ -163,6 +163,30 @@ def test_ppr_batched_against_dense(weighted):
         assert np.abs(scores[:, c] - x).max() < 1e-6, c
 
 
+def test_ppr_batched_columns_stop_at_their_own_pace():
+    """70 columns (three 32-column chunks) converging after different sweep counts: converged columns
+    leave the packed state, host and device outputs agree, every column matches the FP64 solve."""
+    torch = pytest.importorskip("torch")
+    host = hc.gen_kronecker(12, 16, 8)
+    g = hc.Graph.from_host(host)
+    rng = np.random.default_rng(5)
+    k = 70
+    sizes = rng.integers(1, 33, size=k)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    active = np.flatnonzero(host.degrees() > 0)
+    seeds = np.concatenate([rng.choice(active, s, replace=False) for s in sizes]).astype(np.int32)
+    scores, st = g.ppr_batched(off, seeds, tol_l1=1e-7, max_iters=300)
+    assert st.converged
+    dev = torch.empty((host.num_nodes, k), dtype=torch.float32, device="cuda")
+    g.ppr_batched(off, seeds, dev, tol_l1=1e-7, max_iters=300)
+    assert np.array_equal(dev.cpu().numpy(), scores)
+    for c in range(0, k, 3):
+        t = np.zeros(host.num_nodes)
+        t[seeds[off[c]:off[c + 1]]] = 1.0 / sizes[c]
+        x = oracle.pr_dense(host.index, host.neighbors, None, t)
+        assert np.abs(scores[:, c] - x).max() < 1e-6, c
+
+
 def test_dense_multicolumn_forward():
     host = hc.gen_kronecker(10, 16, 6)
     g = hc.Graph.from_host(host)
