@@ -427,20 +427,29 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
 
     const bool dev_depth = is_device_pointer(depth_out);
     const bool dev_parent = is_device_pointer(parent_out);
-    if (!dev_depth) HC_TRY(g->ws_out0.ensure(4 * n));
-    if (!dev_parent) HC_TRY(g->ws_out1.ensure(4 * n));
+    if (!depth_out) HC_TRY(g->ws_out0.ensure(4 * n));
+    if (!parent_out) HC_TRY(g->ws_out1.ensure(4 * n));
+    // Host outputs: staged on the device and copied while the next source runs.
+    const bool host_depth = depth_out && !dev_depth, host_parent = parent_out && !dev_parent;
+    OutPipe pipe;
+    if (host_depth || host_parent) HC_TRY(pipe.init(g, 2, 4 * n));
 
     double total_ms = 0;
     for (int32_t i = 0; i < num_sources; i++) {
         a.src = src[i];
-        a.depth = dev_depth ? depth_out + (size_t)i * n : g->ws_out0.as<int32_t>();
-        a.parent = dev_parent ? parent_out + (size_t)i * n : g->ws_out1.as<int32_t>();
+        int32_t *stage[2] = {nullptr, nullptr};
+        if (host_depth || host_parent) HC_TRY(pipe.acquire(i, stage));
+        a.depth = dev_depth ? depth_out + (size_t)i * n : host_depth ? stage[0] : g->ws_out0.as<int32_t>();
+        a.parent = dev_parent ? parent_out + (size_t)i * n : host_parent ? stage[1] : g->ws_out1.as<int32_t>();
         HC_CUDA_TRY(cudaMemsetAsync(a.ctl, 0, sizeof(BfsCtl), g->stream));
         HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
         HC_TRY(o.collect_stats ? launch_bfs<true>(g, a) : launch_bfs<false>(g, a));
         HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
-        if (depth_out && !dev_depth) HC_TRY(copy_out(depth_out + (size_t)i * n, a.depth, 4 * n, g->stream));
-        if (parent_out && !dev_parent) HC_TRY(copy_out(parent_out + (size_t)i * n, a.parent, 4 * n, g->stream));
+        if (host_depth || host_parent) {
+            void *dst[2] = {host_depth ? (void *)(depth_out + (size_t)i * n) : nullptr,
+                            host_parent ? (void *)(parent_out + (size_t)i * n) : nullptr};
+            HC_TRY(pipe.release(i, dst));
+        }
         BfsCtl c;
         HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
         if (o.collect_stats && stats) {
@@ -473,6 +482,7 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
                              c.trace[l].nf, (c.trace[l + 1].t_ns - c.trace[l].t_ns) * 1e-3);
         }
     }
+    if (host_depth || host_parent) HC_TRY(pipe.finish());
     if (stats) {
         stats->ms = total_ms;
         // Streamed bytes: 16 B offsets per scanned vertex, 4 B per scanned edge,

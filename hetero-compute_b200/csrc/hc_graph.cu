@@ -73,6 +73,58 @@ hc_status copy_out(void *dst_any, const void *src_dev, size_t bytes, cudaStream_
     return HC_OK;
 }
 
+hc_status OutPipe::init(hc_graph *graph, int arrays, size_t each) {
+    g = graph;
+    narr = arrays;
+    bytes = each;
+    pending = false;
+    if (!g->copy_stream) HC_CUDA_TRY(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
+    for (int s = 0; s < 2; s++) {
+        if (!g->ev_ready[s]) HC_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_ready[s], cudaEventDisableTiming));
+        if (!g->ev_done[s]) {
+            HC_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_done[s], cudaEventDisableTiming));
+            HC_CUDA_TRY(cudaEventRecord(g->ev_done[s], g->copy_stream));  // nothing to wait for yet
+        }
+        for (int j = 0; j < arrays; j++) HC_TRY(g->ws_stage[s][j].ensure(each));
+    }
+    return HC_OK;
+}
+
+hc_status OutPipe::acquire(int i, int32_t **bufs) {
+    HC_TRY(flush());
+    const int s = i & 1;
+    HC_CUDA_TRY(cudaStreamWaitEvent(g->stream, g->ev_done[s], 0));
+    for (int j = 0; j < narr; j++) bufs[j] = g->ws_stage[s][j].as<int32_t>();
+    return HC_OK;
+}
+
+hc_status OutPipe::release(int i, void *const *dst) {
+    const int s = i & 1;
+    HC_CUDA_TRY(cudaEventRecord(g->ev_ready[s], g->stream));
+    pending = true;
+    pend_slot = s;
+    for (int j = 0; j < narr; j++) pend_dst[j] = dst[j];
+    return HC_OK;
+}
+
+hc_status OutPipe::flush() {
+    if (!pending) return HC_OK;
+    pending = false;
+    const int s = pend_slot;
+    HC_CUDA_TRY(cudaStreamWaitEvent(g->copy_stream, g->ev_ready[s], 0));
+    for (int j = 0; j < narr; j++)
+        if (pend_dst[j])
+            HC_CUDA_TRY(cudaMemcpyAsync(pend_dst[j], g->ws_stage[s][j].ptr, bytes, cudaMemcpyDefault, g->copy_stream));
+    HC_CUDA_TRY(cudaEventRecord(g->ev_done[s], g->copy_stream));
+    return HC_OK;
+}
+
+hc_status OutPipe::finish() {
+    HC_TRY(flush());
+    HC_CUDA_TRY(cudaStreamSynchronize(g->copy_stream));
+    return HC_OK;
+}
+
 hc_status activate(hc_graph *g) {
     if (!g) return fail(HC_ERR_INVALID_ARG, "null graph handle");
     HC_CUDA_TRY(cudaSetDevice(g->device));
@@ -304,6 +356,8 @@ int64_t hc_graph::bytes_held() const {
                                 &ws_out0, &ws_out1, &ws_ctl, &ws_plan_ms, &ws_plan_mssp, &ws_src};
     int64_t t = 0;
     for (auto *b : bufs) t += (int64_t)b->bytes;
+    for (int s = 0; s < 2; s++)
+        for (int j = 0; j < 2; j++) t += (int64_t)ws_stage[s][j].bytes;
     return t;
 }
 
@@ -416,6 +470,13 @@ hc_status hc_graph_destroy(hc_graph *g) {
                       &g->pr_plan_huge_rows, &g->ws_bfs, &g->ws_sssp, &g->ws_pr, &g->ws_batch,
                       &g->ws_out0, &g->ws_out1, &g->ws_ctl, &g->ws_plan_ms, &g->ws_plan_mssp, &g->ws_src};
     for (auto *b : bufs) b->release();
+    if (g->copy_stream) cudaStreamSynchronize(g->copy_stream);
+    for (int s = 0; s < 2; s++) {
+        for (int j = 0; j < 2; j++) g->ws_stage[s][j].release();
+        if (g->ev_ready[s]) cudaEventDestroy(g->ev_ready[s]);
+        if (g->ev_done[s]) cudaEventDestroy(g->ev_done[s]);
+    }
+    if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
     g->pinned.release();
     if (g->ev_start) cudaEventDestroy(g->ev_start);
     if (g->ev_stop) cudaEventDestroy(g->ev_stop);

@@ -85,6 +85,11 @@ struct hc_graph {
     // autotuned launch parameters (zero fields: built-in defaults)
     hc_tuning tune{};
 
+    // host-output pipeline (per-source results copied while the next computes)
+    hc::DevBuf ws_stage[2][2];  // [slot][array]
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr};
+
     // workspaces
     hc::DevBuf ws_bfs, ws_sssp, ws_pr, ws_batch, ws_out0, ws_out1, ws_ctl, ws_src;
     hc::PinnedBuf pinned;
@@ -98,6 +103,30 @@ namespace hc {
 hc_status activate(hc_graph *g);
 // Builds inv_deg (and, for weighted graphs, inv_wsum / wtn) if missing.
 hc_status ensure_pr_derived(hc_graph *g, bool weighted);
+// Per-source outputs bound for host memory, double-buffered: source i writes
+// staging slot i & 1 on the compute stream, and its copy to the caller runs
+// on a copy stream while the next source computes (overlapped when the
+// destination is pinned).  Before a slot is written again the compute stream
+// waits for that slot's previous copy.
+struct OutPipe {
+    hc_graph *g = nullptr;
+    int narr = 0;
+    size_t bytes = 0;
+    bool pending = false;
+    int pend_slot = 0;
+    void *pend_dst[2] = {nullptr, nullptr};
+    // Staging and events for `arrays` outputs of `bytes` each.
+    hc_status init(hc_graph *graph, int arrays, size_t each);
+    // Staging buffers of source i (after the wait for the slot's last copy).
+    hc_status acquire(int i, int32_t **bufs);
+    // Source i's results are complete on the compute stream once what is
+    // queued there has run; copy them to dst[] (null entries are skipped).
+    // The copy is issued by the next acquire or by finish.
+    hc_status release(int i, void *const *dst);
+    hc_status flush();
+    hc_status finish();
+};
+
 // Whether the PageRank transition is a reversible walk (symmetric structure,
 // and symmetric weights when `weighted`), checked once per graph.
 hc_status ensure_pr_symmetry(hc_graph *g, bool weighted, bool *symmetric);

@@ -656,27 +656,35 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
 
     const bool dev_dist = is_device_pointer(dist_out);
     const bool dev_parent = is_device_pointer(parent_out);
-    if (!dev_dist) HC_TRY(g->ws_out0.ensure(4 * n));
-    if (parent_out && !dev_parent) HC_TRY(g->ws_out1.ensure(4 * n));
+    if (!dist_out) HC_TRY(g->ws_out0.ensure(4 * n));
+    // Host outputs: staged on the device and copied while the next source runs.
+    const bool host_dist = dist_out && !dev_dist, host_parent = parent_out && !dev_parent;
+    OutPipe pipe;
+    if (host_dist || host_parent) HC_TRY(pipe.init(g, 2, 4 * n));
 
     HC_TRY(g->pinned.ensure(sizeof(SsspCtl)));
     volatile int *h_flags = g->pinned.as<int>();
     double total_ms = 0;
     for (int32_t i = 0; i < num_sources; i++) {
         a.src = src[i];
-        a.dist = dev_dist ? dist_out + (size_t)i * n : g->ws_out0.as<int32_t>();
+        int32_t *stage[2] = {nullptr, nullptr};
+        if (host_dist || host_parent) HC_TRY(pipe.acquire(i, stage));
+        a.dist = dev_dist ? dist_out + (size_t)i * n : host_dist ? stage[0] : g->ws_out0.as<int32_t>();
         HC_CUDA_TRY(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), g->stream));
         HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
         HC_TRY(o.collect_stats ? run_source<true>(g, a, h_flags) : run_source<false>(g, a, h_flags));
         HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
         if (parent_out) {
-            int32_t *par = dev_parent ? parent_out + (size_t)i * n : g->ws_out1.as<int32_t>();
+            int32_t *par = dev_parent ? parent_out + (size_t)i * n : stage[1];
             { sssp_parent_init<<<g->sm_count * 4, 256, 0, g->stream>>>(par, g->N, a.src); ::hc::count_launch(); }
             { sssp_parents_fill<<<g->sm_count * 8, 256, 0, g->stream>>>(a.index, a.nbr, a.w, a.dist, g->N, a.src, par); ::hc::count_launch(); }
             HC_CUDA_TRY(cudaGetLastError());
-            if (!dev_parent) HC_TRY(copy_out(parent_out + (size_t)i * n, par, 4 * n, g->stream));
         }
-        if (dist_out && !dev_dist) HC_TRY(copy_out(dist_out + (size_t)i * n, a.dist, 4 * n, g->stream));
+        if (host_dist || host_parent) {
+            void *dst[2] = {host_dist ? (void *)(dist_out + (size_t)i * n) : nullptr,
+                            host_parent ? (void *)(parent_out + (size_t)i * n) : nullptr};
+            HC_TRY(pipe.release(i, dst));
+        }
         SsspCtl c;
         HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
         if (o.collect_stats && stats) {
@@ -710,6 +718,7 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
             }
         }
     }
+    if (host_dist || host_parent) HC_TRY(pipe.finish());
     if (stats) {
         stats->ms = total_ms;
         // 16 B offsets per processed vertex, 8 B (neighbour + weight) per
