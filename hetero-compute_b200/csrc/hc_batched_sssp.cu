@@ -276,17 +276,25 @@ __global__ void __launch_bounds__(256) mssp_tasks(const int64_t *index, const in
 }
 
 // Pull epoch, used while the queue covers a large part of the graph (weights
-// symmetric, so w(u->v) is read from v's row).  Items [0, n_rows) are rows of
-// at most kLongRow edges, one warp each, the only writer of that row; items
-// past n_rows are kLongRow-edge chunks of the longer rows, which merge with
-// atomicMin.  A warp takes the minimum over the neighbours whose activity
-// mask has its lane's bit, four neighbours in flight, and writes the row and
-// its activity mask once.
+// symmetric, so w(u->v) is read from v's row).  Items [row_begin, row_end)
+// are rows of at most kLongRow edges, one warp each, the only writer of that
+// row; the items after them are kLongRow-edge chunks of the longer rows, which
+// merge with atomicMin.  A warp takes the minimum over the neighbours whose
+// activity mask has its lane's bit, four neighbours in flight, and writes the
+// row and its activity mask once.
+//
+// An epoch runs in two launches on degree-sorted graphs: the hub prefix (the
+// rows holding half the edges, and the long-row chunks) first, then the other
+// rows, which count a neighbour as active when it changed in the previous
+// epoch or in this one (`fresh`): most shortest paths pass through hubs, so an
+// improvement travels two hops per epoch.  Any order of pulls is valid, since
+// distances only fall and a lowered row is active for the next epoch.
 template <int SPL>
 __global__ void __launch_bounds__(256) mssp_pull(const int64_t *index, const int32_t *nbr, const int32_t *w,
-                                                 int32_t *dist, int32_t n_rows, const int2 *tasks, int ntasks,
-                                                 const uint32_t *act_cur, uint32_t *act_next, const MsspCtl *ctl,
-                                                 int c, unsigned long long *relaxed) {
+                                                 int32_t *dist, int32_t row_begin, int32_t row_end,
+                                                 const int2 *tasks, int ntasks, const uint32_t *act_cur,
+                                                 uint32_t *act_next, int fresh, const MsspCtl *ctl, int c,
+                                                 unsigned long long *relaxed) {
     const int nq = ctl_queue(ctl, c);
     if (nq == 0 || !ctl_pull(ctl, c)) return;
     constexpr int K = 32 * SPL;
@@ -294,13 +302,14 @@ __global__ void __launch_bounds__(256) mssp_pull(const int64_t *index, const int
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     unsigned long long rel = 0;
+    const int32_t n_rows = row_end - row_begin;
     const int64_t total = (int64_t)n_rows + ntasks;
     for (int64_t it = gwarp; it < total; it += nwarps) {
         int32_t v;
         int64_t b, e;
         bool chunk;
         if (it < n_rows) {
-            v = (int32_t)it;
+            v = row_begin + (int32_t)it;
             b = index[v];
             e = index[v + 1];
             if (e == b || e - b > kLongRow) continue;
@@ -326,6 +335,7 @@ __global__ void __launch_bounds__(256) mssp_pull(const int64_t *index, const int
                 uu = nbr[my];
                 ww = w[my];
                 aa = __ldcg(act_cur + uu);
+                if (fresh) aa |= __ldcg(act_next + uu);  // changed earlier in this epoch
             }
             rel += (unsigned long long)__popc(aa) * SPL;
             unsigned live = __ballot_sync(kFull, aa != 0u);
@@ -432,6 +442,19 @@ hc_status ensure_pull_plan(hc_graph *g) {
     HC_CUDA_TRY(cudaMemcpyAsync(&h, cnt, 4, cudaMemcpyDeviceToHost, g->stream));
     HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
     g->mssp_tasks = h;
+    // Hub prefix of a degree-sorted graph: the fewest rows holding half the
+    // edges (binary search over the offsets, a few 8-byte reads).
+    g->mssp_hub_rows = g->n_active;
+    if (g->degree_sorted && g->n_active > 0) {
+        int32_t lo = 0, hi = g->n_active;
+        while (lo < hi) {
+            const int32_t mid = lo + (hi - lo) / 2;
+            int64_t off = 0;
+            HC_CUDA_TRY(cudaMemcpy(&off, g->index.as<int64_t>() + mid, sizeof(off), cudaMemcpyDeviceToHost));
+            if (off >= g->M / 2) hi = mid; else lo = mid + 1;
+        }
+        g->mssp_hub_rows = std::max<int32_t>(lo, 1);
+    }
     return HC_OK;
 }
 
@@ -512,14 +535,18 @@ void launch_epoch(const hc_graph *g, cudaStream_t st, const MsspBufs &b, int c, 
                                           b.ctl, c, relaxed);
     mssp_tasks<SPL><<<grid, 256, 0, st>>>(index, nbr, w, b.dist, b.tasks, b.act[c], b.act[c ^ 1], b.q[c ^ 1], b.ctl, c,
                                           relaxed);
-    mssp_pull<SPL><<<grid, 256, 0, st>>>(index, nbr, w, b.dist, g->n_active, g->ws_plan_mssp.as<int2>(),
-                                         g->mssp_tasks < 0 ? 0 : g->mssp_tasks, b.act[c], b.act[c ^ 1], b.ctl, c,
+    const int32_t hub = g->mssp_hub_rows > 0 ? g->mssp_hub_rows : g->n_active;
+    mssp_pull<SPL><<<grid, 256, 0, st>>>(index, nbr, w, b.dist, 0, hub, g->ws_plan_mssp.as<int2>(),
+                                         g->mssp_tasks < 0 ? 0 : g->mssp_tasks, b.act[c], b.act[c ^ 1], 0, b.ctl, c,
                                          relaxed);
+    if (hub < g->n_active)
+        mssp_pull<SPL><<<grid, 256, 0, st>>>(index, nbr, w, b.dist, hub, g->n_active, nullptr, 0, b.act[c],
+                                             b.act[c ^ 1], 1, b.ctl, c, relaxed);
     mssp_clear<<<grid, 256, 0, st>>>(b.q[c], b.act[c], b.ctl, c);
     mssp_compact<<<grid, 256, 0, st>>>(index, b.act[c ^ 1], g->N, b.q[c ^ 1], b.ctl, c);
     mssp_end<<<1, 32, 0, st>>>(b.ctl, c, cond, use_cond);
 }
-constexpr int kEpochLaunches = 6;
+constexpr int kEpochLaunches = 7;
 
 template <int SPL>
 hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int max_epochs, int pull_alpha,

@@ -81,6 +81,7 @@ struct hc_graph {
     // batched-SSSP pull plan: (row, chunk) tasks of the rows above its chunk size
     hc::DevBuf ws_plan_mssp;
     int32_t mssp_tasks = -1;
+    int32_t mssp_hub_rows = -1;  // degree-sorted: the row prefix holding half the edges
 
     // autotuned launch parameters (zero fields: built-in defaults)
     hc_tuning tune{};
