@@ -153,10 +153,15 @@ __device__ __forceinline__ uint32_t ld_cg(const uint32_t *p) { return __ldcg(p);
 // True when `p` is device (or managed) memory of the current context.
 bool is_device_pointer(const void *p);
 
-// Device buffer that grows on demand and is freed with its owner.
+// Device buffer that grows on demand and is freed with its owner (or when it
+// goes out of scope; not copyable).
 struct DevBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
     hc_status ensure(size_t want);
     void release();
     template <class T>

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "hc_common.h"
+#include "hc_gen.h"
 
 namespace hc {
 
@@ -43,88 +44,6 @@ hc_status fail(hc_status s, const char *fmt, ...) {
 void clear_error() { g_last_error.clear(); }
 
 namespace {
-
-enum Stream : uint64_t { kRmat = 1, kWeight = 2, kPerm = 3, kUniform = 4 };
-
-// Bijection on [0, 2^bits): rounds of odd multiply + add and xorshift, all
-// invertible modulo 2^bits.  Stands in for the shuffle of
-// src/gapbs/generator.h:53-63 (which needs a serial mt19937 walk).
-struct Permutation {
-    uint32_t mask;
-    int shift;
-    uint32_t mul[4], add[4];
-    Permutation(int bits, uint64_t seed) {
-        mask = bits >= 32 ? 0xffffffffu : ((1u << bits) - 1u);
-        shift = bits / 2 + 1;
-        for (int r = 0; r < 4; r++) {
-            uint64_t k = draw(seed, kPerm, r);
-            mul[r] = (uint32_t)k | 1u;
-            add[r] = (uint32_t)(k >> 32);
-        }
-    }
-    uint32_t operator()(uint32_t x) const {
-        for (int r = 0; r < 4; r++) {
-            x = (x * mul[r] + add[r]) & mask;
-            x ^= x >> shift;
-        }
-        return x & mask;
-    }
-};
-
-// Endpoint pair e of an R-MAT edge list (src/gapbs/generator.h:82-115).
-struct RmatPairs {
-    int scale;
-    uint64_t seed;
-    Permutation perm;
-    RmatPairs(int s, uint64_t sd) : scale(s), seed(sd), perm(s, sd) {}
-    void operator()(int64_t e, uint32_t &src, uint32_t &dst) const {
-        const float A = 0.57f, B = 0.19f, C = 0.19f;
-        const float inv24 = 1.0f / 16777216.0f;
-        uint32_t s = 0, d = 0;
-        const int words = (scale + 1) / 2;
-        for (int k = 0; k < words; k++) {
-            uint64_t h = draw(seed, kRmat, (uint64_t)e * (uint64_t)words + k);
-            for (int half = 0; half < 2; half++) {
-                if (2 * k + half >= scale) break;
-                float r = (float)((half ? (h >> 8) : (h >> 40)) & 0xffffffu) * inv24;
-                s <<= 1;
-                d <<= 1;
-                if (r < A + B) {
-                    if (r > A) d++;
-                } else {
-                    s++;
-                    if (r > A + B + C) d++;
-                }
-            }
-        }
-        src = perm(s);
-        dst = perm(d);
-    }
-};
-
-// Uniform endpoints (src/gapbs/generator.h:65-80).
-struct UniformPairs {
-    int scale;
-    uint64_t seed;
-    void operator()(int64_t e, uint32_t &src, uint32_t &dst) const {
-        uint64_t h = draw(seed, kUniform, (uint64_t)e);
-        uint32_t mask = (uint32_t)((1ull << scale) - 1);
-        src = (uint32_t)h & mask;
-        dst = (uint32_t)(h >> 32) & mask;
-    }
-};
-
-inline uint32_t weight_bits(hc_wtype wt, uint64_t seed, int64_t e) {
-    uint64_t h = draw(seed, kWeight, (uint64_t)e);
-    if (wt == HC_W_I32) return (uint32_t)(1 + (h % 255));  // uniform [1,255]
-    if (wt == HC_W_F32) {
-        float f = (float)((h >> 40) + 1) * (1.0f / 16777216.0f);  // uniform (0,1]
-        uint32_t b;
-        std::memcpy(&b, &f, 4);
-        return b;  // positive floats order like their bit patterns
-    }
-    return 0;
-}
 
 hc_status alloc_csr(hc_csr *out, int32_t n, int64_t m, hc_wtype wt) {
     std::memset(out, 0, sizeof(*out));
@@ -477,30 +396,9 @@ hc_status hc_pick_sources(const int64_t *index, const int32_t *neighbors, int32_
     clear_error();
     if (!index || !out || num_nodes < 1 || count < 0)
         return fail(HC_ERR_INVALID_ARG, "hc_pick_sources: bad arguments");
-    if (const_source >= 0) {
-        for (int32_t i = 0; i < count; i++) out[i] = const_source;
-        return HC_OK;
-    }
-    bool any = false;
-    for (int32_t v = 0; v < num_nodes && !any; v++) {
-        int64_t d = index[v + 1] - index[v];
-        any = d > 1 || (d == 1 && neighbors && neighbors[index[v]] != v);
-    }
-    if (!any) return fail(HC_ERR_INVALID_ARG, "hc_pick_sources: graph has no eligible source");
-    std::mt19937 rng(37525);
-    std::uniform_int_distribution<int32_t> udist(0, num_nodes - 1);
-    for (int32_t i = 0; i < count; i++) {
-        int32_t s;
-        for (;;) {
-            s = udist(rng);
-            int64_t d = index[s + 1] - index[s];
-            if (d == 0) continue;
-            if (d == 1 && neighbors && neighbors[index[s]] == s) continue;
-            break;
-        }
-        out[i] = s;
-    }
-    return HC_OK;
+    // A degree-1 vertex whose only edge is a self-loop is no source.
+    auto self_only = [&](int32_t v) { return neighbors && neighbors[index[v]] == v; };
+    return pick_sources_impl(index, num_nodes, count, const_source, out, self_only);
 }
 
 }  // extern "C"

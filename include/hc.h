@@ -123,6 +123,21 @@ hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors,
                           const void *weights, hc_wtype wtype, int32_t num_nodes,
                           int64_t num_edges, int32_t device, hc_graph **out);
 hc_status hc_graph_destroy(hc_graph *g);
+
+/* Synthetic graphs built on the device: the same CSR as hc_gen_kronecker /
+ * hc_gen_uniform (same scale, edge factor or pairs per vertex, seed and
+ * weights) followed by hc_graph_create, without host memory or an upload.
+ * Replaces the host-side build of the reference's gapbs adapters
+ * (src/gapbs/generator.h:53-165, src/gapbs/builder.h:80-406). */
+typedef enum hc_gen_kind { HC_GEN_KRONECKER = 0, HC_GEN_UNIFORM = 1 } hc_gen_kind;
+hc_status hc_graph_generate(hc_gen_kind kind, int32_t scale, int32_t edge_factor, uint64_t seed,
+                            hc_wtype wtype, int32_t device, hc_graph **out);
+/* Copies the handle's CSR into caller buffers (host or device; any may be
+ * NULL): index [N+1], neighbors [M], weights [M] (4-byte values). */
+hc_status hc_graph_get_csr(hc_graph *g, int64_t *index, int32_t *neighbors, void *weights);
+/* hc_pick_sources on a handle's graph (reads its offsets, and the neighbour of
+ * each degree-1 candidate, from the device). */
+hc_status hc_graph_pick_sources(hc_graph *g, int32_t count, int32_t *out);
 /* Work of this handle goes to `stream` (a cudaStream_t); NULL restores the
  * handle's own stream. */
 hc_status hc_graph_set_stream(hc_graph *g, void *stream);
