@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "libhc.so")
 
 OK, INVALID_ARG, OOM, CUDA, NOT_CONVERGED, TIMEOUT, NO_DEVICE, UNSUPPORTED, IO = range(9)
 W_NONE, W_I32, W_F32 = 0, 1, 2
+GEN_KRONECKER, GEN_UNIFORM = 0, 1  # hc_graph_generate
 VARIANT_AUTO, VARIANT_THREAD, VARIANT_WARP, VARIANT_BLOCK = 0, 1, 2, 3
 INF_DIST = 0x7FFFFFFF
 
@@ -118,6 +119,9 @@ _SIGS = {
     "hc_graph_destroy": (C.c_int, [_P]),
     "hc_graph_set_stream": (C.c_int, [_P, _P]),
     "hc_graph_get_info": (C.c_int, [_P, C.POINTER(GraphInfo)]),
+    "hc_graph_generate": (C.c_int, [C.c_int, C.c_int32, C.c_int32, C.c_uint64, C.c_int, C.c_int32, C.POINTER(_P)]),
+    "hc_graph_get_csr": (C.c_int, [_P, _P, _P, _P]),
+    "hc_graph_pick_sources": (C.c_int, [_P, C.c_int32, _P]),
     "hc_bfs": (C.c_int, [_P, _P, C.c_int32, _P, _P, C.POINTER(BfsOpts), C.POINTER(BfsStats)]),
     "hc_sssp": (C.c_int, [_P, _P, C.c_int32, _P, _P, C.POINTER(SsspOpts), C.POINTER(SsspStats)]),
     "hc_pr_forward": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(PrOpts), C.POINTER(PrStats)]),
@@ -292,6 +296,34 @@ class Graph:
     @classmethod
     def from_host(cls, g: HostCSR, device: int = 0) -> "Graph":
         return cls(g.index, g.neighbors, g.weights, device)
+
+    @classmethod
+    def generate(cls, kind: int, scale: int, edge_factor: int, seed: int = 1, wtype: int = W_NONE,
+                 device: int = 0) -> "Graph":
+        """hc_graph_generate: the gen_kronecker / gen_uniform graph, built on the device."""
+        h = C.c_void_p()
+        _check(lib().hc_graph_generate(kind, scale, edge_factor, seed, wtype, device, C.byref(h)),
+               "hc_graph_generate")
+        self = cls.__new__(cls)
+        self._h = h
+        info = self.info()
+        self.num_nodes, self.num_edges, self.wtype = info.num_nodes, info.num_edges, info.wtype
+        return self
+
+    def csr(self):
+        """(index int64[N+1], neighbors int32[M], weights or None) copied to host memory."""
+        index = np.empty(self.num_nodes + 1, dtype=np.int64)
+        nbr = np.empty(self.num_edges, dtype=np.int32)
+        w = None
+        if self.wtype != W_NONE:
+            w = np.empty(self.num_edges, dtype=np.int32 if self.wtype == W_I32 else np.float32)
+        _check(lib().hc_graph_get_csr(self._h, _ptr(index), _ptr(nbr), _ptr(w)), "hc_graph_get_csr")
+        return index, nbr, w
+
+    def pick_sources(self, count: int) -> np.ndarray:
+        out = np.empty(count, dtype=np.int32)
+        _check(lib().hc_graph_pick_sources(self._h, count, _ptr(out)), "hc_graph_pick_sources")
+        return out
 
     @property
     def handle(self):
