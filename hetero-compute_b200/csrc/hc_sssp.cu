@@ -42,6 +42,7 @@ struct SsspCtl {
     // kernel saves its loop state here and exits with need_pull set, and the
     // next launch (resume set) folds the lowered rows into its queues.
     int need_pull, resume;
+    int finished;  // the run is over: later launches of the chain return at once
     int saved_E, saved_phase, saved_pulls, saved_T;
     unsigned long long t_start;
     int qlen[3];
@@ -256,6 +257,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
     int E = 0, phase = 0, pulls = 0;
     unsigned long long my_v = 0, my_e = 0;
     // Every block reads the same control words (written before this launch).
+    if (__ldcg(&ctl->finished) || __ldcg(&ctl->gs.err)) return;  // a speculative launch past the end
     const bool resumed = __ldcg(&ctl->resume) != 0;
     unsigned long long t_start;
     if (!resumed) {
@@ -439,6 +441,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
         if (threadIdx.x == 0 && e) atomicAdd(&ctl->erelax, e);
     }
     if (gtid == 0 && !__ldcg(&ctl->need_pull)) {
+        ctl->finished = 1;
         ctl->epochs = E;
         ctl->phases = phase;
         ctl->pulls = pulls;
@@ -453,6 +456,8 @@ template <bool kStats>
 __global__ void __launch_bounds__(kPullThreads) sssp_pull_kernel(SsspArgs a) {
     __shared__ int32_t s_acc[kPullThreads / 32][32];
     __shared__ unsigned long long s_red[32];
+    // A speculative launch with no pull epoch pending returns at once.
+    if (!__ldcg(&a.ctl->need_pull) || __ldcg(&a.ctl->gs.err)) return;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long my_e = 0;
     pull_sweep<kStats>(a, gtid >> 5, (gridDim.x * blockDim.x) >> 5, s_acc, my_e);
@@ -543,20 +548,29 @@ hc_status launch_pull(hc_graph *g, const SsspArgs &a) {
 }
 
 // One source: the persistent kernel, and for each pull epoch it hands back,
-// the pull kernel and another persistent launch that resumes the loop.
+// the pull kernel and another persistent launch that resumes the loop.  The
+// chain is queued kSpeculate (pull, resume) pairs at a time without waiting
+// for the host: a pull launch with no epoch pending and a persistent launch
+// after the end return at once.  The host checks once per batch.
+constexpr int kSpeculate = 3;
+
 template <bool kStats>
 hc_status run_source(hc_graph *g, const SsspArgs &a, volatile int *h_flags) {
+    HC_TRY(launch_sssp<kStats>(g, a));
+    if (a.pull_alpha <= 0) return HC_OK;  // no pull epochs: one launch
     for (int round = 0;; round++) {
-        HC_TRY(launch_sssp<kStats>(g, a));
-        if (a.pull_alpha <= 0) return HC_OK;  // no pull epochs: one launch
-        // gs.err and need_pull, adjacent at the head of SsspCtl.
-        HC_CUDA_TRY(cudaMemcpyAsync((void *)h_flags, a.ctl, offsetof(SsspCtl, resume), cudaMemcpyDeviceToHost,
-                                    g->stream));
+        for (int k = 0; k < kSpeculate; k++) {
+            HC_TRY(launch_pull<kStats>(g, a));
+            HC_TRY(launch_sssp<kStats>(g, a));
+        }
+        // gs.err, need_pull, resume and finished, at the head of SsspCtl.
+        HC_CUDA_TRY(cudaMemcpyAsync((void *)h_flags, a.ctl, offsetof(SsspCtl, finished) + sizeof(int),
+                                    cudaMemcpyDeviceToHost, g->stream));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
         const SsspCtl *hc = (const SsspCtl *)h_flags;
-        if (hc->gs.err || !hc->need_pull) return HC_OK;
-        if (round > a.max_epochs) return fail(HC_ERR_NOT_CONVERGED, "hc_sssp: pull rounds exceed the epoch cap");
-        HC_TRY(launch_pull<kStats>(g, a));
+        if (hc->gs.err || hc->finished) return HC_OK;
+        if ((int64_t)round * kSpeculate > a.max_epochs)
+            return fail(HC_ERR_NOT_CONVERGED, "hc_sssp: pull rounds exceed the epoch cap");
     }
 }
 
