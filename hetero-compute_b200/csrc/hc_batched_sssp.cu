@@ -335,7 +335,8 @@ __global__ void __launch_bounds__(256) mssp_pull(const int64_t *index, const int
                 uu = nbr[my];
                 ww = w[my];
                 aa = __ldcg(act_cur + uu);
-                if (fresh) aa |= __ldcg(act_next + uu);  // changed earlier in this epoch
+                // A hub row (below row_begin) may have changed earlier in this epoch.
+                if (fresh && uu < row_begin) aa |= __ldcg(act_next + uu);
             }
             rel += (unsigned long long)__popc(aa) * SPL;
             unsigned live = __ballot_sync(kFull, aa != 0u);

@@ -285,3 +285,35 @@ def test_pagerank_hub_rows_chunked():
     s, st = g.pagerank(tol_l1=1e-7, max_iters=200)
     x, _ = oracle.pr_jacobi_f64(host.index, host.neighbors, tol=1e-12)
     assert np.abs(s - x).max() < 1e-6
+
+
+def test_host_outputs_pinned_and_mixed():
+    """Per-source results bound for host memory are staged and copied while the next source runs:
+    pinned and pageable host outputs, and host/device mixes, give the device outputs' depths and distances
+    and valid parent trees."""
+    torch = pytest.importorskip("torch")
+    host = hc.gen_kronecker(13, 16, 9, wtype=hc.W_I32)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, 7)
+    n = host.num_nodes
+    dd = torch.empty((7, n), dtype=torch.int32, device="cuda")
+    g.bfs(src, dd, torch.empty((7, n), dtype=torch.int32, device="cuda"))
+    pinned_d = torch.empty((7, n), dtype=torch.int32).pin_memory().numpy()
+    pinned_p = torch.empty((7, n), dtype=torch.int32).pin_memory().numpy()
+    g.bfs(src, pinned_d, pinned_p)
+    assert np.array_equal(pinned_d, dd.cpu().numpy())
+    mixed_p = np.empty((7, n), dtype=np.int32)
+    dd2 = torch.empty((7, n), dtype=torch.int32, device="cuda")
+    g.bfs(src, dd2, mixed_p)
+    assert np.array_equal(dd2.cpu().numpy(), dd.cpu().numpy())
+    for i, s in enumerate(src):  # parents may differ between runs (any neighbour one level up is valid)
+        for par in (pinned_p[i], mixed_p[i]):
+            assert oracle.verify_bfs_parents(host.index, host.neighbors, pinned_d[i], par, s)[0] == 0
+    sd = torch.empty((7, n), dtype=torch.int32, device="cuda")
+    g.sssp(src, sd)
+    pinned_s = torch.empty((7, n), dtype=torch.int32).pin_memory().numpy()
+    pinned_sp = torch.empty((7, n), dtype=torch.int32).pin_memory().numpy()
+    dist, parent, _ = g.sssp(src, pinned_s, pinned_sp, want_parent=True)
+    assert np.array_equal(pinned_s, sd.cpu().numpy())
+    for i, s in enumerate(src):
+        assert oracle.verify_sp_tree(host.index, host.neighbors, host.weights, pinned_s[i], pinned_sp[i], s) == 0
