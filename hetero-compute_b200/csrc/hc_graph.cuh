@@ -12,6 +12,8 @@ namespace hc {
 constexpr int kStreamEdges = 2048;
 constexpr int kHubEdges = 4096;
 constexpr int kHubChunk = 2048;
+// Batched SSSP keeps 16-bit distances when no weight exceeds this.
+constexpr int32_t kMsspNarrowMaxW = 0x0FFF;
 
 struct HubInfo {
     int32_t row;
@@ -72,6 +74,7 @@ struct hc_graph {
     // weight statistics, computed once
     int wstats_done = 0;
     int w_negative = 0;
+    int32_t w_max = 0;         // largest weight (0 when none is positive)
     double w_mean = 0.0;
     int w_symmetric = 0;       // w(u->v) == w(v->u) for every edge (rows sorted)
 
@@ -139,6 +142,6 @@ hc_status edge_symmetry(hc_graph *g, const uint32_t *wbits, bool *structure, boo
 const float *pr_weights(const hc_graph *g);
 // Builds the row plan if missing (g->pr_view, g->pr_partial_slots).
 hc_status ensure_plan(hc_graph *g);
-// Computes w_negative, w_mean and w_symmetric once (int32 weights).
+// Computes w_negative, w_max, w_mean and w_symmetric once (int32 weights).
 hc_status ensure_weight_stats(hc_graph *g);
 }  // namespace hc

@@ -499,20 +499,25 @@ __global__ void count_finite(const int32_t *dist, int32_t n, unsigned long long 
     if (threadIdx.x == 0 && c) atomicAdd(out, c);
 }
 
-// Whether any weight is negative, and the weights' sum.
-__global__ void weight_stats(const int64_t *index, const int32_t *w, int32_t n, int *neg, unsigned long long *sum) {
+// Whether any weight is negative (flags[0]), the largest weight (flags[1])
+// and the weights' sum.
+__global__ void weight_stats(const int64_t *index, const int32_t *w, int32_t n, int *flags, unsigned long long *sum) {
     __shared__ unsigned long long s_red[32];
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     unsigned long long s = 0;
+    int32_t mx = 0;
     for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
         const int64_t b = index[v], e = index[v + 1];
         for (int64_t i = b + lane; i < e; i += 32) {
             const int32_t x = w[i];
-            if (x < 0) *neg = 1;
+            if (x < 0) flags[0] = 1;
             s += (unsigned long long)max(x, 0);
+            mx = max(mx, x);
         }
     }
+    mx = __reduce_max_sync(kFull, mx);
+    if (lane == 0 && mx > 0) atomicMax(flags + 1, mx);
     s = block_sum(s, s_red);
     if (threadIdx.x == 0 && s) atomicAdd(sum, s);
 }
@@ -595,6 +600,7 @@ hc_status ensure_weight_stats(hc_graph *g) {
     HC_CUDA_TRY(cudaMemcpyAsync(&hsum, sum, 8, cudaMemcpyDeviceToHost, g->stream));
     HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
     g->w_negative = hf[0];
+    g->w_max = hf[1];
     // Symmetric weights (w(u->v) == w(v->u) for every edge): one hashing pass.
     bool st = false, ws = false;
     HC_TRY(edge_symmetry(g, reinterpret_cast<const uint32_t *>(g->wgt.ptr), &st, &ws));

@@ -159,8 +159,9 @@ hc_status tune_sssp_batched(Tuner &tu, hc_tuning &out) {
     HC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     free_b += g->ws_batch.bytes + g->ws_out0.bytes;
     std::vector<int32_t> groups;
+    const double bytes = g->w_max <= kMsspNarrowMaxW ? 2.0 : 4.0;  // 16- or 32-bit distances
     for (int32_t w : {64, 128, 256, 512})
-        if ((double)g->N * w * 4.0 <= 0.4 * (double)free_b) groups.push_back(w);
+        if ((double)g->N * w * bytes <= 0.4 * (double)free_b) groups.push_back(w);
     if (groups.empty()) groups.push_back(32);
     hc_batch_opts o{};
     o.group = out.mssp_group > 0 ? out.mssp_group : groups.back();

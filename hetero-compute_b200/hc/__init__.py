@@ -82,7 +82,7 @@ GRAPH_AUTO, GRAPH_ON, GRAPH_OFF = 0, 1, 2  # hc_batch_opts.use_graph
 
 class BatchOpts(C.Structure):
     _fields_ = [("group", C.c_int32), ("max_epochs", C.c_int32), ("use_graph", C.c_int32),
-                ("switch_alpha", C.c_int32)]
+                ("switch_alpha", C.c_int32), ("dist_bits", C.c_int32)]
 
 
 class Tuning(C.Structure):
@@ -100,7 +100,8 @@ TUNE_BFS, TUNE_SSSP, TUNE_BFS_BATCHED, TUNE_SSSP_BATCHED, TUNE_ALL = 1, 2, 4, 8,
 
 
 class BatchStats(C.Structure):
-    _fields_ = [("epochs", C.c_int32), ("groups", C.c_int32), ("bytes_model", C.c_double), ("ms", C.c_double)]
+    _fields_ = [("epochs", C.c_int32), ("groups", C.c_int32), ("bytes_model", C.c_double), ("ms", C.c_double),
+                ("wide_groups", C.c_int32), ("reruns", C.c_int32)]
 
 
 _P = C.c_void_p
@@ -421,11 +422,13 @@ class Graph:
                "hc_bfs_batched")
         return depth, st
 
-    def sssp_batched(self, sources, dist=None, *, group=0, max_epochs=0, use_graph=GRAPH_AUTO, switch_alpha=0):
+    def sssp_batched(self, sources, dist=None, *, group=0, max_epochs=0, use_graph=GRAPH_AUTO, switch_alpha=0,
+                     dist_bits=0):
+        """dist_bits: working distances, 0/16 = 16-bit where they fit (else 32-bit), 32 = always 32-bit."""
         src = np.ascontiguousarray(sources, dtype=np.int32)
         if dist is None:
             dist = np.empty((len(src), self.num_nodes), dtype=np.int32)
-        o = BatchOpts(group, max_epochs, use_graph, switch_alpha)
+        o = BatchOpts(group, max_epochs, use_graph, switch_alpha, dist_bits)
         st = BatchStats()
         _check(lib().hc_sssp_batched(self._h, _ptr(src), len(src), _ptr(dist), C.byref(o), C.byref(st)),
                "hc_sssp_batched")

@@ -292,6 +292,10 @@ typedef struct hc_batch_opts {
                              BFS pushes while frontier edges * alpha < M (default 10),
                              else pulls; < 0 pulls every level.  SSSP pulls when the
                              queue's edges * alpha > M (default 2); < 0 pushes only. */
+    int32_t dist_bits;    /* batched SSSP working distances: 0 = 16-bit when every weight
+                             is at most 4095 (a group whose distances do not fit runs
+                             again 32-bit), 16 = the same, 32 = always 32-bit.  The
+                             output is int32 either way. */
 } hc_batch_opts;
 
 typedef struct hc_batch_stats {
@@ -299,6 +303,8 @@ typedef struct hc_batch_stats {
     int32_t groups;
     double bytes_model;
     double ms;
+    int32_t wide_groups;  /* batched SSSP: groups run with 32-bit distances */
+    int32_t reruns;       /* batched SSSP: 16-bit groups run again 32-bit */
 } hc_batch_stats;
 
 /* Multi-source BFS: bit-sliced frontiers, all sources of a group advance in

@@ -66,44 +66,50 @@ def test_sssp_batched_distances(scale, k):
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s)), i
 
 
+@pytest.mark.parametrize("dist_bits", [0, 32])
 @pytest.mark.parametrize("group", [32, 64, 128, 256, 512])
-def test_sssp_batched_group_widths(group):
+def test_sssp_batched_group_widths(group, dist_bits):
     host = hc.gen_kronecker(11, 16, 42, wtype=hc.W_I32)
     g = hc.Graph.from_host(host)
     src = np.concatenate([hc.pick_sources(host, 150), hc.pick_sources(host, 3)])  # ragged last group, duplicates
-    dist, st = g.sssp_batched(src, group=group)
+    dist, st = g.sssp_batched(src, group=group, dist_bits=dist_bits)
+    assert st.wide_groups == (st.groups if dist_bits == 32 or group == 32 else 0)
     assert st.groups == -(-len(src) // group)
     for i, s in enumerate(src):
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s)), i
     torch = pytest.importorskip("torch")
     dd = torch.empty((len(src), host.num_nodes), dtype=torch.int32, device="cuda")
-    g.sssp_batched(src, dd, group=group)
+    g.sssp_batched(src, dd, group=group, dist_bits=dist_bits)
     assert np.array_equal(dd.cpu().numpy(), dist)
 
 
+@pytest.mark.parametrize("dist_bits", [0, 32])
 @pytest.mark.parametrize("switch_alpha", [-1, 0, 1000000])
-def test_sssp_batched_push_and_pull_epochs(switch_alpha):
-    """Push only, the default switch, and pull for every epoch."""
+def test_sssp_batched_push_and_pull_epochs(switch_alpha, dist_bits):
+    """Push only, the default switch, and pull for every epoch; 16- and 32-bit distances."""
     big = hc.gen_kronecker(16, 16, 3, wtype=hc.W_I32)  # rows above the chunk size
     g = hc.Graph.from_host(big)
     src = hc.pick_sources(big, 70)
-    dist, _ = g.sssp_batched(src, group=64, switch_alpha=switch_alpha)
+    dist, _ = g.sssp_batched(src, group=64, switch_alpha=switch_alpha, dist_bits=dist_bits)
     for i in range(0, 70, 9):
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(big.index, big.neighbors, big.weights, src[i])), i
 
 
+@pytest.mark.parametrize("group", [32, 64])
 @pytest.mark.parametrize("use_graph", [hc.GRAPH_ON, hc.GRAPH_OFF])
-def test_sssp_batched_graph_and_host_loop(use_graph):
-    """The epoch loop as a CUDA graph (while node) and as a host loop give the same distances."""
+def test_sssp_batched_graph_and_host_loop(use_graph, group):
+    """The epoch loop as a CUDA graph (while node) and as a host loop give the same distances
+    (32-bit distances at 32 sources per group, 16-bit at 64)."""
     host = hc.gen_grid(50, 40, 4, wtype=hc.W_I32)  # ~100 epochs
     g = hc.Graph.from_host(host)
     src = np.array([0, 1999, 1000, 7, 7, 1234], dtype=np.int32)
-    dist, st = g.sssp_batched(src, group=32, use_graph=use_graph)
+    dist, st = g.sssp_batched(src, group=group, use_graph=use_graph)
     assert st.epochs > 40
+    assert st.wide_groups == (1 if group == 32 else 0)
     for i, s in enumerate(src):
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, s)), i
     before = hc.kernel_launches()
-    g.sssp_batched(src, group=32, use_graph=use_graph)
+    g.sssp_batched(src, group=group, use_graph=use_graph)
     assert hc.kernel_launches() - before >= 6 * st.epochs  # launches inside the graph are counted too
 
 
@@ -116,6 +122,87 @@ def test_sssp_batched_epoch_cap(use_graph):
     assert e.value.status == hc.NOT_CONVERGED
     dist, st = g.sssp_batched(np.array([0], dtype=np.int32), use_graph=use_graph)  # handle still usable
     assert np.array_equal(dist[0], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, 0))
+
+
+def _line(n, w):
+    """Path 0 - 1 - ... - n-1, every edge of weight w both ways."""
+    deg = np.full(n, 2, dtype=np.int64)
+    deg[0] = deg[-1] = 1
+    index = np.concatenate([[0], np.cumsum(deg)]).astype(np.int64)
+    nbr = np.concatenate([[v for v in (u - 1, u + 1) if 0 <= v < n] for u in range(n)]).astype(np.int32)
+    return index, nbr, np.full(len(nbr), w, dtype=np.int32)
+
+
+def test_sssp_batched_16_and_32_bit_agree():
+    """Kronecker, weights [1,255]: 16-bit working distances by default, 32-bit on request, same result."""
+    host = hc.gen_kronecker(12, 16, 43, wtype=hc.W_I32)
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, 130)
+    d16, st16 = g.sssp_batched(src)
+    assert (st16.wide_groups, st16.reruns) == (0, 0)
+    d32, st32 = g.sssp_batched(src, dist_bits=32)
+    assert st32.wide_groups == st32.groups and st32.reruns == 0
+    assert np.array_equal(d16, d32)
+    for i in range(0, len(src), 11):
+        assert np.array_equal(d16[i], oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, src[i])), i
+
+
+@pytest.mark.parametrize("use_graph", [hc.GRAPH_ON, hc.GRAPH_OFF])
+@pytest.mark.parametrize("n,reruns", [(15, 0), (16, 1), (17, 1), (40, 1)])
+def test_sssp_batched_16bit_range(n, reruns, use_graph):
+    """Line of weight 4095 (the largest 16-bit weight): the farthest vertex sits at (n-1)*4095.
+    Up to 15 vertices every distance plus the largest weight stays below the 16-bit
+    unreachable mark (0xF000) and the group finishes 16-bit; from 16 on it runs again
+    32-bit (17 and 40 have distances that 16 bits cannot hold).  The 40-vertex line stops
+    its 16-bit run after a few epochs, as soon as a written distance comes within the
+    largest weight of the mark."""
+    index, nbr, w = _line(n, 4095)
+    g = hc.Graph(index, nbr, w)
+    src = np.array([0, n - 1, n // 2, 0], dtype=np.int32)
+    dist, st = g.sssp_batched(src, use_graph=use_graph)
+    assert st.reruns == reruns
+    assert st.wide_groups == reruns
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(index, nbr, w, s)), i
+    if n == 40:
+        assert st.epochs >= 39  # the 32-bit rerun walks the whole line
+
+
+def test_sssp_batched_16bit_rerun_midway():
+    """Two components: a Kronecker graph (short distances) and a long line of weight 4000.
+    The first 64-source group stays 16-bit; the second holds a line vertex, runs again
+    32-bit, and so do the groups after it; every row matches Dijkstra."""
+    kr = hc.gen_kronecker(10, 8, 44, wtype=hc.W_I32)
+    ln_index, ln_nbr, ln_w = _line(60, 4000)
+    nk = kr.num_nodes
+    index = np.concatenate([kr.index, kr.index[-1] + ln_index[1:]]).astype(np.int64)
+    nbr = np.concatenate([kr.neighbors, ln_nbr + nk]).astype(np.int32)
+    w = np.concatenate([kr.weights, ln_w]).astype(np.int32)
+    g = hc.Graph(index, nbr, w)
+    src = hc.pick_sources(kr, 200)
+    src[70] = nk + 3  # in the second group of 64
+    with_host = np.empty((len(src), nk + 60), dtype=np.int32)
+    dist, st = g.sssp_batched(src, with_host, group=64)
+    assert st.reruns == 1
+    assert st.groups == 4 and st.wide_groups == 3
+    for i in list(range(0, 64, 9)) + [70] + list(range(64, 200, 13)):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(index, nbr, w, src[i])), i
+
+
+def test_sssp_batched_heavy_weights_stay_32bit():
+    """Weights above 4095 never use 16-bit distances."""
+    host = hc.gen_kronecker(10, 8, 45)
+    # symmetric weights: w(u->v) = w(v->u) through a hash of the unordered pair
+    u = np.repeat(np.arange(host.num_nodes), np.diff(host.index))
+    v = host.neighbors
+    lo, hi = np.minimum(u, v).astype(np.int64), np.maximum(u, v).astype(np.int64)
+    w = (((lo * 1000003 + hi) * 2654435761) % 99991 + 4096).astype(np.int32)
+    g = hc.Graph(host.index, host.neighbors, w)
+    src = hc.pick_sources(host, 40)
+    dist, st = g.sssp_batched(src)
+    assert st.wide_groups == st.groups and st.reruns == 0
+    for i in range(0, 40, 5):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, w, src[i])), i
 
 
 def test_sssp_batched_asymmetric_weights():
