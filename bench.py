@@ -312,8 +312,9 @@ def run_suite(a):
 def profile_case(a):
     """One source of BFS and SSSP, then one PageRank solve: the launches an ncu
     capture of bfs_persistent / sssp_persistent / sssp_pull_kernel / pr_sweep
-    selects.  With --suite batched: one 512-source batched BFS and one
-    256-source batched SSSP (device outputs)."""
+    selects.  With --suite batched: one 512-source batched BFS, one 512-source
+    batched SSSP group on 16-bit distances and one 256-source group on int32
+    distances (device outputs)."""
     import hc
     if a.suite == "batched":
         import torch
@@ -323,7 +324,8 @@ def profile_case(a):
         out = torch.empty((512, host.num_nodes), dtype=torch.int32, device="cuda")
         # Host-driven epoch loops, so that each kernel is a plain launch for the profiler.
         g.bfs_batched(src, out, use_graph=hc.GRAPH_OFF)
-        g.sssp_batched(src[:256], out[:256], group=256, use_graph=hc.GRAPH_OFF)
+        g.sssp_batched(src, out, group=512, use_graph=hc.GRAPH_OFF)  # 16-bit distances
+        g.sssp_batched(src[:256], out[:256], group=256, dist_bits=32, use_graph=hc.GRAPH_OFF)
         torch.cuda.synchronize()
         g.close()
         print(json.dumps({"mode": "profile", "suite": "batched", "scale": a.scale, "num_edges": host.num_edges}))
