@@ -245,6 +245,7 @@ template <bool kStats>
 __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
     __shared__ unsigned long long s_red[32];
     __shared__ int s_min[32];
+    __shared__ uint32_t s_fold[kSsspThreads / 32][2][32];  // per warp: near / far masks of its 32 words
     SsspCtl *ctl = a.ctl;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthreads = gridDim.x * blockDim.x;
@@ -299,8 +300,16 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
             after_pull = false;
             int32_t *fpile = (phase & 1) ? a.far1 : a.far0;
             int *fpile_len = &ctl->far_len[phase & 1];
-            // Lowered vertices back into the near queue / far pile.
+            // Lowered vertices back into the near queue / far pile.  A warp
+            // takes 32 words of the changed bitmap; pass 1 classifies their
+            // vertices a word at a time (lane l takes vertex 32j + l of word j:
+            // coalesced reads; each vertex is in one bit, so its stamps need
+            // no atomics) and keeps the ballots in shared memory; pass 2
+            // writes the queue and pile entries at offsets taken with one
+            // atomicAdd per warp.
             unsigned long long mf_next = 0;
+            const int wib = threadIdx.x >> 5;
+            const uint32_t below = (1u << lane) - 1u;
             for (int w0 = gwarp * 32; w0 < W_act; w0 += nwarps * 32) {
                 const int w = w0 + lane;
                 uint32_t bits = 0;
@@ -308,20 +317,69 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
                     bits = __ldcg(a.changed + w);
                     if (bits) a.changed[w] = 0;
                 }
-                while (__any_sync(kFull, bits != 0)) {
-                    bool near = false, far = false;
-                    int32_t v = 0;
-                    if (bits) {
-                        v = w * 32 + __ffs(bits) - 1;
-                        bits &= bits - 1;
-                        const int32_t d = __ldcg(a.dist + v);
-                        if (d < T) near = atomicMax(a.stamp + v, next_e) < next_e;
-                        else far = atomicMax(a.fstamp + v, phase + 1) < phase + 1;
-                        if (near) mf_next += (unsigned long long)(a.index[v + 1] - a.index[v]);
+                const unsigned words = __ballot_sync(kFull, bits != 0u);
+                int n_near = 0, n_far = 0;
+                // Four words per round, their loads issued together.
+                for (unsigned left = words; left;) {
+                    int j[4];
+                    bool mine[4];
+                    int32_t d[4], sp[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        j[k] = left ? __ffs(left) - 1 : -1;
+                        if (left) left &= left - 1u;
+                        const uint32_t word = __shfl_sync(kFull, bits, j[k] < 0 ? 0 : j[k]);
+                        mine[k] = j[k] >= 0 && ((word >> lane) & 1u);
+                        d[k] = mine[k] ? __ldcg(a.dist + (w0 + j[k]) * 32 + lane) : 0;
                     }
-                    warp_append(near, v, qnext, &ctl->qlen[nxt]);
-                    if (use_far) warp_append(far, v, fpile, fpile_len);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const int32_t v = (w0 + j[k]) * 32 + lane;
+                        sp[k] = !mine[k] ? 0 : d[k] < T ? a.stamp[v] : a.fstamp[v];
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const int32_t v = (w0 + j[k]) * 32 + lane;
+                        bool near = false, far = false;
+                        if (mine[k]) {
+                            if (d[k] < T) {
+                                near = sp[k] < next_e;
+                                if (near) a.stamp[v] = next_e;
+                            } else {
+                                far = sp[k] < phase + 1;
+                                if (far) a.fstamp[v] = phase + 1;
+                            }
+                            if (near) mf_next += (unsigned long long)(a.index[v + 1] - a.index[v]);
+                        }
+                        const uint32_t nm = __ballot_sync(kFull, near), fm = __ballot_sync(kFull, far);
+                        if (lane == 0 && j[k] >= 0) {
+                            s_fold[wib][0][j[k]] = nm;
+                            s_fold[wib][1][j[k]] = fm;
+                        }
+                        n_near += __popc(nm);
+                        n_far += __popc(fm);
+                    }
                 }
+                if (!use_far) n_far = 0;
+                int nbase = 0, fbase = 0;
+                if (lane == 0) {
+                    if (n_near) nbase = atomicAdd(&ctl->qlen[nxt], n_near);
+                    if (n_far) fbase = atomicAdd(fpile_len, n_far);
+                }
+                nbase = __shfl_sync(kFull, nbase, 0);
+                fbase = __shfl_sync(kFull, fbase, 0);
+                __syncwarp();
+                for (unsigned left = words; left;) {
+                    const int j = __ffs(left) - 1;
+                    left &= left - 1u;
+                    const uint32_t nm = s_fold[wib][0][j], fm = use_far ? s_fold[wib][1][j] : 0u;
+                    const int32_t v = (w0 + j) * 32 + lane;
+                    if ((nm >> lane) & 1u) qnext[nbase + __popc(nm & below)] = v;
+                    if ((fm >> lane) & 1u) fpile[fbase + __popc(fm & below)] = v;
+                    nbase += __popc(nm);
+                    fbase += __popc(fm);
+                }
+                __syncwarp();
             }
             mf_next = block_sum(mf_next, s_red);
             if (threadIdx.x == 0 && mf_next) atomicAdd(&ctl->mf[nxt], mf_next);
@@ -357,21 +415,64 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
             const int32_t T_old = T;
             const long long tn = ((long long)mfar / a.delta + 1) * (long long)a.delta;
             T = (int32_t)(tn < (long long)kInfDist ? tn : (long long)kInfDist);
-            // Split: [T_old, T) joins the epoch-E queue, >= T stays far.
+            // Split: [T_old, T) joins the epoch-E queue, >= T stays far.  A
+            // warp takes 1024 consecutive pile entries: pass 1 classifies them
+            // 32 at a time and keeps the ballots in shared memory, pass 2
+            // writes them at offsets taken with one atomicAdd per warp.
             unsigned long long mf_split = 0;
-            for (int i0 = gwarp * 32; i0 < fl; i0 += nwarps * 32) {
-                const int i = i0 + lane;
-                bool to_near = false, to_far = false;
-                int32_t v = 0;
-                if (i < fl) {
-                    v = __ldcg(fcur + i);
-                    const int32_t d = __ldcg(a.dist + v);
-                    if (d >= T_old && d < T) to_near = atomicMax(a.stamp + v, E) < E;
-                    else if (d >= T) to_far = atomicMax(a.fstamp + v, phase + 2) < phase + 2;
-                    if (to_near) mf_split += (unsigned long long)(a.index[v + 1] - a.index[v]);
+            const int wib = threadIdx.x >> 5;
+            const uint32_t below = (1u << lane) - 1u;
+            // Rounds of 32 entries per warp chunk: enough for every warp to
+            // get one chunk, at most 32 (the shared ballot slots).
+            const int per = min(32, max(1, (fl + 32 * nwarps - 1) / (32 * nwarps)));
+            for (int c0 = gwarp * 32 * per; c0 < fl; c0 += nwarps * 32 * per) {
+                const int rounds = min(per, (fl - c0 + 31) / 32);
+                int n_near = 0, n_far = 0;
+                for (int j0 = 0; j0 < rounds; j0 += 4) {
+                    int32_t v[4], d[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const int i = c0 + 32 * (j0 + k) + lane;
+                        v[k] = (j0 + k < rounds && i < fl) ? __ldcg(fcur + i) : -1;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; k++) d[k] = v[k] >= 0 ? __ldcg(a.dist + v[k]) : 0;
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        bool to_near = false, to_far = false;
+                        if (v[k] >= 0) {
+                            if (d[k] >= T_old && d[k] < T) to_near = atomicMax(a.stamp + v[k], E) < E;
+                            else if (d[k] >= T) to_far = atomicMax(a.fstamp + v[k], phase + 2) < phase + 2;
+                            if (to_near) mf_split += (unsigned long long)(a.index[v[k] + 1] - a.index[v[k]]);
+                        }
+                        const uint32_t nm = __ballot_sync(kFull, to_near), fm = __ballot_sync(kFull, to_far);
+                        if (lane == 0 && j0 + k < rounds) {
+                            s_fold[wib][0][j0 + k] = nm;
+                            s_fold[wib][1][j0 + k] = fm;
+                        }
+                        n_near += __popc(nm);
+                        n_far += __popc(fm);
+                    }
                 }
-                warp_append(to_near, v, qcur, &ctl->qlen[cur]);
-                warp_append(to_far, v, fnew, &ctl->far_len[(phase + 1) & 1]);
+                int nbase = 0, fbase = 0;
+                if (lane == 0) {
+                    if (n_near) nbase = atomicAdd(&ctl->qlen[cur], n_near);
+                    if (n_far) fbase = atomicAdd(&ctl->far_len[(phase + 1) & 1], n_far);
+                }
+                nbase = __shfl_sync(kFull, nbase, 0);
+                fbase = __shfl_sync(kFull, fbase, 0);
+                __syncwarp();
+                for (int j = 0; j < rounds; j++) {
+                    const uint32_t nm = s_fold[wib][0][j], fm = s_fold[wib][1][j];
+                    if ((nm | fm) >> lane & 1u) {
+                        const int32_t v = __ldcg(fcur + c0 + 32 * j + lane);
+                        if ((nm >> lane) & 1u) qcur[nbase + __popc(nm & below)] = v;
+                        else fnew[fbase + __popc(fm & below)] = v;
+                    }
+                    nbase += __popc(nm);
+                    fbase += __popc(fm);
+                }
+                __syncwarp();
             }
             mf_split = block_sum(mf_split, s_red);
             if (threadIdx.x == 0 && mf_split) atomicAdd(&ctl->mf[cur], mf_split);
