@@ -28,6 +28,21 @@ namespace {
 
 constexpr int kBfsThreads = 512;
 constexpr int kTraceLevels = 64;
+// Bottom-up levels copy the first kHubWords words of the frontier bitmap
+// (the 262144 highest-degree vertices of a degree-sorted graph, which most
+// edges point at) into shared memory and probe them there.
+constexpr int kHubWords = 8192;
+
+// Frontier bit of u: from the shared copy when u is in it, else from the
+// bitmap in global memory.  Both loads always issue (no branch, so the probes
+// of a round stay in flight); a copied vertex points its global load at word
+// 0, one line for the whole warp.  u < 0 (no edge) reads as 0.
+__device__ __forceinline__ uint32_t frontier_word(const uint32_t *s_fb, int hub_v, const uint32_t *fcur, int32_t u) {
+    const bool hub = u >= 0 && u < hub_v;
+    const uint32_t sw = s_fb[hub ? (u >> 5) : 0];
+    const uint32_t gw = u >= 0 ? __ldcg(fcur + (hub ? 0 : (u >> 5))) : 0u;
+    return hub ? sw : gw;
+}
 
 struct LevelCnt {
     int nf;                 // vertices in this frontier
@@ -112,8 +127,9 @@ struct TopDownVisit {
 };
 
 template <bool kStats>
-__global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
+__global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
     __shared__ unsigned long long s_red[32];
+    __shared__ uint32_t s_fb[kHubWords];
     BfsCtl *ctl = a.ctl;
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -228,6 +244,12 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
             bu_levels++;
             const int next_depth = L + 1;
             int found_local = 0;
+            // The frontier bitmap is complete (grid barrier) and read-only in
+            // this level: copy its hub prefix.
+            const int hub_w = min(kHubWords, W_act);
+            const int hub_v = hub_w << 5;
+            for (int i = threadIdx.x; i < hub_w; i += blockDim.x) s_fb[i] = __ldcg(fcur + i);
+            __syncthreads();
             // Rows of degree >= 32: warp per vertex, 32 probes per step.
             // AUTO = thread granularity with four probes in flight: on the
             // degree-sorted Kronecker graphs it beats warp-per-row for the
@@ -251,7 +273,7 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
                     int32_t u = 0;
                     if (i < e) {
                         u = a.nbr[i];
-                        hit = (__ldcg(fcur + (u >> 5)) >> (u & 31)) & 1u;
+                        hit = (frontier_word(s_fb, hub_v, fcur, u) >> (u & 31)) & 1u;
                     }
                     const unsigned bal = __ballot_sync(kFull, hit);
                     if (kStats) probes += bal ? (int64_t)__ffs(bal) : ((e - e0) < 32 ? (e - e0) : (int64_t)32);
@@ -286,7 +308,7 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_persistent(BfsArgs a) {
 #pragma unroll
                         for (int j = 0; j < 4; j++) u[j] = i + j < e ? a.nbr[i + j] : -1;
 #pragma unroll
-                        for (int j = 0; j < 4; j++) wd[j] = u[j] >= 0 ? __ldcg(fcur + (u[j] >> 5)) : 0u;
+                        for (int j = 0; j < 4; j++) wd[j] = frontier_word(s_fb, hub_v, fcur, u[j]);
 #pragma unroll
                         for (int j = 0; j < 4; j++)
                             if (par < 0 && u[j] >= 0 && ((wd[j] >> (u[j] & 31)) & 1u)) {
