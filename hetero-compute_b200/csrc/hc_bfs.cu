@@ -29,20 +29,9 @@ namespace {
 constexpr int kBfsThreads = 512;
 constexpr int kTraceLevels = 64;
 // Bottom-up levels copy the first kHubWords words of the frontier bitmap
-// (the 262144 highest-degree vertices of a degree-sorted graph, which most
+// (the 131072 highest-degree vertices of a degree-sorted graph, which most
 // edges point at) into shared memory and probe them there.
-constexpr int kHubWords = 8192;
-
-// Frontier bit of u: from the shared copy when u is in it, else from the
-// bitmap in global memory.  Both loads always issue (no branch, so the probes
-// of a round stay in flight); a copied vertex points its global load at word
-// 0, one line for the whole warp.  u < 0 (no edge) reads as 0.
-__device__ __forceinline__ uint32_t frontier_word(const uint32_t *s_fb, int hub_v, const uint32_t *fcur, int32_t u) {
-    const bool hub = u >= 0 && u < hub_v;
-    const uint32_t sw = s_fb[hub ? (u >> 5) : 0];
-    const uint32_t gw = u >= 0 ? __ldcg(fcur + (hub ? 0 : (u >> 5))) : 0u;
-    return hub ? sw : gw;
-}
+constexpr int kHubWords = 4096;
 
 struct LevelCnt {
     int nf;                 // vertices in this frontier

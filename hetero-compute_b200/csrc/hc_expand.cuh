@@ -111,6 +111,19 @@ __device__ __forceinline__ void expand_tasks(const int64_t *__restrict__ index, 
 }
 
 // Appends `v` for every lane with `take` set to q[*len ...], one atomic per warp.
+// Word of a frontier bitmap that holds vertex u's bit: from a shared-memory
+// copy of the bitmap's first hub_v / 32 words when u is in it, else from the
+// bitmap in global memory.  Both loads always issue (no branch, so the probes
+// of a round stay in flight); a copied vertex points its global load at word
+// 0, one line for the whole warp.  u < 0 (no edge) reads as 0.  On
+// degree-sorted graphs the copied prefix holds the hubs most edges point at.
+__device__ __forceinline__ uint32_t frontier_word(const uint32_t *s_fb, int hub_v, const uint32_t *fb, int32_t u) {
+    const bool hub = u >= 0 && u < hub_v;
+    const uint32_t sw = s_fb[hub ? (u >> 5) : 0];
+    const uint32_t gw = u >= 0 ? __ldcg(fb + (hub ? 0 : (u >> 5))) : 0u;
+    return hub ? sw : gw;
+}
+
 __device__ __forceinline__ void warp_append(bool take, int32_t v, int32_t *q, int *len) {
     const unsigned bal = __ballot_sync(kFull, take);
     if (!bal) return;
