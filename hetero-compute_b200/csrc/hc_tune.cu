@@ -127,6 +127,16 @@ hc_status tune_sssp(Tuner &tu, hc_tuning &out) {
     for (double f : {0.25, 0.5, 1.0, 2.0, 4.0}) deltas.push_back((int32_t)std::max(1.0, std::floor(base * f)));
     descend(o, &o.delta, deltas, best, run);
     if (g->w_symmetric) descend(o, &o.pull_alpha, {1, 2, 4, 8, -1}, best, run);
+    // Second, finer pass around the winners.
+    std::vector<int32_t> fine;
+    for (double f : {0.7, 0.85, 1.2, 1.4}) fine.push_back((int32_t)std::max(1.0, std::floor(o.delta * f)));
+    descend(o, &o.delta, fine, best, run);
+    if (g->w_symmetric && o.pull_alpha > 0) {
+        std::vector<int32_t> near;
+        for (int32_t x : {o.pull_alpha - 1, o.pull_alpha + 1, o.pull_alpha * 3 / 2})
+            if (x >= 1) near.push_back(x);
+        descend(o, &o.pull_alpha, near, best, run);
+    }
     out.sssp_delta = o.delta;
     out.sssp_pull_alpha = o.pull_alpha;
     return HC_OK;
