@@ -205,6 +205,25 @@ def test_sssp_batched_heavy_weights_stay_32bit():
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, w, src[i])), i
 
 
+@pytest.mark.parametrize("dist_bits", [0, 32])
+def test_sssp_batched_zero_weights_and_isolated_sources(dist_bits):
+    """All-zero weights (every reached distance 0) and sources without edges (only their own
+    distance is finite) in the same group as ordinary sources."""
+    host = hc.gen_kronecker(11, 8, 46)
+    w = np.zeros(host.num_edges, dtype=np.int32)
+    g = hc.Graph(host.index, host.neighbors, w)
+    deg = host.degrees()
+    isolated = np.flatnonzero(deg == 0)[:3].astype(np.int32)
+    assert len(isolated) == 3
+    src = np.concatenate([hc.pick_sources(host, 70), isolated, isolated[:1]])
+    dist, st = g.sssp_batched(src, dist_bits=dist_bits)
+    assert st.reruns == 0
+    for i, s in enumerate(src):
+        assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, host.neighbors, w, s)), i
+    for i in range(70, len(src)):
+        assert (dist[i] == 0).sum() == 1 and (dist[i] == np.iinfo(np.int32).max).sum() == host.num_nodes - 1
+
+
 def test_sssp_batched_asymmetric_weights():
     """w(u->v) != w(v->u): epochs stay push, weights read from u's row."""
     host = hc.gen_kronecker(12, 8, 3)
