@@ -138,3 +138,42 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(hc.HCError) as e:
         hc.Graph.from_host(g)
     assert e.value.status == hc.NO_DEVICE
+
+
+# ctypes mirrors of the public structs in include/hc.h (class name -> C type).
+_STRUCTS = {"CSR": "hc_csr", "GraphInfo": "hc_graph_info", "BfsOpts": "hc_bfs_opts", "BfsStats": "hc_bfs_stats",
+            "SsspOpts": "hc_sssp_opts", "SsspStats": "hc_sssp_stats", "PrOpts": "hc_pr_opts",
+            "PrStats": "hc_pr_stats", "BatchOpts": "hc_batch_opts", "BatchStats": "hc_batch_stats",
+            "Tuning": "hc_tuning"}
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """Every ctypes struct the Python binding passes through the C ABI has the size and field
+    offsets the C compiler gives the header's struct (a field added on one side only shifts
+    every field after it)."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not found")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "hc.h"', "int main(void) {"]
+    for py, c in _STRUCTS.items():
+        cls = getattr(hc, py)
+        lines.append(f'printf("{py} size %zu\\n", sizeof({c}));')
+        for name, _ in cls._fields_:
+            lines.append(f'printf("{py} {name} %zu\\n", offsetof({c}, {name}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            py, name, val = line.split()
+            got[(py, name)] = int(val)
+    for py in _STRUCTS:
+        cls = getattr(hc, py)
+        assert got[(py, "size")] == C.sizeof(cls), py
+        for name, _ in cls._fields_:
+            assert got[(py, name)] == getattr(cls, name).offset, (py, name)
