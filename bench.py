@@ -584,7 +584,9 @@ def main():
     value = world * a.steps * runs * (m / 2) / (total_ms / 1e3) / 1e9
 
     # End to end through the public API with host buffers: sources from pinned
-    # host memory in, depth/parent/distances/scores back to pinned host memory.
+    # host memory in, and back to pinned host memory what the reference's
+    # drivers return: BFS parents (bfs_gpu), SSSP distances (sssp_pull_gpu),
+    # PageRank scores (pr_pull_gpu).
     # The host buffers are placed (and the calls made) from the CPUs of the
     # GPU's NUMA node, where copies to and from the GPU are fastest; the
     # thread's CPU set is restored afterwards.
@@ -593,7 +595,6 @@ def main():
     if near:
         os.sched_setaffinity(0, near)
     src_pin = torch.from_numpy(src.copy()).pin_memory()
-    h_depth = torch.empty((k, n), dtype=torch.int32).pin_memory().numpy()
     h_parent = torch.empty((k, n), dtype=torch.int32).pin_memory().numpy()
     h_dist = torch.empty((k, n), dtype=torch.int32).pin_memory().numpy()
     h_scores = torch.empty(n, dtype=torch.float32).pin_memory().numpy()
@@ -603,7 +604,7 @@ def main():
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         s_np = src_pin.numpy()
-        g.bfs(s_np, h_depth, h_parent)
+        g.bfs(s_np, None, h_parent, want_depth=False)
         g.sssp(s_np, h_dist)
         g.pagerank(None, h_scores, tol_l1=1e-4, max_iters=50)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
@@ -664,7 +665,7 @@ def main():
             "config": workload(a) | {"num_nodes": n, "num_edges": m, "parallelism": f"replicas x{world}"},
             "roofline": roof, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": int(src.nbytes),
-                    "d2h_bytes_per_step": int(3 * k * n * 4 + n * 4),
+                    "d2h_bytes_per_step": int(2 * k * n * 4 + n * 4),
                     "host_cpus": (f"{len(near)} of {len(saved_cpus)}, the GPU's NUMA node" if near
                                   else f"all {len(saved_cpus)}")},
             "gpu_launches": launches, "clocks": clk.summary(), "per_algo": per_algo, "tuning": tuning,

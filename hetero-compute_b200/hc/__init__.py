@@ -351,10 +351,11 @@ class Graph:
 
     # -- algorithms.  Outputs: numpy (host) unless torch CUDA tensors are given.
     def bfs(self, sources, depth=None, parent=None, *, alpha=0, beta=0, direction=0, bu_variant=VARIANT_AUTO,
-            stats=False, want_parent=True):
+            stats=False, want_parent=True, want_depth=True):
+        """want_depth=False with depth=None returns parents only (the reference's bfs_gpu output)."""
         src = np.ascontiguousarray(sources, dtype=np.int32) if not hasattr(sources, "data_ptr") else sources
         k = len(src)
-        if depth is None:
+        if depth is None and want_depth:
             depth = np.empty((k, self.num_nodes), dtype=np.int32)
         if parent is None and want_parent:
             parent = np.empty((k, self.num_nodes), dtype=np.int32)

@@ -306,8 +306,11 @@ def test_host_outputs_pinned_and_mixed():
     dd2 = torch.empty((7, n), dtype=torch.int32, device="cuda")
     g.bfs(src, dd2, mixed_p)
     assert np.array_equal(dd2.cpu().numpy(), dd.cpu().numpy())
+    only_p = torch.empty((7, n), dtype=torch.int32).pin_memory().numpy()
+    d_none, _, _ = g.bfs(src, None, only_p, want_depth=False)  # parents only, as the reference's bfs_gpu
+    assert d_none is None
     for i, s in enumerate(src):  # parents may differ between runs (any neighbour one level up is valid)
-        for par in (pinned_p[i], mixed_p[i]):
+        for par in (pinned_p[i], mixed_p[i], only_p[i]):
             assert oracle.verify_bfs_parents(host.index, host.neighbors, pinned_d[i], par, s)[0] == 0
     sd = torch.empty((7, n), dtype=torch.int32, device="cuda")
     g.sssp(src, sd)
