@@ -73,6 +73,7 @@ struct WideDist {
     __device__ static W cand(W du, W w) { return du == kInfDist ? kInfDist : du + w; }
     __device__ static bool lowers(W nd, W d) { return nd < d; }
     __device__ static void atomic_lower(W *p, W nd, W) { atomicMin(p, nd); }
+    __device__ static W lower_of(W a, W b) { return min(a, b); }
     __device__ static void note(W &, W) {}
 };
 
@@ -97,6 +98,7 @@ struct NarrowDist {
             old = prev;
         }
     }
+    __device__ static W lower_of(W a, W b) { return __vminu2(a, b); }
     // Running per-halfword maximum of the finite values written.
     __device__ static void note(W &mx, W x) { mx = __vmaxu2(mx, x & __vcmpltu2(x, kInfWord)); }
 };
@@ -277,7 +279,7 @@ __device__ __forceinline__ void relax_range(const int64_t *index, const int32_t 
                     const W nd = D::cand(du[s], wt[k]);
                     if (ok[k] && D::lowers(nd, d[k][s])) {
                         D::atomic_lower(dist + (size_t)v[k] * KW + lane * SPL + s, nd, d[k][s]);
-                        D::note(wmax, nd);
+                        D::note(wmax, D::lower_of(nd, d[k][s]));  // only the halves that fell
                         imp[k] = true;
                     }
                 }
