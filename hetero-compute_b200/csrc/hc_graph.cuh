@@ -66,6 +66,10 @@ struct hc_graph {
     hc::PrPlanDev pr_view{};   // host copy of its pointers and counts
     int32_t pr_partial_slots = 0;
     hc::DevBuf pr_plan_huge_rows;
+    // level schedule of the reference-order PageRank sweep (hc_pr_ordered.cu):
+    // order[N] | level_off[levels + 1] | deg as fp32 [N]; levels -1 = not built
+    hc::DevBuf pr_ord;
+    int32_t pr_ord_levels = -1;
 
     // symmetry of the PageRank transition (-1: not checked yet)
     int pr_sym_struct = -1;    // every edge u->v has v->u (rows sorted)

@@ -127,6 +127,7 @@ _SIGS = {
     "hc_sssp": (C.c_int, [_P, _P, C.c_int32, _P, _P, C.POINTER(SsspOpts), C.POINTER(SsspStats)]),
     "hc_pr_forward": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(PrOpts), C.POINTER(PrStats)]),
     "hc_pr_backward": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(PrOpts), C.POINTER(PrStats)]),
+    "hc_pr_pull_ordered": (C.c_int, [_P, _P, _P, C.POINTER(PrOpts), C.POINTER(PrStats)]),
     "hc_ppr_batched": (C.c_int, [_P, _P, _P, C.c_int32, _P, C.POINTER(PrOpts), C.POINTER(PrStats)]),
     "hc_bfs_batched": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(BatchOpts), C.POINTER(BatchStats)]),
     "hc_sssp_batched": (C.c_int, [_P, _P, C.c_int32, _P, C.POINTER(BatchOpts), C.POINTER(BatchStats)]),
@@ -388,6 +389,17 @@ class Graph:
                "hc_pr_forward")
         return scores, st
 
+    def pagerank_ordered(self, init=None, scores=None, *, damping=0.85, eps_vertex=5e-8, max_iters=0):
+        """hc_pr_pull_ordered: in-place sweeps in vertex order with the per-vertex eps rule, the reference's
+        single-thread pr_pull_cpu bit for bit (max_iters 0 = until a sweep stores nothing)."""
+        if scores is None:
+            scores = np.empty(self.num_nodes, dtype=np.float32)
+        o = PrOpts(damping, 0.0, eps_vertex, max_iters, 0, VARIANT_AUTO, 0)
+        st = PrStats()
+        _check(lib().hc_pr_pull_ordered(self._h, _ptr(init), _ptr(scores), C.byref(o), C.byref(st)),
+               "hc_pr_pull_ordered")
+        return scores, st
+
     def pagerank_backward(self, scores, dL_dscores, *, damping=0.85, tol_l1=1e-7, eps_vertex=0.0, max_iters=500,
                           weighted=False, want_dw=True, dteleport=None, dweights=None, accel=0):
         if dteleport is None:
@@ -467,8 +479,9 @@ def sssp_pull_gpu(g: Graph, source_id: int):
     return dist[0]
 
 
-def pr_pull_gpu(g: Graph, *, eps_vertex: float = 5e-8, max_iters: int = 201):
-    """pr_pull_gpu (src/kernels/gpu/pr.cuh:42-118): reference stopping rule (no vertex moves by more than
-    5e-8, at most 201 sweeps)."""
-    scores, _ = g.pagerank(tol_l1=0.0, eps_vertex=eps_vertex, max_iters=max_iters)
+def pr_pull_gpu(g: Graph, init_score=None, *, eps_vertex: float = 5e-8, max_iters: int = 201):
+    """pr_pull_gpu (src/kernels/gpu/pr.cuh:42-118): the reference's in-place sweep and stopping rule (a score
+    moves only by more than 5e-8; stop when a sweep moves none, at most 201 sweeps), in the single-thread
+    vertex order of pr_pull_cpu (src/kernels/cpu/pr.cuh:33-65), so the scores equal that code's bit for bit."""
+    scores, _ = g.pagerank_ordered(init_score, eps_vertex=eps_vertex, max_iters=max_iters)
     return scores

@@ -256,6 +256,24 @@ hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t ncols,
                         float *scores_out, const hc_pr_opts *opts,
                         hc_pr_stats *stats);
 
+/* PageRank in the reference's own sweep order: scores updated in place from
+ * vertex 0 to N-1, each vertex reading this sweep's scores of lower
+ * neighbours and the previous sweep's of higher ones, a score stored only
+ * when it moves by more than eps_vertex, until a sweep stores nothing (or
+ * max_iters sweeps).  This is pr_pull_cpu with epoch_pr_pull_cpu_one_to_one
+ * on one thread (src/kernels/cpu/pr.cuh:33-65, :157-187), and the rule of
+ * pr_pull_gpu's epoch kernels (src/kernels/gpu/pr.cuh:42-118, :140-174)
+ * without their run-to-run variation: the output equals the reference's
+ * single-thread scores bit for bit.  Runs as a level schedule (built once per
+ * graph) on the device; needs every edge to have a reverse
+ * (HC_ERR_UNSUPPORTED otherwise).  init_scores: [num_nodes] fp32 or NULL for
+ * 1/N.  opts: damping (0 -> 0.85), eps_vertex (0 -> 5e-8), max_iters (0 ->
+ * no cap); tol_l1, weighted, variant and accel are ignored (unweighted
+ * degrees, as the reference).  stats->iterations = sweeps, converged = 1 when
+ * the last sweep stored nothing, changed = scores stored by the last sweep. */
+hc_status hc_pr_pull_ordered(hc_graph *g, const float *init_scores, float *scores_out,
+                             const hc_pr_opts *opts, hc_pr_stats *stats);
+
 /* Adjoint of hc_pr_forward for ncols == 1.  Given the converged scores x and
  * dL/dx, solves lambda = dL/dx + d A^T lambda and returns
  * dL/dteleport = (1-d) lambda and, if dL_dweights != NULL, the gradient

@@ -350,7 +350,11 @@ inline double sssp_pull_gpu(const CSRWGraph &g, sssp_gpu_epoch_func epoch_kernel
 }
 
 // pr_pull_gpu (src/kernels/gpu/pr.cuh:42-118): at most 201 epochs, stops
-// when no vertex moves by more than 5e-8.
+// when no vertex moves by more than 5e-8.  With epoch_pr_auto the sweeps run
+// in the reference's single-thread vertex order (hc_pr_pull_ordered), so the
+// scores equal pr_pull_cpu's on one thread bit for bit; the named epoch
+// kernels run the reference's own host loop, whose order (and so its stopping
+// point) varies with the thread schedule, as the reference's does.
 inline double pr_pull_gpu(const CSRWGraph &g, pr_gpu_epoch_func epoch_kernel, weight_t *init_score,
                           weight_t **const ret_score, int block_count = 64, int thread_count = 1024) {
     using namespace hc_compat;
@@ -368,7 +372,7 @@ inline double pr_pull_gpu(const CSRWGraph &g, pr_gpu_epoch_func epoch_kernel, we
         o.eps_vertex = 5e-8f;
         o.max_iters = 201;
         hc_pr_stats st{};
-        check(hc_pr_forward(hg, nullptr, 1, score, &o, &st), "hc_pr_forward");
+        check(hc_pr_pull_ordered(hg, init_score, score, &o, &st), "hc_pr_pull_ordered");
         ms = st.ms;
         hc_graph_destroy(hg);
     } else {

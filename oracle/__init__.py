@@ -40,7 +40,7 @@ def lib():
         L.or_sssp_dijkstra.restype = C.c_int
         L.or_verify_sp_tree.argtypes = [P, P, P, P, P, C.c_int32, C.c_int32]
         L.or_verify_sp_tree.restype = C.c_int64
-        L.or_pr_pull.argtypes = [P, P, C.c_int32, C.c_float, C.c_float, C.c_int32, P]
+        L.or_pr_pull.argtypes = [P, P, C.c_int32, C.c_float, C.c_float, C.c_int32, P, P]
         L.or_pr_pull.restype = C.c_int32
         L.or_pr_jacobi_f64.argtypes = [P, P, P, C.c_int32, P, C.c_double, C.c_double, C.c_int32, P]
         L.or_pr_jacobi_f64.restype = C.c_int32
@@ -81,11 +81,13 @@ def verify_sp_tree(index, nbr, w, dist, parent, src):
                                        _p(np.ascontiguousarray(parent, dtype=np.int32)), len(index) - 1, int(src)))
 
 
-def pr_pull(index, nbr, damping=0.85, eps=5e-8, max_iters=0):
-    """Reference CPU PageRank on one thread (src/kernels/cpu/pr.cuh:33-65)."""
+def pr_pull(index, nbr, damping=0.85, eps=5e-8, max_iters=0, init=None):
+    """Reference CPU PageRank on one thread (src/kernels/cpu/pr.cuh:33-65); init (fp32 [N]) replaces the
+    uniform 1/N start, as the caller's init_score of pr_pull_gpu (src/kernels/gpu/pr.cuh:42-46)."""
     n = len(index) - 1
     s = np.empty(n, dtype=np.float32)
-    it = lib().or_pr_pull(_p(index), _p(nbr), n, damping, eps, max_iters, _p(s))
+    ini = None if init is None else np.ascontiguousarray(init, dtype=np.float32)
+    it = lib().or_pr_pull(_p(index), _p(nbr), n, damping, eps, max_iters, _p(ini), _p(s))
     return s, int(it)
 
 

@@ -154,16 +154,18 @@ int64_t or_verify_sp_tree(const int64_t *index, const int32_t *nbr, const int32_
 /* ------------------------------------------------------------- PageRank */
 
 /* pr_pull_cpu with epoch_pr_pull_cpu_one_to_one on one thread:
- * src/kernels/cpu/pr.cuh:33-65 and :157-187.  Scores start at 1/N (the
- * reference ignores init_scores), each sweep updates in place in vertex
+ * src/kernels/cpu/pr.cuh:33-65 and :157-187.  Scores start at 1/N as the
+ * CPU reference does (it ignores init_scores), or at init_scores when given
+ * (the caller's init_score of pr_pull_gpu, src/kernels/gpu/pr.cuh:42-46,
+ * 77-80); each sweep updates in place in vertex
  * order: new = (1 - d)/N + d * sum_u score[u]/deg(u) in float, written only
  * when |new - old| > eps; stops after a sweep with no write, or after
  * max_iters sweeps (the CPU reference has no cap).  Returns the sweeps run. */
 int32_t or_pr_pull(const int64_t *index, const int32_t *nbr, int32_t n, float damping, float eps,
-                   int32_t max_iters, float *score) {
+                   int32_t max_iters, const float *init_scores, float *score) {
     const float init = 1.0f / (float)n;
     const float base = (1.0f - damping) / (float)n;
-    for (int32_t i = 0; i < n; i++) score[i] = init;
+    for (int32_t i = 0; i < n; i++) score[i] = init_scores ? init_scores[i] : init;
     int32_t it = 0;
     for (;;) {
         int64_t updated = 0;

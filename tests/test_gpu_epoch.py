@@ -67,11 +67,17 @@ def test_epoch_pr_pull(golden, variant):
         if int(upd.item()) == 0:
             break
     # In-place sweeps stop on the per-vertex 5e-8 rule wherever their update
-    # order leaves them; hold the kernel to the reference's own accuracy.
+    # order leaves them, as the reference's own GPU epoch kernels do (their
+    # scores vary from run to run); the single-thread order is checked bit for
+    # bit by hc_pr_pull_ordered.  Three L-inf numbers, printed and bounded.
     x, _ = oracle.pr_jacobi_f64(host.index, host.neighbors, tol=1e-15, max_iters=3000)
-    ref_err = np.abs(arr["pr_scores"] - x).max()
-    err = np.abs(score.cpu().numpy() - x).max()
-    assert err <= max(1e-5, 1.5 * ref_err), (err, ref_err)
+    s = score.cpu().numpy()
+    ref = arr["pr_scores"]
+    gpu_ref, ref_64, gpu_64 = (float(np.abs(s - ref).max()), float(np.abs(ref - x).max()),
+                               float(np.abs(s - x).max()))
+    print(f"epoch pagerank variant {variant}: |GPU-ref| {gpu_ref:.3e}  |ref-FP64| {ref_64:.3e}  "
+          f"|GPU-FP64| {gpu_64:.3e}")
+    assert gpu_ref <= 1e-5 and gpu_64 <= 1e-5, (gpu_ref, ref_64, gpu_64)
 
 
 @pytest.mark.parametrize("variant", [hc.VARIANT_THREAD, hc.VARIANT_WARP])
