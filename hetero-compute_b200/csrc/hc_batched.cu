@@ -62,8 +62,6 @@ struct MsCtl {
 // Default direction switch: push while the frontier's edges times
 // kMsPushAlpha stay below M.
 constexpr int kMsPushAlpha = 10;
-// Wall-clock bound of one group's level loop (checked between levels).
-constexpr unsigned long long kMsLimitNs = 60ull * 1000000000ull;
 
 __device__ __forceinline__ bool ms_live(const MsCtl *c) { return !c->stop && !c->fin; }
 __device__ __forceinline__ bool ms_push(const MsCtl *c) {
@@ -434,7 +432,7 @@ __global__ void msbfs_end(MsCtl *ctl, double pull_bytes, cudaGraphConditionalHan
         } else if (ctl->level >= ctl->max_levels) {
             ctl->stop = 1;
             ctl->status = HC_ERR_NOT_CONVERGED;
-        } else if (globaltimer_ns() - ctl->t0 > kMsLimitNs) {
+        } else if (globaltimer_ns() - ctl->t0 > c_limits.loop_ns) {
             ctl->stop = 1;
             ctl->status = HC_ERR_TIMEOUT;
         } else {

@@ -36,8 +36,6 @@ constexpr int kLongRow = 2048;
 // M: a pull reads every row of the distance matrix once, a push only the rows
 // its queue's edges reach.
 constexpr int kPullAlpha = 2;
-// Wall-clock bound of one group's epoch loop (checked between epochs).
-constexpr unsigned long long kGroupLimitNs = 60ull * 1000000000ull;
 
 // Distance words.
 //
@@ -122,6 +120,7 @@ struct MsspCtl {
     unsigned maxw;                  // largest finite distance written so far (narrow epochs)
     int w_max;                      // largest edge weight
     int narrow;                     // 16-bit distance words
+    int overflow;                   // 32-bit words: a distance wrapped past INT32_MAX (transpose)
 };
 
 __device__ __forceinline__ int ctl_queue(const MsspCtl *ctl, int c) { return ctl->stop ? 0 : ctl->qlen[c]; }
@@ -596,7 +595,7 @@ __global__ void mssp_end(MsspCtl *ctl, int c, cudaGraphConditionalHandle cond, i
             ctl->status = HC_ERR_NOT_CONVERGED;
             go = false;
         }
-        if (go && globaltimer_ns() - ctl->t0 > kGroupLimitNs) {
+        if (go && globaltimer_ns() - ctl->t0 > c_limits.loop_ns) {
             ctl->stop = 1;
             ctl->status = HC_ERR_TIMEOUT;
             go = false;
@@ -622,12 +621,16 @@ __global__ void mssp_transpose(const typename D::W *dist, int32_t n, int nsrc, i
     __shared__ int32_t tile[TV][K + 1];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
     unsigned mx = 0;
+    bool wrapped = false;
     for (int64_t vb = (int64_t)blockIdx.x * TV; vb < n; vb += (int64_t)gridDim.x * TV) {
         for (int r = ty; r < TV; r += 8) {
             const int64_t v = vb + r;
             for (int c = tx; c < KW; c += 32) {
                 const typename D::W x = v < n ? dist[(size_t)v * KW + c] : D::kInfWord;
                 if constexpr (D::kPer == 1) {
+                    // Sums of non-negative weights only fall, so a wrapped
+                    // one stays negative to the end.
+                    wrapped |= (int32_t)x < 0;
                     tile[r][c] = x;
                 } else {
 #pragma unroll
@@ -652,6 +655,8 @@ __global__ void mssp_transpose(const typename D::W *dist, int32_t n, int nsrc, i
     if constexpr (D::kPer == 2) {
         mx = __reduce_max_sync(kFull, mx);
         if (tx == 0 && mx) atomicMax(&ctl->maxf, mx);
+    } else {
+        if (__any_sync(kFull, wrapped) && tx == 0) ctl->overflow = 1;
     }
 }
 
@@ -783,6 +788,14 @@ hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int 
         HC_CUDA_TRY(cudaMemcpyAsync(hctl, b.ctl, sizeof(MsspCtl), cudaMemcpyDeviceToHost, g->stream));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
         *fits = (int64_t)hctl->maxf + g->w_max < (int64_t)kInf16;
+    } else if (dst && (int64_t)g->w_max * std::max<int64_t>(g->n_active - 1, 0) >= (int64_t)kInfDist) {
+        // A path of n_active - 1 largest weights could pass INT32_MAX: read
+        // the transpose's wrap flag.
+        HC_CUDA_TRY(cudaMemcpyAsync(hctl, b.ctl, sizeof(MsspCtl), cudaMemcpyDeviceToHost, g->stream));
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (hctl->overflow)
+            return fail(HC_ERR_UNSUPPORTED, "hc_sssp_batched: a distance exceeds INT32_MAX (largest weight %d)",
+                        g->w_max);
     }
     return HC_OK;
 }

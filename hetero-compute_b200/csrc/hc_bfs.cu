@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
             break;
         }
         if (gtid == 0) {
-            if (globaltimer_ns() - t_start > kRunLimitNs) atomicExch(&ctl->gs.err, (int)HC_ERR_TIMEOUT);
+            if (globaltimer_ns() - t_start > c_limits.run_ns) atomicExch(&ctl->gs.err, (int)HC_ERR_TIMEOUT);
             ctl->cnt[old].nf = 0;
             ctl->cnt[old].tasks = 0;
             ctl->cnt[old].mf = 0;
@@ -528,7 +528,7 @@ constexpr int64_t kNoAllocMaxEdges = 1ll << 24;
 constexpr size_t na_align(size_t b) { return (b + 255) / 256 * 256; }
 constexpr size_t kNaWords = (size_t)kNoAllocMaxNodes / 32;
 constexpr size_t kNaTasks = (size_t)(kNoAllocMaxEdges / kTaskEdges + kNoAllocMaxEdges / (kSmallDeg + 1) + 64);
-constexpr size_t kNoAllocBytes = na_align(sizeof(BfsCtl)) + 4 * na_align(4 * kNaWords) +
+constexpr size_t kNoAllocBytes = na_align(sizeof(BfsCtl)) + na_align(sizeof(int)) + 4 * na_align(4 * kNaWords) +
                                  2 * na_align(4 * (size_t)kNoAllocMaxNodes) + na_align(sizeof(int2) * kNaTasks);
 
 static __device__ __align__(256) unsigned char g_bfs_scratch[kNoAllocBytes];
@@ -602,6 +602,7 @@ extern "C" hc_status hc_bfs_noalloc(const int64_t *index, const int32_t *neighbo
     };
     BfsArgs a{};
     a.ctl = reinterpret_cast<BfsCtl *>(take(sizeof(BfsCtl)));
+    int *check_flag = reinterpret_cast<int *>(take(sizeof(int)));
     a.visited = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
     a.fb0 = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
     a.fb1 = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
@@ -624,6 +625,15 @@ extern "C" hc_status hc_bfs_noalloc(const int64_t *index, const int32_t *neighbo
     a.bu_variant = HC_VARIANT_THREAD;
     a.max_levels = num_nodes + 1;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // The caller's CSR is checked before the traversal reads it (offsets
+    // rising from 0 to num_edges, neighbour ids in [0, num_nodes)); the check
+    // writes its flag into the fixed array too.
+    HC_TRY(csr_check_async(index, neighbors, 1, num_nodes, num_edges, check_flag, sms, s));
+    int bad = 0;
+    HC_CUDA_TRY(cudaMemcpyAsync(&bad, check_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (bad & 1) return fail(HC_ERR_INVALID_ARG, "hc_bfs_noalloc: offsets must rise from 0 to num_edges");
+    if (bad & 2) return fail(HC_ERR_INVALID_ARG, "hc_bfs_noalloc: neighbour id outside [0, num_nodes)");
     // The array keeps the previous call's contents; the control block must
     // start at zero (the kernel initialises everything else it reads).
     HC_CUDA_TRY(cudaMemsetAsync(a.ctl, 0, sizeof(BfsCtl), s));

@@ -30,12 +30,36 @@ namespace hc {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int32_t kInfDist = 0x7fffffff;
 
-// Bound on every device-side spin: a wait that lasts longer than this gives
-// up, records HC_ERR_TIMEOUT and lets the kernel return.
+// Time limits of the device-side waits (defaults below; hc_set_time_limits
+// shortens them so that tests can make each one run out):
+//   wait  every device-side spin: a wait that lasts longer gives up, records
+//         HC_ERR_TIMEOUT and lets the kernel return;
+//   run   one persistent run (all its epochs): past it the run records
+//         HC_ERR_TIMEOUT and every block leaves at the next barrier;
+//   loop  one batched group's epoch loop (a CUDA-graph while loop), checked
+//         by the kernel that ends each epoch.
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
-// Bound on one persistent run (all its epochs): past it the run records
-// HC_ERR_TIMEOUT and every block leaves at the next barrier.
 constexpr unsigned long long kRunLimitNs = 20000000000ull;
+constexpr unsigned long long kLoopLimitNs = 60000000000ull;
+struct TimeLimits {
+    unsigned long long wait_ns, run_ns, loop_ns;
+};
+// One copy per translation unit (no relocatable device code); every copy is
+// registered with the setter behind hc_set_time_limits.
+static __constant__ TimeLimits c_limits = {kWaitLimitNs, kRunLimitNs, kLoopLimitNs};
+using LimitSetter = hc_status (*)(const TimeLimits &);
+void register_limit_setter(LimitSetter f);
+static hc_status set_unit_limits(const TimeLimits &t) {
+    if (cudaMemcpyToSymbol(c_limits, &t, sizeof(t)) != cudaSuccess)
+        return fail(HC_ERR_CUDA, "hc_set_time_limits: cudaMemcpyToSymbol failed");
+    return HC_OK;
+}
+namespace {
+struct LimitSetterReg {
+    LimitSetterReg() { register_limit_setter(&set_unit_limits); }
+};
+static LimitSetterReg g_limit_setter_reg;
+}  // namespace
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
     unsigned long long t;
@@ -55,7 +79,7 @@ __device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
 
 // Grid-wide barrier for cooperative (co-resident) launches.  Arrival is an
 // atomic on `count`; the last block to arrive resets it and bumps `gen`.
-// Waiters poll `gen` with an acquire load and give up after kWaitLimitNs,
+// Waiters poll `gen` with an acquire load and give up after the wait limit,
 // setting *err.  Once *err is set every later barrier returns at once, so a
 // failed run drains in bounded time.  Returns false when the run must stop.
 struct GridSync {
@@ -84,7 +108,7 @@ __device__ __forceinline__ bool grid_barrier(GridSync *gs) {
                 unsigned long long t0 = globaltimer_ns();
                 while (ld_acquire_u32(&gs->gen) == my_gen) {
                     if (*(volatile int *)&gs->err) { ok = 0; break; }
-                    if (globaltimer_ns() - t0 > kWaitLimitNs) {
+                    if (globaltimer_ns() - t0 > c_limits.wait_ns) {
                         atomicExch(&gs->err, (int)HC_ERR_TIMEOUT);
                         ok = 0;
                         break;

@@ -177,6 +177,45 @@ __global__ void analyze_rows(const int64_t *index, const int32_t *nbr, int32_t n
     }
 }
 
+}  // namespace
+
+// One pass over a caller's CSR: every row [index[v], index[v+1]) inside
+// [0, m], index[0] == 0, index[n] == m, and every neighbour id in [0, n).
+// A row whose bounds fail is not read, so the check itself stays inside the
+// arrays (index[n + 1] entries, neighbours m entries of `stride` int32 words:
+// 1 for an id array, 2 for the reference's interleaved {id, weight} layout).
+// Sets bit 0 of *flag for a bad offset and bit 1 for a bad neighbour id.
+__global__ void csr_check(const int64_t *index, const int32_t *nbr, int stride, int32_t n, int64_t m, int *flag) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const int64_t b = index[v], e = index[v + 1];
+        const bool row_ok = b >= 0 && b <= e && e <= m && (v != 0 || b == 0) && (v != n - 1 || e == m);
+        if (!row_ok) {
+            if (lane == 0) atomicOr(flag, 1);
+            continue;
+        }
+        bool bad = false;
+        for (int64_t i = b + lane; i < e; i += 32) {
+            const int32_t x = nbr[i * stride];
+            bad |= x < 0 || x >= n;
+        }
+        if (__any_sync(kFull, bad) && lane == 0) atomicOr(flag, 2);
+    }
+}
+
+hc_status csr_check_async(const int64_t *index, const int32_t *nbr, int stride, int32_t n, int64_t m, int *flag_dev,
+                          int sm_count, cudaStream_t s) {
+    HC_CUDA_TRY(cudaMemsetAsync(flag_dev, 0, sizeof(int), s));
+    if (n < 1) return HC_OK;
+    const int blocks = (int)std::min<int64_t>((int64_t)sm_count * 8, ((int64_t)n + 7) / 8);
+    { csr_check<<<blocks, 256, 0, s>>>(index, nbr, stride, n, m, flag_dev); ::hc::count_launch(); }
+    HC_CUDA_TRY(cudaGetLastError());
+    return HC_OK;
+}
+
+namespace {
+
 __global__ void build_inv_deg(const int64_t *index, int32_t n, float *inv_deg) {
     const int stride = gridDim.x * blockDim.x;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
@@ -458,6 +497,29 @@ hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const 
         g->n_warp_rows = 0;
     }
     *out = g;
+    return HC_OK;
+}
+
+hc_status hc_csr_check(const int64_t *index, const void *neighbors, int32_t interleaved, int32_t num_nodes,
+                       int64_t num_edges, void *stream) {
+    clear_error();
+    if (!index || num_nodes < 1 || num_edges < 0 || (num_edges > 0 && !neighbors))
+        return fail(HC_ERR_INVALID_ARG, "hc_csr_check: bad arguments (N=%d, M=%lld)", num_nodes, (long long)num_edges);
+    if (!is_device_pointer(index) || (num_edges > 0 && !is_device_pointer(neighbors)))
+        return fail(HC_ERR_INVALID_ARG, "hc_csr_check: index and neighbours must be device memory");
+    int dev = 0, sms = 0;
+    HC_CUDA_TRY(cudaGetDevice(&dev));
+    HC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DevBuf flag;
+    HC_TRY(flag.ensure(sizeof(int)));
+    HC_TRY(csr_check_async(index, static_cast<const int32_t *>(neighbors), interleaved ? 2 : 1, num_nodes, num_edges,
+                           flag.as<int>(), sms, s));
+    int h = 0;
+    HC_CUDA_TRY(cudaMemcpyAsync(&h, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h & 1) return fail(HC_ERR_INVALID_ARG, "hc_csr_check: offsets must rise from 0 to num_edges");
+    if (h & 2) return fail(HC_ERR_INVALID_ARG, "hc_csr_check: neighbour id outside [0, num_nodes)");
     return HC_OK;
 }
 

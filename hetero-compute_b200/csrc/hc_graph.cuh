@@ -135,6 +135,11 @@ struct OutPipe {
     hc_status finish();
 };
 
+// Checks a caller's CSR on the device (offsets rising from 0 to m, neighbour
+// ids in [0, n); `stride` 2 for interleaved {id, weight} edges): clears
+// *flag_dev, then sets bit 0 (offsets) / bit 1 (ids) on a violation.
+hc_status csr_check_async(const int64_t *index, const int32_t *nbr, int stride, int32_t n, int64_t m, int *flag_dev,
+                          int sm_count, cudaStream_t s);
 // Whether the PageRank transition is a reversible walk (symmetric structure,
 // and symmetric weights when `weighted`), checked once per graph.
 hc_status ensure_pr_symmetry(hc_graph *g, bool weighted, bool *symmetric);

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
             }
             return;
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0 && globaltimer_ns() - t_start > kRunLimitNs)
+        if (blockIdx.x == 0 && threadIdx.x == 0 && globaltimer_ns() - t_start > c_limits.run_ns)
             atomicExch(&a.ctl->gs.err, (int)HC_ERR_TIMEOUT);
         if (s + 1 == a.sweep_end && blockIdx.x == 0 && threadIdx.x == 0) a.ctl->last_updated = u;
     }

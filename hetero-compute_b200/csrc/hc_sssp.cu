@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
             E++;
             continue;
         }
-        if (gtid == 0 && globaltimer_ns() - t_start > kRunLimitNs) atomicExch(&ctl->gs.err, (int)HC_ERR_TIMEOUT);
+        if (gtid == 0 && globaltimer_ns() - t_start > c_limits.run_ns) atomicExch(&ctl->gs.err, (int)HC_ERR_TIMEOUT);
         int nq = __ldcg(&ctl->qlen[cur]);
         if (nq == 0) {
             if (!use_far) break;
@@ -600,6 +600,15 @@ __global__ void count_finite(const int32_t *dist, int32_t n, unsigned long long 
     if (threadIdx.x == 0 && c) atomicAdd(out, c);
 }
 
+// Distances are int32 sums of non-negative weights.  A sum past INT32_MAX
+// wraps to a negative value, and a relaxation only ever lowers a distance, so
+// the run overflowed exactly when some final distance is negative.
+__global__ void any_negative(const int32_t *dist, int32_t n, int *flag) {
+    bool neg = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) neg |= dist[i] < 0;
+    if (__any_sync(kFull, neg) && (threadIdx.x & 31) == 0) *flag = 1;
+}
+
 // Whether any weight is negative (flags[0]), the largest weight (flags[1])
 // and the weights' sum.
 __global__ void weight_stats(const int64_t *index, const int32_t *w, int32_t n, int *flags, unsigned long long *sum) {
@@ -785,6 +794,12 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
 
     HC_TRY(g->pinned.ensure(sizeof(SsspCtl)));
     volatile int *h_flags = g->pinned.as<int>();
+    // Overflow is possible only when a path of n_active - 1 edges of the
+    // largest weight can pass INT32_MAX; then each source's distances are
+    // checked after its run (a flag in the control block's spare half).
+    static_assert(sizeof(SsspCtl) <= 2048, "SsspCtl overlaps its spare slots");
+    const bool check_overflow = (int64_t)g->w_max * std::max<int64_t>(g->n_active - 1, 0) >= (int64_t)kInfDist;
+    int *neg_flag = (int *)((char *)a.ctl + 2056);
     double total_ms = 0;
     for (int32_t i = 0; i < num_sources; i++) {
         a.src = src[i];
@@ -807,6 +822,12 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
             HC_TRY(pipe.release(i, dst));
         }
         SsspCtl c;
+        int negative = 0;
+        if (check_overflow) {
+            HC_CUDA_TRY(cudaMemsetAsync(neg_flag, 0, sizeof(int), g->stream));
+            { any_negative<<<g->sm_count * 4, 256, 0, g->stream>>>(a.dist, g->N, neg_flag); ::hc::count_launch(); }
+            HC_CUDA_TRY(cudaMemcpyAsync(&negative, neg_flag, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+        }
         HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
         if (o.collect_stats && stats) {
             unsigned long long *cnt = (unsigned long long *)((char *)a.ctl + 2048);
@@ -820,6 +841,9 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
         if (c.gs.err) return fail((hc_status)c.gs.err, "hc_sssp: device run from source %d ended with status %d",
                                   src[i], c.gs.err);
+        if (negative)
+            return fail(HC_ERR_UNSUPPORTED, "hc_sssp: a distance from source %d exceeds INT32_MAX (int32 "
+                        "distances; largest weight %d)", src[i], g->w_max);
         float ms = 0;
         HC_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_start, g->ev_stop));
         total_ms += ms;

@@ -141,6 +141,9 @@ _SIGS = {
     "hc_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "hc_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "hc_bfs_noalloc": (C.c_int, [_P, _P, C.c_int32, C.c_int64, C.c_int32, _P, _P, _P]),
+    "hc_set_time_limits": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint64, C.c_uint64]),
+    "hc_csr_check": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_int64, _P]),
+    "hc_selftest_grid_barrier": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "hc_epoch_sssp_pull": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, _P, C.c_int, C.c_int32, C.c_int32, _P]),
     "hc_epoch_pr_pull": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, _P, C.c_int32, _P, C.c_int, C.c_int32,
                                    C.c_int32, _P]),
@@ -188,6 +191,19 @@ def _ptr(x):
 def kernel_launches() -> int:
     """Kernels this process has launched through libhc so far."""
     return int(lib().hc_kernel_launches())
+
+
+def set_time_limits(device: int = 0, wait_ns: int = 0, run_ns: int = 0, loop_ns: int = 0):
+    """hc_set_time_limits: bounds of the device-side waits on `device` (0 = default: 2 s per barrier wait,
+    20 s per persistent run, 60 s per batched epoch loop)."""
+    _check(lib().hc_set_time_limits(device, wait_ns, run_ns, loop_ns), "hc_set_time_limits")
+
+
+def selftest_grid_barrier(device: int, blocks: int, withhold_block: int) -> int:
+    """hc_selftest_grid_barrier: the grid barrier's recorded status with one block held back (-1: none)."""
+    st = C.c_int32(-1)
+    _check(lib().hc_selftest_grid_barrier(device, blocks, withhold_block, C.byref(st)), "hc_selftest_grid_barrier")
+    return int(st.value)
 
 
 # ------------------------------------------------------------------ graphs

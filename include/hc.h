@@ -188,7 +188,12 @@ hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sources,
  * any stream capture).  All calls share the array: calls that overlap on the
  * GPU (other streams, other host threads) race and must not be issued.
  * Runs on `stream` (a cudaStream_t, NULL = legacy default) and returns after
- * the run has finished. */
+ * the run has finished.  Before the traversal a check pass (its flag also in
+ * the fixed array) refuses, with HC_ERR_INVALID_ARG, offsets that do not
+ * rise from 0 to num_edges and neighbour ids outside [0, num_nodes).  It
+ * uses Beamer's fixed alpha = 15 / beta = 18 and thread-per-vertex bottom-up
+ * levels over every vertex (no degree analysis, no tuned values), so it can
+ * be slower than hc_bfs on the same graph. */
 hc_status hc_bfs_noalloc(const int64_t *index, const int32_t *neighbors, int32_t num_nodes,
                          int64_t num_edges, int32_t source, int32_t *depth_out,
                          int32_t *parent_out, void *stream);
@@ -216,6 +221,12 @@ typedef struct hc_sssp_stats {
 
 /* Single-source shortest paths over int32 weights (graph wtype HC_W_I32).
  * dist_out: [num_sources][num_nodes] int32, INT32_MAX = unreachable.
+ * Distances are int32: when a path of num_active - 1 edges of the largest
+ * weight could pass INT32_MAX, each source's distances are checked after its
+ * run: a distance above INT32_MAX returns HC_ERR_UNSUPPORTED (one of exactly
+ * INT32_MAX reads as unreachable).  The reference's float distances lose
+ * integer exactness above 2^24 instead (src/kernels/gpu/sssp.cuh:120-281).
+ * hc_sssp_batched checks its 32-bit groups the same way.
  * parent_out (optional): a shortest-path tree, parent[src] = src.
  * Replaces sssp_pull_gpu (src/kernels/gpu/sssp.cuh:42-100). */
 hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_sources,
@@ -388,12 +399,42 @@ hc_status hc_device_synchronize(void);
 /* Kernels launched by this library in this process so far. */
 int64_t hc_kernel_launches(void);
 
+/* ------------------------------------------------------- time limits */
+/* No counterpart in the reference, whose host loops wait without a bound.
+ * Every device-side wait here is bounded: a grid barrier gives up after
+ * wait_ns (default 2 s), one persistent run after run_ns (20 s), one batched
+ * group's epoch loop after loop_ns (60 s); each then ends its call with
+ * HC_ERR_TIMEOUT and leaves the handle usable.  hc_set_time_limits replaces
+ * the three bounds on `device` for every later launch in this process
+ * (0 = the default); it exists so that tests can make each wait run out. */
+hc_status hc_set_time_limits(int32_t device, uint64_t wait_ns, uint64_t run_ns, uint64_t loop_ns);
+/* Runs the grid barrier alone on `device` with `blocks` (1..64) co-resident
+ * blocks, block `withhold_block` never arriving (-1: all arrive), and returns
+ * the barrier's recorded status in *status_out: HC_OK when all arrived,
+ * HC_ERR_TIMEOUT when the others gave up after the wait limit. */
+hc_status hc_selftest_grid_barrier(int32_t device, int32_t blocks, int32_t withhold_block,
+                                   int32_t *status_out);
+
 /* ------------------------------------------------ reference epoch kernels */
 /* One epoch of the reference's in-place pull kernels over [start_id, end_id),
  * device pointers only, launched on `stream` with the given shape and
  * granularity, adding to *updated (device int32).  These keep the epoch-kernel
  * contract of src/kernels/kernel_types.cuh:36-63 for callers that drive their
- * own epoch loop. */
+ * own epoch loop.  Like the reference's kernels they trust the CSR they are
+ * given (the contract carries no vertex or edge count to check against, and a
+ * per-epoch pass would double each epoch's traffic): check it once with
+ * hc_csr_check before the loop, as the reference-shaped drivers in
+ * hc_compat.hpp do. */
+
+/* Checks a CSR in device memory: offsets rising from index[0] == 0 to
+ * index[num_nodes] == num_edges and every neighbour id in [0, num_nodes);
+ * HC_ERR_INVALID_ARG otherwise.  `neighbors` holds num_edges int32 ids, or,
+ * with interleaved = 1, the reference's {int32 v; float w} wnode_t array
+ * (src/graph.cuh:37-41).  One pass on `stream`; returns when it is done.
+ * Replaces nothing in the reference, whose drivers upload without a check
+ * (src/kernels/gpu/sssp.cuh:51-61). */
+hc_status hc_csr_check(const int64_t *index, const void *neighbors, int32_t interleaved,
+                       int32_t num_nodes, int64_t num_edges, void *stream);
 
 /* sssp_gpu_epoch_func (src/kernels/kernel_types.cuh:36-37): wnodes is the
  * reference's interleaved {int32 v; float w} edge array. */

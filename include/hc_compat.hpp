@@ -265,6 +265,7 @@ inline double bfs_gpu(const CSRUWGraph &g, const nid_t source_id, nid_t **const 
             par(4 * (size_t)g.num_nodes), f0(4 * words), f1(4 * words), cnt(4);
         check(hc_memcpy(idx.p, g.index, 8 * ((size_t)g.num_nodes + 1)), "hc_memcpy");
         check(hc_memcpy(nbr.p, g.neighbors, 4 * (size_t)g.num_edges), "hc_memcpy");
+        check(hc_csr_check(idx.as<int64_t>(), nbr.p, 0, g.num_nodes, g.num_edges, nullptr), "hc_csr_check");
         for (nid_t i = 0; i < g.num_nodes; i++) parents[i] = INVALID_NODE;
         parents[source_id] = source_id;
         check(hc_memcpy(par.p, parents, 4 * (size_t)g.num_nodes), "hc_memcpy");
@@ -332,6 +333,7 @@ inline double sssp_pull_gpu(const CSRWGraph &g, sssp_gpu_epoch_func epoch_kernel
         check(hc_memcpy(idx.p, g.index, 8 * ((size_t)g.num_nodes + 1)), "hc_memcpy");
         check(hc_memcpy(nb.p, g.neighbors, 8 * (size_t)g.num_edges), "hc_memcpy");
         check(hc_memcpy(dd.p, init_dist, 4 * (size_t)g.num_nodes), "hc_memcpy");
+        check(hc_csr_check(idx.as<int64_t>(), nb.p, 1, g.num_nodes, g.num_edges, nullptr), "hc_csr_check");
         auto t0 = std::chrono::steady_clock::now();
         nid_t updated = 1;
         while (updated != 0) {
@@ -384,6 +386,7 @@ inline double pr_pull_gpu(const CSRWGraph &g, pr_gpu_epoch_func epoch_kernel, we
         check(hc_memcpy(nb.p, g.neighbors, 8 * (size_t)g.num_edges), "hc_memcpy");
         check(hc_memcpy(sc.p, init_score, 4 * (size_t)g.num_nodes), "hc_memcpy");
         check(hc_memcpy(dg.p, deg.data(), 8 * (size_t)g.num_nodes), "hc_memcpy");
+        check(hc_csr_check(idx.as<int64_t>(), nb.p, 1, g.num_nodes, g.num_edges, nullptr), "hc_csr_check");
         auto t0 = std::chrono::steady_clock::now();
         nid_t updated = 1;
         for (int it = 0; updated != 0 && it <= 200; it++) {
