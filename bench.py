@@ -10,7 +10,13 @@ edges (src/benchmarks/gpu_benchmark.cuh:259), value = runs * M/2 / time.
 
   python bench.py [--gpus N --steps K --warmup W]          this engine
   python bench.py --impl reference [...]                   the reference's own
-        OpenMP CPU code (oracle/_ref), host cores, bounded sample per step
+        OpenMP CPU code (oracle/_ref), host cores, the full workload per step
+
+After the timed steps (N = 1): the reference's CPU step (cpu_baseline) with
+parity checks of the GPU's outputs against the reference's (key "parity"),
+512 batched BFS / SSSP sources against 512 sequential plain launches (key
+"batched") and PageRank forward + adjoint against the forward (key
+"adjoint"), each with its own parity check.
 
 Under torchrun (N > 1) each rank holds a replica of the graph and runs its own
 64 sources (weak scaling, no data-path collective); time is the max over ranks.
@@ -47,10 +53,12 @@ def parse():
     p.add_argument("--edge-factor", type=int, default=16)
     p.add_argument("--sources", type=int, default=64)
     p.add_argument("--seed", type=int, default=1)
-    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true",
+                   help="skip the reference's CPU step and the parity checks against it")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the batched (512 sources) and adjoint sections of the default run")
     p.add_argument("--no-tune", dest="tune", action="store_false",
                    help="skip the (untimed) autotuner pass and use the built-in launch parameters")
-    p.add_argument("--cpu-budget-s", type=float, default=20.0)
     p.add_argument("--mode", choices=["bench", "profile"], default="bench",
                    help="profile: one BFS, one SSSP and one PageRank solve, untimed (for ncu captures)")
     p.add_argument("--suite", choices=["plain", "batched", "adjoint", "grid", "roofline", "large"], default="plain",
@@ -421,75 +429,218 @@ class ClockSampler:
 
 # ----------------------------------------------------------- CPU legs
 
-def reference_sample(host, a, budget_s: float, threads: int):
-    """Times the reference's own CPU code (oracle/_ref) on a bounded sample of the step; returns
-    (gteps_estimate, detail).  The step time is extrapolated from per-run means: 64 x BFS + 64 x SSSP + 1 PR."""
-    import hc
+def _ref_graph_files(tmp, index, nbr, weights, writer):
+    """.sg (BFS) and .wsg (SSSP, PageRank) files of the benchmark graph for the reference's loader."""
+    sg, wsg = os.path.join(tmp, "g.sg"), os.path.join(tmp, "g.wsg")
+    writer(sg, index, nbr, None)
+    writer(wsg, index, nbr, weights)
+    return sg, wsg
+
+
+def _ref_step_ms(sg, wsg, k, threads, repeats, warmup):
+    """The reference's own CPU code (oracle/_ref) on the step's workload: bfs_do_cpu and sssp_pull_cpu from
+    the first k SourcePicker sources, then pr_pull_cpu, `repeats` times with the graph loaded once per
+    algorithm; returns per-step milliseconds (sum of the reference drivers' own timings) and the raw runs."""
     import oracle
+    bfs = oracle.run_reference("bfs", sg, k, "-", threads=threads, repeats=repeats, warmup=warmup)
+    sssp = oracle.run_reference("sssp", wsg, k, "-", threads=threads, repeats=repeats, warmup=warmup)
+    pr = oracle.run_reference("pr", wsg, 0, "-", threads=threads, repeats=repeats, warmup=min(warmup, 1))
+    steps = []
+    for r in range(repeats):
+        steps.append(sum(bfs["ms"][r * k:(r + 1) * k]) + sum(sssp["ms"][r * k:(r + 1) * k]) + pr["ms"][r])
+    per_run = {"bfs_ms": float(np.mean(bfs["ms"])), "sssp_ms": float(np.mean(sssp["ms"])),
+               "pagerank_ms": float(np.mean(pr["ms"]))}
+    return steps, per_run, bfs["sources"]
+
+
+def cpu_leg(host, a, gpu):
+    """cpu_baseline: one full step of the reference's own OpenMP code (oracle/_ref) on all host cores, timed
+    by the reference's drivers, with nothing extrapolated.  The same leg checks the GPU's results against the
+    reference's outputs for the first sources (and the oracle, as the checker):
+      BFS   GPU depths == the oracle's serial BFS depths; GPU parents a valid BFS tree; the reference's
+            bfs_do_cpu parents a valid tree for the GPU's depths (tests/bfs/bfs_verify.cu:133-233 rules)
+      SSSP  GPU distances == the reference's sssp_pull_cpu distances, bit for bit (inf as INT32_MAX)
+      PR    the reference-order sweep (hc_pr_pull_ordered) == the reference's pr_pull_cpu on one thread, bit
+            for bit; the timed Jacobi PageRank's L-inf distance to the reference and to the FP64 fixed point
+    `gpu` holds host copies of the GPU outputs."""
+    import oracle
+    import hc
+    threads = os.cpu_count() or 1
     m = host.num_edges
     with tempfile.TemporaryDirectory() as tmp:
-        sg, wsg = os.path.join(tmp, "g.sg"), os.path.join(tmp, "g.wsg")
-        hc.write_graph(sg, hc.HostCSR(host.index, host.neighbors))
-        hc.write_graph(wsg, host)
-        if os.path.exists(oracle.REF_DRIVER):
-            kind = "reference"
-            t0 = time.time()
-            bfs = oracle.run_reference("bfs", sg, 4, "-", threads=threads)
-            left = budget_s - (time.time() - t0)
-            sssp = oracle.run_reference("sssp", wsg, 1, "-", threads=threads)
-            pr = oracle.run_reference("pr", wsg, 0, "-", threads=threads)
-            t_bfs = float(np.mean(bfs["ms"])) / 1e3
-            t_sssp = float(np.mean(sssp["ms"])) / 1e3
-            t_pr = float(pr["ms"][0]) / 1e3
-            sample = (f"reference bfs_do_cpu x{len(bfs['ms'])}, sssp_pull_cpu x{len(sssp['ms'])}, "
-                      f"pr_pull_cpu x1 on {threads} OpenMP threads; step = 64 bfs + 64 sssp + 1 pr "
-                      f"extrapolated from per-run means")
-            del left
-        else:
-            kind = "port"
-            src = hc.pick_sources(host, 2)
-            t0 = time.time()
-            oracle.bfs_depth(host.index, host.neighbors, src[0])
-            t_bfs = time.time() - t0
-            t0 = time.time()
-            oracle.sssp_dijkstra(host.index, host.neighbors, host.weights, src[0])
-            t_sssp = time.time() - t0
-            t0 = time.time()
-            oracle.pr_pull(host.index, host.neighbors, max_iters=5)
-            t_pr = (time.time() - t0) * 10
-            threads = 1
-            sample = "oracle port (1 thread): bfs x1, dijkstra x1, pagerank 5 sweeps scaled to 50"
-    runs = 2 * a.sources + 1
-    t_step = a.sources * t_bfs + a.sources * t_sssp + t_pr
-    gteps = runs * (m / 2) / t_step / 1e9
-    return gteps, {"kind": kind, "cores": threads, "sample": sample,
-                   "per_run_s": {"bfs": t_bfs, "sssp": t_sssp, "pagerank": t_pr}}
+        sg, wsg = _ref_graph_files(tmp, host.index, host.neighbors, host.weights,
+                                   lambda p, i, n, w: hc.write_graph(p, hc.HostCSR(i, n, w)))
+        if not os.path.exists(oracle.REF_DRIVER):
+            return ({"value": None, "unit": "GTEPS", "cores": None, "kind": "unavailable",
+                     "sample": "the reference's CPU code was not built (oracle/_ref absent)"}, None)
+        steps, per_run, _ = _ref_step_ms(sg, wsg, a.sources, threads, 1, 1)
+        runs = 2 * a.sources + 1
+        cpu = {"value": runs * (m / 2) / (steps[0] / 1e3) / 1e9, "unit": "GTEPS", "cores": threads,
+               "kind": "reference",
+               "sample": f"one full step (bfs_do_cpu x{a.sources} + sssp_pull_cpu x{a.sources} + pr_pull_cpu x1) "
+                         f"on {threads} OpenMP threads, {steps[0]:.0f} ms by the reference's own timers",
+               "per_run_ms": per_run}
+        # Parity on the first sources, against the reference's own outputs.
+        kp = min(4, a.sources)
+        par = {}
+        out = os.path.join(tmp, "out.bin")
+        n = host.num_nodes
+        ref = oracle.run_reference("bfs", sg, kp, out, threads=threads)
+        ref_par = np.fromfile(out, dtype=np.int32).reshape(kp, n)
+        ok = list(ref["sources"]) == list(gpu["sources"])  # both sides drew the same SourcePicker sources
+        for i, s in enumerate(ref["sources"]):
+            d = oracle.bfs_depth(host.index, host.neighbors, s)
+            ok &= bool(np.array_equal(gpu["depth"][i], d))
+            ok &= oracle.verify_bfs_parents(host.index, host.neighbors, d, gpu["parent"][i], s)[0] == 0
+            ok &= oracle.verify_bfs_parents(host.index, host.neighbors, d, ref_par[i], s)[0] == 0
+        par["bfs"] = {"sources": kp, "ok": bool(ok),
+                      "check": "depths == serial BFS; GPU parents and the reference's bfs_do_cpu parents valid trees"}
+        ref = oracle.run_reference("sssp", wsg, kp, out, threads=threads)
+        ref_d = np.fromfile(out, dtype=np.float32).reshape(kp, n)
+        want = np.where(np.isinf(ref_d), 0x7FFFFFFF, ref_d).astype(np.int64)
+        ok = bool(np.array_equal(gpu["dist"][:kp].astype(np.int64), want))
+        par["sssp"] = {"sources": kp, "ok": ok, "check": "bit-exact vs the reference's sssp_pull_cpu"}
+        ref = oracle.run_reference("pr", wsg, 0, out, threads=1)
+        ref_pr = np.fromfile(out, dtype=np.float32)
+        ordered = gpu["pr_ordered"]
+        par["pagerank_reference_order"] = {
+            "ok": bool(np.array_equal(ordered.view(np.uint32), ref_pr.view(np.uint32))),
+            "sweeps": gpu["pr_ordered_sweeps"],
+            "check": "hc_pr_pull_ordered bit-exact vs the reference's pr_pull_cpu on one thread"}
+        x64, it64 = oracle.pr_jacobi_f64(host.index, host.neighbors, tol=1e-11, max_iters=1000)
+        s = gpu["pr"]
+        e_ref, e_64, r_64 = (float(np.abs(s - ref_pr).max()), float(np.abs(s - x64).max()),
+                             float(np.abs(ref_pr - x64).max()))
+        par["pagerank"] = {"ok": e_64 <= 1e-5, "gpu_vs_reference_linf": e_ref, "gpu_vs_fp64_linf": e_64,
+                           "reference_vs_fp64_linf": r_64, "max_score": float(x64.max()),
+                           "check": "timed Jacobi PageRank (L1 tol 1e-4) within 1e-5 of the FP64 fixed point; its "
+                                    "distance to the reference is the reference's own stopping error (its "
+                                    "per-vertex 5e-8 rule)"}
+    return cpu, par
 
 
 def run_reference_arm(a):
-    import hc
+    """--impl reference: the reference's own OpenMP CPU code (oracle/_ref) on all host cores, on the same
+    workload and config as the GPU arm.  Every timed step is a full step (64 bfs_do_cpu + 64 sssp_pull_cpu
+    + 1 pr_pull_cpu) timed by the reference's own drivers; the graph is built by the numpy restatement of
+    the generator (oracle/gen.py, bit-identical to the library's) and written as the .sg/.wsg files the
+    reference loads, so no part of this project's library is loaded in this process."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    host = hc.gen_kronecker(a.scale, a.edge_factor, a.seed, hc.W_I32)
+    from oracle import gen
+    import oracle
+    t0 = time.time()
+    index, nbr, w = gen.build("kronecker", a.scale, a.edge_factor, a.seed, gen.W_I32)
+    gen_s = time.time() - t0
+    n, m = len(index) - 1, len(nbr)
     threads = os.cpu_count() or 1
-    vals = []
-    detail = None
-    for i in range(a.warmup + a.steps):
-        v, detail = reference_sample(host, a, a.cpu_budget_s, threads)
-        if i >= a.warmup:
-            vals.append(v)
-    value = float(np.mean(vals))
-    ms_step = (2 * a.sources + 1) * (host.num_edges / 2) / (value * 1e9) * 1e3
+    if not os.path.exists(oracle.REF_DRIVER):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's CPU code was not built here "
+                                                              "(oracle/_ref/ref_driver absent)"}))
+        return
+    t1 = time.time()
+    with tempfile.TemporaryDirectory() as tmp:
+        sg, wsg = _ref_graph_files(tmp, index, nbr, w, gen.write_graph)
+        del index, nbr, w
+        # Warm-up: one run per algorithm from the first source (the CPU needs no more); then K full steps.
+        steps, per_run, _ = _ref_step_ms(sg, wsg, a.sources, threads, a.steps, max(1, a.warmup))
+    wall = time.time() - t1
+    total = float(np.sum(steps))
+    runs = 2 * a.sources + 1
+    value = a.steps * runs * (m / 2) / (total / 1e3) / 1e9
+    sample = (f"every step the full workload: bfs_do_cpu x{a.sources} + sssp_pull_cpu x{a.sources} + "
+              f"pr_pull_cpu x1 on {threads} OpenMP threads, timed by the reference's drivers; warm-up: "
+              f"{max(1, a.warmup)} run(s) of each from the first source")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": a.gpus,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": total / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32", "data": "synthetic",
-        "config": workload(a),
-        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": detail["cores"], "kind": detail["kind"],
-                         "sample": detail["sample"]},
+        "config": workload(a) | {"num_nodes": n, "num_edges": m, "parallelism": f"replicas x{a.gpus}"},
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "detail": detail}))
+        "detail": {"per_run_ms": per_run, "step_ms": steps, "graph_gen_s": gen_s, "timed_wall_s": wall,
+                   "graph": "oracle/gen.py (numpy restatement; bit-identical to the library's generator)"}}))
+
+
+# ----------------------------------------------------------- extra sections
+
+def batched_section(g, host, a, torch, dev, stream, k=512):
+    """Batched multi-source BFS and SSSP (one launch sequence for all sources of a group) against k
+    sequential plain launches, on the benchmark graph; parity: every batched row equals the plain run's
+    (the plain path itself is checked against the reference in the CPU leg and the tests)."""
+    import hc
+    n, m = host.num_nodes, host.num_edges
+    src = hc.pick_sources(host, k)
+    out = {"sources": k}
+    if a.tune:  # untimed: group widths and switch points for both batched paths
+        out["tuning"] = g.autotune(src, hc.TUNE_BFS_BATCHED | hc.TUNE_SSSP_BATCHED)
+    seq = torch.empty((k, n), dtype=torch.int32, device=dev)
+    bat = torch.empty((k, n), dtype=torch.int32, device=dev)
+    par1 = torch.empty((1, n), dtype=torch.int32, device=dev)
+    for name, run_b, run_p in [
+            ("bfs", lambda: g.bfs_batched(src, bat), lambda i: g.bfs(src[i:i + 1], seq[i:i + 1], par1)),
+            ("sssp", lambda: g.sssp_batched(src, bat), lambda i: g.sssp(src[i:i + 1], seq[i:i + 1]))]:
+        run_b()  # warm-up: workspaces and plans sized once
+        run_p(0)
+        tb = min(_time_cuda(run_b, torch, dev, 1) for _ in range(2))
+        tp = _time_cuda(lambda: [run_p(i) for i in range(k)], torch, dev, 1)
+        out[name] = {"batched_ms": tb, "sequential_ms": tp, "speedup": tp / tb,
+                     "batched_gteps": k * (m / 2) / tb / 1e6, "sequential_gteps": k * (m / 2) / tp / 1e6,
+                     "parity": bool(torch.equal(bat, seq))}
+    del seq, bat
+    torch.cuda.empty_cache()
+    out["ok"] = out["bfs"]["parity"] and out["sssp"]["parity"]
+    out["config"] = (f"kronecker-s{a.scale}-ef{a.edge_factor}: {k} BFS and {k} SSSP sources batched vs {k} "
+                     f"sequential plain launches (device outputs [{k}][N] int32)")
+    return out
+
+
+def adjoint_section(g, host, a, torch, dev):
+    """PageRank forward + hand-written adjoint against the forward alone (weighted: the int32 weights as
+    fp32, row-normalised; L = c . x with seeded Gaussian c; L1 tolerance 1e-6 forward, 1e-6 relative
+    adjoint).  Parity at full size through two exact identities:
+      linearity        x is linear in the teleport t, so c . x = (dL/dt) . t
+      row scaling      A does not change when one row's weights are scaled, so sum_k w_uk dL/dw_uk = 0
+                       for every row u"""
+    n, m = host.num_nodes, host.num_edges
+    rng = np.random.default_rng(a.seed)
+    c = torch.from_numpy(rng.standard_normal(n).astype(np.float32)).to(dev)
+    x = torch.empty(n, dtype=torch.float32, device=dev)
+    dt = torch.empty(n, dtype=torch.float32, device=dev)
+    dw = torch.empty(m, dtype=torch.float32, device=dev)
+    opts = dict(tol_l1=1e-6, max_iters=200, weighted=True)
+
+    def fwd():
+        return g.pagerank(None, x, **opts)
+
+    def bwd():
+        return g.pagerank_backward(x, c, dteleport=dt, dweights=dw, **opts)
+    fwd()
+    bwd()  # warm-up: fp32 weights, transposed weights, symmetry check, workspaces
+    tf = min(_time_cuda(fwd, torch, dev, 1) for _ in range(3))
+    tfb = min(_time_cuda(lambda: (fwd(), bwd()), torch, dev, 1) for _ in range(3))
+    _, fst = fwd()
+    _, _, bst = bwd()
+    x64, c64 = x.double(), c.double()
+    lhs = float((c64 * x64).sum())
+    rhs = float(dt.double().sum() / n)  # t = 1/N everywhere
+    lin = abs(lhs - rhs) / float((c64 * x64).abs().sum())
+    deg = torch.from_numpy(np.diff(host.index)).to(dev)
+    rows = torch.repeat_interleave(torch.arange(n, device=dev), deg)
+    w = torch.from_numpy(host.weights.astype(np.float32)).to(dev).double()
+    wg = w * dw.double()
+    row_sum = torch.zeros(n, dtype=torch.float64, device=dev).index_add_(0, rows, wg)
+    row_abs = torch.zeros(n, dtype=torch.float64, device=dev).index_add_(0, rows, wg.abs())
+    scale_inv = float(row_sum.abs().max() / row_abs.max())
+    del rows, w, wg, row_sum, row_abs, dw
+    torch.cuda.empty_cache()
+    return {"forward_ms": tf, "forward_adjoint_ms": tfb, "ratio": tfb / tf,
+            "forward_iterations": int(fst.iterations), "adjoint_iterations": int(bst.iterations),
+            "parity": {"linearity_rel_err": lin, "row_scaling_rel_err": scale_inv,
+                       "ok": lin <= 1e-4 and scale_inv <= 1e-4, "tolerance": 1e-4},
+            "config": f"kronecker-s{a.scale}-ef{a.edge_factor}: weighted PageRank (int32 weights as fp32, "
+                      f"row-normalised), L = c.x, c ~ N(0,1) seed {a.seed}; tol 1e-6"}
 
 
 # ----------------------------------------------------------- GPU arm
@@ -649,13 +800,34 @@ def main():
                             "(profiles/traffic.json)" if traffic else None,
             "bytes_model_per_unit": per_algo[dom]["bytes_model"] / (k if dom != "pagerank" else 1)}
 
+    # The GPU's outputs for the parity checks: what the last end-to-end step returned to host memory
+    # (parents, distances, scores) and the timed steps' depths, for the first sources; and the
+    # reference-order PageRank (untimed).
+    extras = {}
     cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        try:
-            v, d = reference_sample(host, a, a.cpu_budget_s, os.cpu_count() or 1)
-            cpu = {"value": v, "unit": "GTEPS", "cores": d["cores"], "kind": d["kind"], "sample": d["sample"]}
-        except Exception as ex:  # reported, not fatal
-            cpu = {"value": None, "unit": "GTEPS", "cores": None, "kind": "unavailable", "sample": str(ex)}
+    parity = None
+    if rank == 0 and world == 1:
+        kp = min(4, k)
+        ordered, ost = g.pagerank_ordered()
+        gpu_out = {"sources": src[:kp].tolist(), "depth": depth[:kp].cpu().numpy(), "parent": h_parent[:kp].copy(),
+                   "dist": h_dist[:kp].copy(), "pr": h_scores.copy(), "pr_ordered": ordered,
+                   "pr_ordered_sweeps": int(ost.iterations), "pr_ordered_ms": ost.ms}
+        del depth, parent, dist_o, flush
+        torch.cuda.empty_cache()
+        if not a.no_extras:
+            extras["batched"] = batched_section(g, host, a, torch, dev, stream)
+            extras["adjoint"] = adjoint_section(g, host, a, torch, dev)
+        if not a.no_cpu_baseline:
+            try:
+                cpu, parity = cpu_leg(host, a, gpu_out)
+            except Exception as ex:  # reported, not fatal
+                cpu = {"value": None, "unit": "GTEPS", "cores": None, "kind": "unavailable", "sample": repr(ex)}
+        if parity is not None:
+            parity["pagerank_reference_order"]["ms"] = gpu_out["pr_ordered_ms"]
+            for key in ("batched", "adjoint"):
+                if key in extras:
+                    parity[key] = {"ok": extras[key]["ok"] if key == "batched" else extras[key]["parity"]["ok"]}
+            parity["ok"] = all(v["ok"] for v in parity.values() if isinstance(v, dict))
 
     if rank == 0:
         print(json.dumps({
@@ -668,8 +840,8 @@ def main():
                     "d2h_bytes_per_step": int(2 * k * n * 4 + n * 4),
                     "host_cpus": (f"{len(near)} of {len(saved_cpus)}, the GPU's NUMA node" if near
                                   else f"all {len(saved_cpus)}")},
-            "gpu_launches": launches, "clocks": clk.summary(), "per_algo": per_algo, "tuning": tuning,
-            "graph_gen_s": gen_s}), flush=True)
+            "gpu_launches": launches, "clocks": clk.summary(), "parity": parity, "per_algo": per_algo,
+            **extras, "tuning": tuning, "graph_gen_s": gen_s}), flush=True)
     g.close()
     if world > 1:
         dist.destroy_process_group()

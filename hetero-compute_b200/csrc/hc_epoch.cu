@@ -39,6 +39,10 @@ __device__ __forceinline__ T block_reduce_min_or_sum(T v, T *sm, bool is_min) {
 }
 
 __device__ __forceinline__ void add_count(int32_t *counter, int c) {
+    if (blockDim.x & 31) {  // thread-variant blocks need not fill whole warps
+        if (c) atomicAdd(counter, c);
+        return;
+    }
     c = warp_sum(c);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(counter, c);
 }
@@ -100,10 +104,14 @@ __global__ void sssp_epoch_block(const int64_t *index, const WNode *nb, int32_t 
 }
 
 // ------------------------------------------------------------------ PR
+// The thread variant does the reference CPU epoch's fp32 operations one by
+// one (src/kernels/cpu/pr.cuh:157-187: divide, add in row order, multiply,
+// add; no multiply-add contraction), so a one-thread launch over [0, N)
+// sweeps in the single-thread CPU order and reproduces pr_pull_cpu bit for bit.
 __global__ void pr_epoch_thread(const int64_t *index, const WNode *nb, int32_t s, int32_t e, float *score,
                                 int32_t *updated, int32_t n, const int64_t *deg) {
     int c = 0;
-    const float base = (1.0f - kDamp) / n;
+    const float base = __fdiv_rn(__fsub_rn(1.0f, kDamp), __int2float_rn(n));
     const int stride = gridDim.x * blockDim.x;
     const int32_t span = (e - s + stride - 1) / stride * stride;
     for (int32_t v = s + blockIdx.x * blockDim.x + threadIdx.x; v < s + span; v += stride) {
@@ -112,10 +120,10 @@ __global__ void pr_epoch_thread(const int64_t *index, const WNode *nb, int32_t s
             const int64_t b = index[v - s], en = index[v - s + 1];
             for (int64_t i = b; i < en; i++) {
                 const int32_t u = nb[i].v;
-                t += score[u] / (float)deg[u];
+                t = __fadd_rn(t, __fdiv_rn(score[u], __ll2float_rn(deg[u])));
             }
-            const float ns = base + kDamp * t;
-            if (fabsf(ns - score[v]) > kPrEps) {
+            const float ns = __fadd_rn(base, __fmul_rn(kDamp, t));
+            if (fabsf(__fsub_rn(ns, score[v])) > kPrEps) {
                 score[v] = ns;
                 c++;
             }
@@ -228,7 +236,6 @@ hc_status check_shape(int32_t blocks, int32_t threads, hc_variant v) {
     // Same rule as the reference drivers (src/kernels/gpu/sssp.cuh:47-49).
     if (v != HC_VARIANT_THREAD && threads % 32 != 0)
         return fail(HC_ERR_INVALID_ARG, "thread count must be divisible by 32");
-    if (threads % 32 != 0) return fail(HC_ERR_INVALID_ARG, "thread count must be a multiple of 32 (warp collectives)");
     return HC_OK;
 }
 

@@ -145,12 +145,14 @@ def pr_dense_grad(index, nbr, c, w=None, teleport=None, damping=0.85):
     return x, dt, dw
 
 
-def run_reference(algo, graph_path, nsrc, out_path, threads=None, timeout=None):
-    """Runs the reference's own CPU code (oracle/_ref/ref_driver); returns its JSON line as a dict."""
+def run_reference(algo, graph_path, nsrc, out_path, threads=None, timeout=None, repeats=1, warmup=0):
+    """Runs the reference's own CPU code (oracle/_ref/ref_driver); returns its JSON line as a dict.
+    repeats: the source sequence runs that many times in one process (per-run ms for each); warmup: untimed
+    runs from the first source before them."""
     import json
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
-    r = subprocess.run([REF_DRIVER, algo, graph_path, str(nsrc), out_path], capture_output=True, text=True,
-                       env=env, check=True, timeout=timeout)
+    r = subprocess.run([REF_DRIVER, algo, graph_path, str(nsrc), out_path, str(repeats), str(warmup)],
+                       capture_output=True, text=True, env=env, check=True, timeout=timeout)
     return json.loads(r.stdout.strip().splitlines()[-1])

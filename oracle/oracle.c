@@ -195,6 +195,7 @@ int32_t or_pr_jacobi_f64(const int64_t *index, const int32_t *nbr, const float *
     double *y = (double *)malloc(sizeof(double) * (size_t)n);
     double *inv = (double *)malloc(sizeof(double) * (size_t)n);
     if (!y || !inv) { free(y); free(inv); return -1; }
+#pragma omp parallel for schedule(static)
     for (int32_t u = 0; u < n; u++) {
         double s = 0.0;
         for (int64_t e = index[u]; e < index[u + 1]; e++) s += w ? (double)w[e] : 1.0;
@@ -204,6 +205,9 @@ int32_t or_pr_jacobi_f64(const int64_t *index, const int32_t *nbr, const float *
     int32_t it = 0;
     for (; it < max_iters; it++) {
         double l1 = 0.0;
+        /* Each y[v] is one thread's sequential row sum, so x does not depend
+         * on the thread count; only the L1 total's rounding does. */
+#pragma omp parallel for schedule(dynamic, 4096) reduction(+ : l1)
         for (int32_t v = 0; v < n; v++) {
             double acc = 0.0;
             for (int64_t e = index[v]; e < index[v + 1]; e++) {

@@ -1,5 +1,5 @@
-"""Graphs built on the device (hc_graph_generate) equal the host generator's CSR bit for bit, and the
-device source picker draws the host picker's sources."""
+"""Graphs built on the device (hc_graph_generate) equal the host generator's CSR and the numpy
+restatement's (oracle/gen.py) bit for bit, and the device source picker draws the host picker's sources."""
 import hashlib
 
 import numpy as np
@@ -32,6 +32,20 @@ def test_device_build_equals_host_build(kind, scale, ef, wtype):
     assert np.array_equal(g.pick_sources(16), hc.pick_sources(host, 16))
     info = g.info()
     assert info.degree_sorted == 1
+
+
+@pytest.mark.parametrize("kind,scale,ef,seed,wtype", [
+    (hc.GEN_KRONECKER, 13, 16, 5, hc.W_I32), (hc.GEN_UNIFORM, 13, 8, 6, hc.W_F32),
+    (hc.GEN_KRONECKER, 20, 16, 1, hc.W_I32)])
+def test_device_build_equals_numpy_restatement(kind, scale, ef, seed, wtype):
+    """The device builder against the independent numpy restatement of the construction (oracle/gen.py),
+    up to scale 20 (33 M directed edges)."""
+    from oracle import gen
+    idx, nbr, w = gen.build("kronecker" if kind == hc.GEN_KRONECKER else "uniform", scale, ef, seed, wtype)
+    g = hc.Graph.generate(kind, scale, ef, seed, wtype)
+    index, neighbors, weights = g.csr()
+    assert np.array_equal(index, idx) and np.array_equal(neighbors, nbr)
+    assert np.array_equal(weights.view(np.uint32), np.asarray(w).view(np.uint32))
 
 
 def test_device_build_repeatable_and_usable():
