@@ -230,6 +230,47 @@ __global__ void bfs_epoch_warp(const int64_t *index, const int32_t *nbr, int32_t
     if (lane == 0 && c) atomicAdd(count, c);
 }
 
+// The sync-warp variant (src/kernels/gpu/bfs.cuh:234-288): the warp probes
+// sync_iters 32-edge chunks of the row before it votes, trading wasted probes
+// for fewer votes.  The parent taken is the first frontier neighbour in row
+// order among the probed chunks.
+__global__ void bfs_epoch_sync_warp(const int64_t *index, const int32_t *nbr, int32_t *parents, int32_t s, int32_t e,
+                                    const uint32_t *frontier, uint32_t *next, int32_t *count, int sync_iters) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    int c = 0;
+    for (int32_t v = s + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); v < e; v += nw) {
+        if (parents[v] != -1) continue;
+        const int64_t b = index[v - s], en = index[v - s + 1];
+        const int64_t chunks = (en - b + 31) / 32;
+        for (int64_t c0 = 0; c0 < chunks; c0 += sync_iters) {
+            int first = 0x7fffffff;  // (chunk within the group) * 32 + lane of this lane's first hit
+            int32_t hit = 0;
+            for (int k = 0; k < sync_iters && first == 0x7fffffff; k++) {
+                const int64_t i = b + (c0 + k) * 32 + lane;
+                if (i < en) {
+                    const int32_t u = nbr[i];
+                    if (in_frontier(frontier, u)) {
+                        first = k * 32 + lane;
+                        hit = u;
+                    }
+                }
+            }
+            const int best = warp_min(first);
+            if (best != 0x7fffffff) {
+                const int32_t p = __shfl_sync(kFull, hit, best & 31);
+                if (lane == 0) {
+                    parents[v] = p;
+                    atomicOr(next + (v >> 5), 1u << (v & 31));
+                    c++;
+                }
+                break;
+            }
+        }
+    }
+    if (lane == 0 && c) atomicAdd(count, c);
+}
+
 hc_status check_shape(int32_t blocks, int32_t threads, hc_variant v) {
     if (blocks < 1 || threads < 1 || threads > 1024)
         return fail(HC_ERR_INVALID_ARG, "epoch launch shape %d x %d is invalid", blocks, threads);
@@ -314,6 +355,22 @@ hc_status hc_epoch_bfs_pull(const int64_t *index, const int32_t *neighbors, int3
     else
         { bfs_epoch_warp<<<block_count, thread_count, 0, s>>>(index, neighbors, parents, start_id, end_id, frontier,
                                                             next_frontier, num_nodes); ::hc::count_launch(); }
+    HC_CUDA_TRY(cudaGetLastError());
+    return HC_OK;
+}
+
+hc_status hc_epoch_bfs_sync_pull(const int64_t *index, const int32_t *neighbors, int32_t *parents, int32_t start_id,
+                                 int32_t end_id, const uint32_t *frontier, uint32_t *next_frontier, int32_t *num_nodes,
+                                 int32_t sync_iters, int32_t block_count, int32_t thread_count, void *stream) {
+    clear_error();
+    if (!index || !parents || !frontier || !next_frontier || !num_nodes || start_id > end_id || start_id < 0 ||
+        sync_iters < 1)
+        return fail(HC_ERR_INVALID_ARG, "hc_epoch_bfs_sync_pull: bad arguments");
+    HC_TRY(check_shape(block_count, thread_count, HC_VARIANT_WARP));
+    if (start_id == end_id) return HC_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    { bfs_epoch_sync_warp<<<block_count, thread_count, 0, s>>>(index, neighbors, parents, start_id, end_id, frontier,
+                                                             next_frontier, num_nodes, sync_iters); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     return HC_OK;
 }

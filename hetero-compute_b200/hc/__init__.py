@@ -149,6 +149,8 @@ _SIGS = {
                                    C.c_int32, _P]),
     "hc_epoch_bfs_pull": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, _P, _P, _P, C.c_int, C.c_int32, C.c_int32,
                                     _P]),
+    "hc_epoch_bfs_sync_pull": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32, C.c_int32,
+                                         C.c_int32, _P]),
 }
 
 _lib = None

@@ -426,6 +426,16 @@ hc_status hc_selftest_grid_barrier(int32_t device, int32_t blocks, int32_t withh
  * hc_csr_check before the loop, as the reference-shaped drivers in
  * hc_compat.hpp do. */
 
+/* epoch_bfs_sync_pull_gpu_warp<sync_iters> (src/kernels/gpu/bfs.cuh:234-288):
+ * the warp-per-vertex bottom-up epoch that probes sync_iters (>= 1) 32-edge
+ * chunks of a row before the warp votes.  Same arguments as hc_epoch_bfs_pull;
+ * thread_count a multiple of 32. */
+hc_status hc_epoch_bfs_sync_pull(const int64_t *index, const int32_t *neighbors,
+                                 int32_t *parents, int32_t start_id, int32_t end_id,
+                                 const uint32_t *frontier, uint32_t *next_frontier,
+                                 int32_t *num_nodes, int32_t sync_iters,
+                                 int32_t block_count, int32_t thread_count, void *stream);
+
 /* Checks a CSR in device memory: offsets rising from index[0] == 0 to
  * index[num_nodes] == num_edges and every neighbour id in [0, num_nodes);
  * HC_ERR_INVALID_ARG otherwise.  `neighbors` holds num_edges int32 ids, or,

@@ -149,6 +149,7 @@ struct hc_epoch_kernel {
     hc_variant variant;
     bool engine;  // true: this library's device-driven path
     const char *name;
+    int sync_iters;  // > 0: the sync-warp BFS epoch probing that many chunks per vote
 };
 using bfs_gpu_epoch_func = const hc_epoch_kernel *;
 using sssp_gpu_epoch_func = const hc_epoch_kernel *;
@@ -169,7 +170,12 @@ inline const hc_epoch_kernel hc_k_pr_auto[] = {{HC_VARIANT_AUTO, true, "pr_gpu_a
 // Reference kernel names (src/kernels/gpu/*.cuh).
 inline const bfs_gpu_epoch_func epoch_bfs_pull_gpu_one_to_one = hc_k_bfs_one;
 inline const bfs_gpu_epoch_func epoch_bfs_pull_gpu_warp = hc_k_bfs_warp;
-inline const bfs_gpu_epoch_func epoch_bfs_sync_pull_gpu_warp = hc_k_bfs_warp;
+// epoch_bfs_sync_pull_gpu_warp<sync_iters> (src/kernels/gpu/bfs.cuh:234-288),
+// spelled as the reference's callers spell it (`epoch_bfs_sync_pull_gpu_warp<2>`).
+template <offset_t sync_iters = 1>
+inline const hc_epoch_kernel hc_k_bfs_sync[] = {{HC_VARIANT_WARP, false, "bfs_gpu_sync_warp", (int)sync_iters}};
+template <offset_t sync_iters = 1>
+inline const bfs_gpu_epoch_func epoch_bfs_sync_pull_gpu_warp = hc_k_bfs_sync<sync_iters>;
 inline const bfs_gpu_epoch_func epoch_bfs_auto = hc_k_bfs_auto;
 inline const sssp_gpu_epoch_func epoch_sssp_pull_gpu_one_to_one = hc_k_sssp_one;
 inline const sssp_gpu_epoch_func epoch_sssp_pull_gpu_warp_red = hc_k_sssp_warp;
@@ -278,9 +284,16 @@ inline double bfs_gpu(const CSRUWGraph &g, const nid_t source_id, nid_t **const 
         do {
             check(hc_dev_memset(cnt.p, 0, 4), "hc_dev_memset");
             check(hc_dev_memset(next, 0, 4 * words), "hc_dev_memset");
-            check(hc_epoch_bfs_pull(idx.as<int64_t>(), nbr.as<int32_t>(), par.as<int32_t>(), 0, g.num_nodes, cur, next,
-                                    cnt.as<int32_t>(), epoch_kernel->variant, block_count, thread_count, nullptr),
-                  "hc_epoch_bfs_pull");
+            if (epoch_kernel->sync_iters > 0)
+                check(hc_epoch_bfs_sync_pull(idx.as<int64_t>(), nbr.as<int32_t>(), par.as<int32_t>(), 0, g.num_nodes,
+                                             cur, next, cnt.as<int32_t>(), epoch_kernel->sync_iters, block_count,
+                                             thread_count, nullptr),
+                      "hc_epoch_bfs_sync_pull");
+            else
+                check(hc_epoch_bfs_pull(idx.as<int64_t>(), nbr.as<int32_t>(), par.as<int32_t>(), 0, g.num_nodes, cur,
+                                        next, cnt.as<int32_t>(), epoch_kernel->variant, block_count, thread_count,
+                                        nullptr),
+                      "hc_epoch_bfs_pull");
             check(hc_memcpy(&found, cnt.p, 4), "hc_memcpy");
             std::swap(cur, next);
         } while (found != 0);

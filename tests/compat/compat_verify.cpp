@@ -90,18 +90,23 @@ int main(int argc, char *argv[]) {
         SourcePicker<CSRUWGraph> sp(&g);
         nid_t source_id = sp.next_vertex();
         std::vector<nid_t> depth = serial_depth(g, source_id);
-        for (BFSGPU k : get_kernels(BFSGPU::undefined)) {
+        auto check_bfs = [&](const std::string &name, bfs_gpu_epoch_func kernel) {
             nid_t *parents = nullptr;
-            bfs_gpu(g, source_id, &parents, get_kernel(k));
+            bfs_gpu(g, source_id, &parents, kernel);
             nid_t bad = 0;
             for (nid_t u = 0; u < g.num_nodes; u++) {
                 if (parents[u] == INVALID_NODE) bad += depth[u] != INVALID_NODE;
                 else if (u == source_id) bad += parents[u] != source_id;
                 else bad += depth[u] != depth[parents[u]] + 1;
             }
-            report(to_string(k), bad == 0, std::to_string(bad) + " bad parents");
+            report(name, bad == 0, std::to_string(bad) + " bad parents");
             delete[] parents;
-        }
+        };
+        for (BFSGPU k : get_kernels(BFSGPU::undefined)) check_bfs(to_string(k), get_kernel(k));
+        // The sync-warp kernel as profile/bfs/benchmark_bfs.cu:242-260 names it.
+        check_bfs("GPU sync warp (sync_iters = 1)", epoch_bfs_sync_pull_gpu_warp<1>);
+        check_bfs("GPU sync warp (sync_iters = 2)", epoch_bfs_sync_pull_gpu_warp<2>);
+        check_bfs("GPU sync warp (sync_iters = 3)", epoch_bfs_sync_pull_gpu_warp<3>);
     }
     {
         CSRWGraph g = load_graph_from_file<CSRWGraph>(argv[2]);

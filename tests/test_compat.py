@@ -33,4 +33,4 @@ def test_compat_drivers_verify(tmp_path):
     r = subprocess.run([exe, sg, wsg], capture_output=True, text=True, timeout=600)
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count("success") == 3 + 4 + 4
+    assert r.stdout.count("success") == 3 + 3 + 4 + 4

@@ -128,6 +128,35 @@ def test_epoch_bfs_pull(golden, variant):
         assert oracle.verify_bfs_parents(host.index, host.neighbors, d, par.cpu().numpy(), s)[0] == 0
 
 
+@pytest.mark.parametrize("sync_iters", [1, 2, 3])
+def test_epoch_bfs_sync_pull(golden, sync_iters):
+    """epoch_bfs_sync_pull_gpu_warp<sync_iters> (src/kernels/gpu/bfs.cuh:234-288): valid BFS parents."""
+    rec, arr = golden["kron12_ef8"]
+    from conftest import make_graph
+    host = make_graph(rec)
+    n = host.num_nodes
+    words = (n + 31) // 32
+    idx = torch.from_numpy(host.index).cuda()
+    nbr = torch.from_numpy(host.neighbors).cuda()
+    for s in rec["bfs_sources"][:3]:
+        par = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+        par[s] = s
+        f = [torch.zeros(words, dtype=torch.int32, device="cuda") for _ in range(2)]
+        f[0][s // 32] = np.int32(np.uint32(1 << (s % 32)).view(np.int32))
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        cur = 0
+        while True:
+            cnt.zero_()
+            f[1 - cur].zero_()
+            _call(hc.lib().hc_epoch_bfs_sync_pull, idx.data_ptr(), nbr.data_ptr(), par.data_ptr(), 0, n,
+                  f[cur].data_ptr(), f[1 - cur].data_ptr(), cnt.data_ptr(), sync_iters, 64, 256, None)
+            cur = 1 - cur
+            if int(cnt.item()) == 0:
+                break
+        d = oracle.bfs_depth(host.index, host.neighbors, s)
+        assert oracle.verify_bfs_parents(host.index, host.neighbors, d, par.cpu().numpy(), s)[0] == 0
+
+
 def test_epoch_rejects_bad_shape():
     s = hc.lib().hc_epoch_sssp_pull(None, None, 0, 10, None, None, hc.VARIANT_WARP, 64, 256, None)
     assert s == hc.INVALID_ARG
