@@ -596,6 +596,37 @@ def batched_section(g, host, a, torch, dev, stream, k=512):
     return out
 
 
+def batched_ranks_section(g, host, a, torch, dev, rank, world, k=512):
+    """N > 1: the batched engine sharded by source (weak scaling, no data-path collective): every rank runs
+    k sources of its own (picks [r*k, (r+1)*k) of the SourcePicker sequence) in one batched BFS and one
+    batched SSSP call; time = max over ranks; parity: the first rows against the plain runs on each rank."""
+    import hc
+    from hc.shard import max_over_ranks, rank_sources
+    n, m = host.num_nodes, host.num_edges
+    src = rank_sources(host, k, rank)
+    bat = torch.empty((k, n), dtype=torch.int32, device=dev)
+    one = torch.empty((1, n), dtype=torch.int32, device=dev)
+    par1 = torch.empty((1, n), dtype=torch.int32, device=dev)
+    out = {"sources_per_rank": k, "ranks": world}
+    ok = True
+    for name, run_b, run_p in [("bfs", lambda: g.bfs_batched(src, bat), lambda i: g.bfs(src[i:i + 1], one, par1)),
+                               ("sssp", lambda: g.sssp_batched(src, bat), lambda i: g.sssp(src[i:i + 1], one))]:
+        run_b()
+        ms = max_over_ranks(_time_cuda(run_b, torch, dev, 1), dev)
+        for i in (0, k // 2, k - 1):
+            run_p(i)
+            ok &= bool(torch.equal(bat[i:i + 1], one))
+        out[name] = {"batched_ms": ms, "batched_gteps": world * k * (m / 2) / ms / 1e6}
+    t = torch.tensor([1.0 if ok else 0.0], device=dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+    out["ok"] = bool(t.item() == 1.0)
+    del bat
+    torch.cuda.empty_cache()
+    return out
+
+
 def adjoint_section(g, host, a, torch, dev):
     """PageRank forward + hand-written adjoint against the forward alone (weighted: the int32 weights as
     fp32, row-normalised; L = c . x with seeded Gaussian c; L1 tolerance 1e-6 forward, 1e-6 relative
@@ -829,6 +860,9 @@ def main():
                     parity[key] = {"ok": extras[key]["ok"] if key == "batched" else extras[key]["parity"]["ok"]}
             parity["ok"] = all(v["ok"] for v in parity.values() if isinstance(v, dict))
 
+    if world > 1 and not a.no_extras:
+        # Every rank takes the same collective steps here (max-over-ranks timings, the parity reduction).
+        extras["batched"] = batched_ranks_section(g, host, a, torch, dev, rank, world)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": a.steps,

@@ -400,30 +400,17 @@ int64_t hc_graph::bytes_held() const {
     return t;
 }
 
-using namespace hc;
+namespace hc {
 
-extern "C" {
-
-hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const void *weights,
-                          hc_wtype wtype, int32_t num_nodes, int64_t num_edges, int32_t device,
-                          hc_graph **out) {
-    clear_error();
-    if (!out) return fail(HC_ERR_INVALID_ARG, "hc_graph_create: null output handle");
+hc_status graph_alloc(int32_t num_nodes, int64_t num_edges, hc_wtype wtype, int32_t device, hc_graph **out) {
     *out = nullptr;
-    if (!index || num_nodes < 1 || num_edges < 0 || (num_edges > 0 && !neighbors))
-        return fail(HC_ERR_INVALID_ARG, "hc_graph_create: bad CSR (N=%d, M=%lld)", num_nodes,
-                    (long long)num_edges);
-    if (wtype != HC_W_NONE && !weights)
-        return fail(HC_ERR_INVALID_ARG, "hc_graph_create: weight type given without weights");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
-        return fail(HC_ERR_NO_DEVICE, "hc_graph_create: no CUDA device visible");
+        return fail(HC_ERR_NO_DEVICE, "no CUDA device visible");
     }
-    if (device < 0 || device >= ndev)
-        return fail(HC_ERR_INVALID_ARG, "hc_graph_create: device %d out of range (%d)", device, ndev);
+    if (device < 0 || device >= ndev) return fail(HC_ERR_INVALID_ARG, "device %d out of range (%d)", device, ndev);
     HC_CUDA_TRY(cudaSetDevice(device));
-
     hc_graph *g = new hc_graph();
     g->device = device;
     g->N = num_nodes;
@@ -441,26 +428,26 @@ hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const 
     g->stream = g->own_stream;
     if (cudaEventCreate(&g->ev_start) != cudaSuccess || cudaEventCreate(&g->ev_stop) != cudaSuccess)
         return bail(fail(HC_ERR_CUDA, "cudaEventCreate failed"));
-
     hc_status st;
     if ((st = g->index.ensure(sizeof(int64_t) * ((size_t)num_nodes + 1))) != HC_OK) return bail(st);
     if ((st = g->nbr.ensure(sizeof(int32_t) * (size_t)(num_edges + kNbrPad))) != HC_OK) return bail(st);
     if (cudaMemsetAsync(g->nbr.ptr, 0, g->nbr.bytes, g->stream) != cudaSuccess)
         return bail(fail(HC_ERR_CUDA, "memset failed"));
-    if ((st = copy_in(g->index.ptr, index, sizeof(int64_t) * ((size_t)num_nodes + 1), g->stream)) != HC_OK)
-        return bail(st);
-    if ((st = copy_in(g->nbr.ptr, neighbors, sizeof(int32_t) * (size_t)num_edges, g->stream)) != HC_OK)
-        return bail(st);
     if (wtype != HC_W_NONE) {
         if ((st = g->wgt.ensure(4 * (size_t)(num_edges + kNbrPad))) != HC_OK) return bail(st);
         if (cudaMemsetAsync(g->wgt.ptr, 0, g->wgt.bytes, g->stream) != cudaSuccess)
             return bail(fail(HC_ERR_CUDA, "memset failed"));
-        if ((st = copy_in(g->wgt.ptr, weights, 4 * (size_t)num_edges, g->stream)) != HC_OK) return bail(st);
     }
+    *out = g;
+    return HC_OK;
+}
 
-    // Validate and analyse on the device (works for host or device inputs).
+hc_status graph_finish(hc_graph *g, const char *who) {
+    const int32_t num_nodes = g->N;
+    const int64_t num_edges = g->M;
+    // Validate and analyse on the device.
     DevBuf abuf;
-    if ((st = abuf.ensure(sizeof(Analysis))) != HC_OK) return bail(st);
+    HC_TRY(abuf.ensure(sizeof(Analysis)));
     Analysis init;
     std::memset(&init, 0, sizeof(init));
     init.first_zero = num_nodes;
@@ -469,23 +456,21 @@ hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const 
     if (cudaMemcpyAsync(abuf.ptr, &init, sizeof(init), cudaMemcpyHostToDevice, g->stream) != cudaSuccess ||
         cudaMemcpyAsync(&ends[0], g->index.as<int64_t>(), 8, cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
         cudaMemcpyAsync(&ends[1], g->index.as<int64_t>() + num_nodes, 8, cudaMemcpyDeviceToHost, g->stream) != cudaSuccess)
-        return bail(fail(HC_ERR_CUDA, "analysis setup failed"));
+        return fail(HC_ERR_CUDA, "%s: analysis setup failed", who);
     const int grid = g->sm_count * 8;
     { analyze_index<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), num_nodes, num_edges, abuf.as<Analysis>()); ::hc::count_launch(); }
     Analysis res;
     if (cudaMemcpyAsync(&res, abuf.ptr, sizeof(res), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
         cudaStreamSynchronize(g->stream) != cudaSuccess)
-        return bail(fail(HC_ERR_CUDA, "graph analysis failed: %s", cudaGetErrorString(cudaGetLastError())));
+        return fail(HC_ERR_CUDA, "%s: graph analysis failed: %s", who, cudaGetErrorString(cudaGetLastError()));
     if (ends[0] != 0 || ends[1] != num_edges || res.bad_index)
-        return bail(fail(HC_ERR_INVALID_ARG,
-                         "hc_graph_create: index must be non-decreasing from 0 to num_edges"));
+        return fail(HC_ERR_INVALID_ARG, "%s: index must be non-decreasing from 0 to num_edges", who);
     { analyze_rows<<<grid, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->nbr.as<int32_t>(), num_nodes,
                                                 abuf.as<Analysis>()); ::hc::count_launch(); }
     if (cudaMemcpyAsync(&res, abuf.ptr, sizeof(res), cudaMemcpyDeviceToHost, g->stream) != cudaSuccess ||
         cudaStreamSynchronize(g->stream) != cudaSuccess)
-        return bail(fail(HC_ERR_CUDA, "graph analysis failed: %s", cudaGetErrorString(cudaGetLastError())));
-    if (res.bad_nbr) return bail(fail(HC_ERR_INVALID_ARG, "hc_graph_create: neighbour id outside [0, N)"));
-
+        return fail(HC_ERR_CUDA, "%s: graph analysis failed: %s", who, cudaGetErrorString(cudaGetLastError()));
+    if (res.bad_nbr) return fail(HC_ERR_INVALID_ARG, "%s: neighbour id outside [0, N)", who);
     g->degree_sorted = !res.unsorted;
     g->rows_sorted = !res.rows_unsorted;
     g->max_degree = res.max_degree;
@@ -496,6 +481,40 @@ hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const 
     } else {
         g->n_warp_rows = 0;
     }
+    return HC_OK;
+}
+
+}  // namespace hc
+
+using namespace hc;
+
+extern "C" {
+
+hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors, const void *weights,
+                          hc_wtype wtype, int32_t num_nodes, int64_t num_edges, int32_t device,
+                          hc_graph **out) {
+    clear_error();
+    if (!out) return fail(HC_ERR_INVALID_ARG, "hc_graph_create: null output handle");
+    *out = nullptr;
+    if (!index || num_nodes < 1 || num_edges < 0 || (num_edges > 0 && !neighbors))
+        return fail(HC_ERR_INVALID_ARG, "hc_graph_create: bad CSR (N=%d, M=%lld)", num_nodes,
+                    (long long)num_edges);
+    if (wtype != HC_W_NONE && !weights)
+        return fail(HC_ERR_INVALID_ARG, "hc_graph_create: weight type given without weights");
+    hc_graph *g = nullptr;
+    HC_TRY(graph_alloc(num_nodes, num_edges, wtype, device, &g));
+    auto bail = [&](hc_status s) {
+        hc_graph_destroy(g);
+        return s;
+    };
+    hc_status st;
+    if ((st = copy_in(g->index.ptr, index, sizeof(int64_t) * ((size_t)num_nodes + 1), g->stream)) != HC_OK)
+        return bail(st);
+    if ((st = copy_in(g->nbr.ptr, neighbors, sizeof(int32_t) * (size_t)num_edges, g->stream)) != HC_OK)
+        return bail(st);
+    if (wtype != HC_W_NONE && (st = copy_in(g->wgt.ptr, weights, 4 * (size_t)num_edges, g->stream)) != HC_OK)
+        return bail(st);
+    if ((st = graph_finish(g, "hc_graph_create")) != HC_OK) return bail(st);
     *out = g;
     return HC_OK;
 }

@@ -135,6 +135,12 @@ struct OutPipe {
     hc_status finish();
 };
 
+// A handle for an N-vertex, M-edge graph on `device` with its CSR arrays
+// allocated (neighbour and weight pads zeroed) and not yet filled.
+hc_status graph_alloc(int32_t num_nodes, int64_t num_edges, hc_wtype wtype, int32_t device, hc_graph **out);
+// Validates the filled CSR (offsets 0..M non-decreasing, ids in [0, N)) and
+// records its degree analysis; `who` names the caller in error messages.
+hc_status graph_finish(hc_graph *g, const char *who);
 // Checks a caller's CSR on the device (offsets rising from 0 to m, neighbour
 // ids in [0, n); `stride` 2 for interleaved {id, weight} edges): clears
 // *flag_dev, then sets bit 0 (offsets) / bit 1 (ids) on a violation.

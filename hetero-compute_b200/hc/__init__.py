@@ -122,6 +122,7 @@ _SIGS = {
     "hc_graph_get_info": (C.c_int, [_P, C.POINTER(GraphInfo)]),
     "hc_graph_generate": (C.c_int, [C.c_int, C.c_int32, C.c_int32, C.c_uint64, C.c_int, C.c_int32, C.POINTER(_P)]),
     "hc_graph_get_csr": (C.c_int, [_P, _P, _P, _P]),
+    "hc_graph_load": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_P)]),
     "hc_graph_pick_sources": (C.c_int, [_P, C.c_int32, _P]),
     "hc_bfs": (C.c_int, [_P, _P, C.c_int32, _P, _P, C.POINTER(BfsOpts), C.POINTER(BfsStats)]),
     "hc_sssp": (C.c_int, [_P, _P, C.c_int32, _P, _P, C.POINTER(SsspOpts), C.POINTER(SsspStats)]),
@@ -324,6 +325,17 @@ class Graph:
         h = C.c_void_p()
         _check(lib().hc_graph_generate(kind, scale, edge_factor, seed, wtype, device, C.byref(h)),
                "hc_graph_generate")
+        self = cls.__new__(cls)
+        self._h = h
+        info = self.info()
+        self.num_nodes, self.num_edges, self.wtype = info.num_nodes, info.num_edges, info.wtype
+        return self
+
+    @classmethod
+    def load(cls, path: str, weighted: int = 0, device: int = 0) -> "Graph":
+        """hc_graph_load: a .sg (weighted 0) or .wsg (1: fp32 weights, 2: int32) file streamed to the device."""
+        h = C.c_void_p()
+        _check(lib().hc_graph_load(path.encode(), weighted, device, C.byref(h)), "hc_graph_load")
         self = cls.__new__(cls)
         self._h = h
         info = self.info()

@@ -22,6 +22,13 @@ def split_batch(sources: np.ndarray, rank: int, world: int) -> np.ndarray:
     return sources[bounds[rank]:bounds[rank + 1]]
 
 
+def run_sharded(run, sources: np.ndarray, rank: int, world: int) -> np.ndarray:
+    """One batch of sources over all ranks (strong scaling): this rank runs `run` on its contiguous share
+    (split_batch) -- a batched BFS / SSSP call returning [k_r, N] rows -- and every rank receives all rows in
+    the batch's source order."""
+    return gather_rows(np.asarray(run(split_batch(sources, rank, world))), world)
+
+
 def max_over_ranks(value: float, device=None) -> float:
     """Max of a per-rank scalar (the timing rule for multi-GPU numbers)."""
     import torch

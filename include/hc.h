@@ -124,6 +124,16 @@ hc_status hc_graph_create(const int64_t *index, const int32_t *neighbors,
                           int64_t num_edges, int32_t device, hc_graph **out);
 hc_status hc_graph_destroy(hc_graph *g);
 
+/* A .sg / .wsg file (layout as hc_csr_read; weighted 0 = .sg, 1 = .wsg with
+ * fp32 weights, 2 = .wsg with weights converted to int32, which must be
+ * non-negative integers) streamed into a device graph on `device`: chunks
+ * go through two pinned staging buffers, file reads overlapping the copies,
+ * so host memory stays at 64 MB whatever the graph's size.  Checked like
+ * hc_graph_create; a short or inconsistent file returns HC_ERR_IO.  Replaces
+ * load_graph_from_file (src/graph.cuh:207-239) plus the drivers' per-call
+ * upload (src/kernels/gpu/sssp.cuh:51-61). */
+hc_status hc_graph_load(const char *path, int32_t weighted, int32_t device, hc_graph **out);
+
 /* Synthetic graphs built on the device: the same CSR as hc_gen_kronecker /
  * hc_gen_uniform (same scale, edge factor or pairs per vertex, seed and
  * weights) followed by hc_graph_create, without host memory or an upload.

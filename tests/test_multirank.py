@@ -24,7 +24,7 @@ def _worker(rank, world, port, q):
     sys.path[:0] = [root, os.path.join(root, "hetero-compute_b200")]
     import hc
     import oracle
-    from hc.shard import gather_rows, max_over_ranks, rank_sources, split_batch
+    from hc.shard import gather_rows, max_over_ranks, rank_sources, run_sharded, split_batch
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world,
@@ -39,8 +39,13 @@ def _worker(rank, world, port, q):
         # split_batch: pad each rank's slice to a common width with -1 before gathering
         part = split_batch(np.arange(11), rank, world)
         parts = gather_rows(np.pad(part, (0, 6 - len(part)), constant_values=-1)[None, :], world)
+        # One batch of 11 sources split over the ranks (uneven shares), each rank's share run by a stand-in
+        # for the batched BFS (the oracle, row per source), rows gathered in source order.
+        batch = hc.pick_sources(host, 11)
+        rows = run_sharded(lambda ss: np.stack([oracle.bfs_depth(host.index, host.neighbors, s) for s in ss]),
+                           batch, rank, world)
         if rank == 0:
-            q.put((allsrc, alld, t, parts))
+            q.put((allsrc, alld, t, parts, rows))
     finally:
         dist.destroy_process_group()
 
@@ -57,7 +62,7 @@ def test_two_rank_source_sharding():
     procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    allsrc, alld, t, parts = q.get(timeout=120)
+    allsrc, alld, t, parts, rows = q.get(timeout=120)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
@@ -69,3 +74,7 @@ def test_two_rank_source_sharding():
     assert t == 2.0
     got = parts[parts >= 0]
     assert np.array_equal(np.sort(got), np.arange(11))
+    batch = hc.pick_sources(host, 11)
+    assert rows.shape == (11, host.num_nodes)
+    for i, s in enumerate(batch):
+        assert np.array_equal(rows[i], oracle.bfs_depth(host.index, host.neighbors, s))
