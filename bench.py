@@ -715,7 +715,7 @@ def main():
     src = rank_sources(host, k, rank)
     src_dev = torch.from_numpy(src).to(dev)
     # Untimed: the autotuner picks the BFS / SSSP launch parameters on this graph.
-    tuning = g.autotune(src, hc.TUNE_BFS | hc.TUNE_SSSP) if a.tune else None
+    tuning = g.autotune(src, hc.TUNE_BFS | hc.TUNE_BFS_LEVELS | hc.TUNE_SSSP) if a.tune else None
 
     depth = torch.empty((k, n), dtype=torch.int32, device=dev)
     parent = torch.empty((k, n), dtype=torch.int32, device=dev)

@@ -27,6 +27,7 @@ namespace hc {
 namespace {
 
 constexpr int kBfsThreads = 512;
+constexpr int kBuSplitLevels = HC_BFS_SPLIT_LEVELS;
 constexpr int kTraceLevels = 64;
 // Bottom-up levels copy the first kHubWords words of the frontier bitmap
 // (the 131072 highest-degree vertices of a degree-sorted graph, which most
@@ -63,6 +64,12 @@ struct BfsArgs {
     BfsCtl *ctl;
     int32_t src;
     int alpha, beta, direction, bu_variant, max_levels;
+    // Per bottom-up level warp/thread split (the per-epoch granularity
+    // selector): bottom-up level k (0 = the first) runs warp per vertex on
+    // [0, bu_split[min(k, bu_split_levels - 1)]) and thread per vertex after;
+    // bu_split_levels 0 = the fixed split of bu_variant.
+    int32_t bu_split[kBuSplitLevels];
+    int bu_split_levels;
 };
 
 __device__ __forceinline__ uint32_t *fb_sel(const BfsArgs &a, int i) {
@@ -245,9 +252,11 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
             // >= 32-edge prefix (0.36 vs 0.68 ms per source at scale 22), since
             // the first probes of a sorted row usually hit.  BLOCK selects the
             // warp path only for that prefix.
-            const int n_warp = a.bu_variant == HC_VARIANT_WARP
-                                   ? a.n_active
-                                   : (a.bu_variant == HC_VARIANT_BLOCK ? a.n_warp_rows : 0);
+            const int n_warp = a.bu_split_levels > 0
+                                   ? a.bu_split[min(bu_levels - 1, a.bu_split_levels - 1)]
+                                   : a.bu_variant == HC_VARIANT_WARP
+                                         ? a.n_active
+                                         : (a.bu_variant == HC_VARIANT_BLOCK ? a.n_warp_rows : 0);
             const int n_warp_al = min(((n_warp + 31) >> 5) << 5, W_act << 5);
             for (int v = gwarp; v < n_warp_al; v += nwarps) {
                 if (v >= a.n_active) break;
@@ -394,6 +403,9 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
     // Zero fields: the handle's tuned values, else Beamer's alpha = 15, beta = 18.
     if (o.alpha <= 0) o.alpha = g->tune.bfs_alpha > 0 ? g->tune.bfs_alpha : 15;
     if (o.beta <= 0) o.beta = g->tune.bfs_beta > 0 ? g->tune.bfs_beta : 18;
+    // AUTO: the handle's per-level split table when the autotuner left one,
+    // else its tuned variant.
+    const bool by_level = o.bu_variant == HC_VARIANT_AUTO && g->tune.bfs_bu_split_levels > 0;
     if (o.bu_variant == HC_VARIANT_AUTO) o.bu_variant = (hc_variant)g->tune.bfs_bu_variant;
     if (o.direction < 0 || o.direction > 2) return fail(HC_ERR_INVALID_ARG, "hc_bfs: direction must be 0, 1 or 2");
     if (stats) std::memset(stats, 0, sizeof(*stats));
@@ -435,6 +447,12 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
     a.direction = o.direction;
     a.bu_variant = (int)o.bu_variant;
     a.max_levels = g->N + 1;
+    a.bu_split_levels = 0;
+    if (by_level) {
+        a.bu_split_levels = std::min(g->tune.bfs_bu_split_levels, kBuSplitLevels);
+        for (int k = 0; k < a.bu_split_levels; k++)
+            a.bu_split[k] = std::max(0, std::min(g->tune.bfs_bu_split[k], g->n_active));
+    }
 
     const bool dev_depth = is_device_pointer(depth_out);
     const bool dev_parent = is_device_pointer(parent_out);

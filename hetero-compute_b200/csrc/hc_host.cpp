@@ -391,6 +391,33 @@ hc_status hc_csr_write(const char *path, const hc_csr *g) {
     return HC_OK;
 }
 
+hc_status hc_equal_edge_ranges(const int64_t *index, int32_t num_nodes, int32_t num_segments, int32_t chunk_size,
+                               int32_t *ranges_out) {
+    clear_error();
+    if (!index || !ranges_out || num_nodes < 1 || num_segments < 1 || chunk_size < 1)
+        return fail(HC_ERR_INVALID_ARG, "hc_equal_edge_ranges: bad arguments");
+    const int64_t m = index[num_nodes] - index[0];
+    const int64_t avg = m / num_segments;
+    ranges_out[0] = 0;
+    int32_t seg = 0;
+    int64_t acc = 0;
+    int32_t v = 0;
+    for (; v < num_nodes; v++) {
+        acc += index[v + 1] - index[v];
+        if (acc >= avg && seg + 1 < num_segments) {  // the reference has no bound on seg here
+            ranges_out[seg + 1] = v;
+            acc = 0;
+            seg++;
+        }
+    }
+    for (int32_t s = seg + 1; s <= num_segments; s++) ranges_out[s] = num_nodes;
+    for (int32_t s = 1; s < num_segments; s++) {
+        const int32_t r = ranges_out[s] % chunk_size;
+        if (r != 0) ranges_out[s] = r < chunk_size / 2 ? ranges_out[s] - r : std::min(ranges_out[s] - r + chunk_size, num_nodes);
+    }
+    return HC_OK;
+}
+
 hc_status hc_pick_sources(const int64_t *index, const int32_t *neighbors, int32_t num_nodes,
                           int32_t count, int32_t const_source, int32_t *out) {
     clear_error();

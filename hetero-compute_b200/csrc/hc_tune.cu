@@ -107,6 +107,63 @@ hc_status tune_bfs(Tuner &tu, hc_tuning &out) {
     return HC_OK;
 }
 
+// The per-epoch granularity selector of bottom-up BFS: for each bottom-up
+// level in turn (up to HC_BFS_SPLIT_LEVELS, as many as the sample runs have),
+// the warp/thread split point is searched among the 32-aligned bounds of
+// equal-edge vertex segments (hc_equal_edge_ranges, the reference's
+// compute_equal_edge_ranges segmentation), the other levels held at their
+// current split, whole BFS calls timed.  The table is kept only if some level
+// moved off the tuned variant's fixed split.
+hc_status tune_bfs_levels(Tuner &tu, hc_tuning &out) {
+    hc_graph *g = tu.g;
+    const int k = (int)std::min<size_t>(tu.src.size(), 16);
+    hc_bfs_opts o{};
+    o.alpha = out.bfs_alpha > 0 ? out.bfs_alpha : 15;
+    o.beta = out.bfs_beta > 0 ? out.bfs_beta : 18;
+    const int var = out.bfs_bu_variant > 0 ? out.bfs_bu_variant : HC_VARIANT_THREAD;
+    const int32_t base = var == HC_VARIANT_WARP ? g->n_active : (var == HC_VARIANT_BLOCK ? g->n_warp_rows : 0);
+    // Bottom-up levels per run on the samples.
+    o.bu_variant = (hc_variant)var;
+    hc_bfs_stats st{};
+    HC_TRY(hc_bfs(g, tu.src.data(), k, nullptr, nullptr, &o, &st));
+    const int levels = std::min(HC_BFS_SPLIT_LEVELS, (st.bu_levels + k - 1) / std::max(k, 1));
+    if (levels < 1) return HC_OK;
+    // Candidates: 32-aligned bounds of 16 equal-edge segments of the active rows.
+    std::vector<int64_t> index((size_t)g->N + 1);
+    HC_CUDA_TRY(cudaMemcpyAsync(index.data(), g->index.ptr, sizeof(int64_t) * index.size(), cudaMemcpyDeviceToHost,
+                                g->stream));
+    HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    std::vector<int32_t> bounds(17);
+    HC_TRY(hc_equal_edge_ranges(index.data(), std::max(g->n_active, 1), 16, 32, bounds.data()));
+    std::vector<int32_t> cands(bounds.begin(), bounds.end());
+    cands.push_back(g->n_warp_rows);
+    std::sort(cands.begin(), cands.end());
+    cands.erase(std::unique(cands.begin(), cands.end()), cands.end());
+
+    hc_tuning &live = g->tune;  // trials read the table from the handle (bu_variant AUTO)
+    live.bfs_bu_variant = var;
+    live.bfs_bu_split_levels = levels;
+    for (int l = 0; l < levels; l++) live.bfs_bu_split[l] = base;
+    o.bu_variant = HC_VARIANT_AUTO;
+    auto run = [&](const hc_bfs_opts &x) { return tu.bfs(x, k); };
+    double best = run(o);
+    if (best == kFailed) return fail(HC_ERR_CUDA, "hc_autotune: BFS level trial failed");
+    bool moved = false;
+    for (int l = 0; l < levels; l++) {
+        descend(o, &live.bfs_bu_split[l], cands, best, run);
+        moved |= live.bfs_bu_split[l] != base;
+    }
+    if (moved) {
+        out.bfs_bu_split_levels = levels;
+        for (int l = 0; l < HC_BFS_SPLIT_LEVELS; l++) out.bfs_bu_split[l] = l < levels ? live.bfs_bu_split[l] : 0;
+    } else {
+        out.bfs_bu_split_levels = 0;
+    }
+    live.bfs_bu_split_levels = 0;
+    live.bfs_bu_variant = 0;
+    return HC_OK;
+}
+
 hc_status tune_sssp(Tuner &tu, hc_tuning &out) {
     hc_graph *g = tu.g;
     if (g->wtype != HC_W_I32) return HC_OK;  // no SSSP on this graph
@@ -210,6 +267,7 @@ extern "C" hc_status hc_autotune(hc_graph *g, const int32_t *sample_sources, int
     std::memset(&g->tune, 0, sizeof(g->tune));
     hc_status st = HC_OK;
     if (st == HC_OK && (what & HC_TUNE_BFS)) st = tune_bfs(tu, t);
+    if (st == HC_OK && (what & HC_TUNE_BFS_LEVELS)) st = tune_bfs_levels(tu, t);
     if (st == HC_OK && (what & HC_TUNE_SSSP)) st = tune_sssp(tu, t);
     if (st == HC_OK && (what & HC_TUNE_BFS_BATCHED)) st = tune_bfs_batched(tu, t);
     if (st == HC_OK && (what & HC_TUNE_SSSP_BATCHED)) st = tune_sssp_batched(tu, t);
@@ -238,6 +296,11 @@ extern "C" hc_status hc_set_tuning(hc_graph *g, const hc_tuning *t) {
         return fail(HC_ERR_INVALID_ARG, "hc_set_tuning: bad BFS variant %d", t->bfs_bu_variant);
     if (t->bfs_alpha < 0 || t->bfs_beta < 0 || t->mbfs_group < 0 || t->mssp_group < 0)
         return fail(HC_ERR_INVALID_ARG, "hc_set_tuning: negative threshold or group");
+    if (t->bfs_bu_split_levels < 0 || t->bfs_bu_split_levels > HC_BFS_SPLIT_LEVELS)
+        return fail(HC_ERR_INVALID_ARG, "hc_set_tuning: bad split level count %d", t->bfs_bu_split_levels);
+    for (int l = 0; l < t->bfs_bu_split_levels; l++)
+        if (t->bfs_bu_split[l] < 0 || t->bfs_bu_split[l] > g->N)
+            return fail(HC_ERR_INVALID_ARG, "hc_set_tuning: split %d outside [0, N]", t->bfs_bu_split[l]);
     g->tune = *t;
     return HC_OK;
 }

@@ -90,13 +90,16 @@ class Tuning(C.Structure):
     _fields_ = [("bfs_alpha", C.c_int32), ("bfs_beta", C.c_int32), ("bfs_bu_variant", C.c_int32),
                 ("sssp_delta", C.c_int32), ("sssp_pull_alpha", C.c_int32), ("mbfs_group", C.c_int32),
                 ("mbfs_switch_alpha", C.c_int32), ("mssp_group", C.c_int32), ("mssp_switch_alpha", C.c_int32),
-                ("trials", C.c_int32), ("tune_ms", C.c_double)]
+                ("trials", C.c_int32), ("tune_ms", C.c_double), ("bfs_bu_split", C.c_int32 * 8),
+                ("bfs_bu_split_levels", C.c_int32)]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["bfs_bu_split"] = list(d["bfs_bu_split"])[:self.bfs_bu_split_levels]
+        return d
 
 
-TUNE_BFS, TUNE_SSSP, TUNE_BFS_BATCHED, TUNE_SSSP_BATCHED, TUNE_ALL = 1, 2, 4, 8, 15
+TUNE_BFS, TUNE_SSSP, TUNE_BFS_BATCHED, TUNE_SSSP_BATCHED, TUNE_BFS_LEVELS, TUNE_ALL = 1, 2, 4, 8, 16, 31
 
 
 class BatchStats(C.Structure):
@@ -491,7 +494,11 @@ class Graph:
         return t.as_dict()
 
     def set_tuning(self, values: dict):
-        t = Tuning(**{k: v for k, v in values.items() if k in dict(Tuning._fields_)})
+        vals = {k: v for k, v in values.items() if k in dict(Tuning._fields_)}
+        split = list(vals.pop("bfs_bu_split", []))
+        t = Tuning(**vals)
+        for i, x in enumerate(split[:8]):
+            t.bfs_bu_split[i] = x
         _check(lib().hc_set_tuning(self._h, C.byref(t)), "hc_set_tuning")
 
 

@@ -366,6 +366,7 @@ hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_t num_sourc
  * means "the tuned value", or the built-in default while a field is untuned
  * (zero here).  No counterpart in the reference, whose variant and launch
  * shape are chosen by hand per call (src/kernels/gpu/bfs.cuh:352-360). */
+#define HC_BFS_SPLIT_LEVELS 8
 typedef struct hc_tuning {
     int32_t bfs_alpha;          /* hc_bfs_opts.alpha */
     int32_t bfs_beta;           /* hc_bfs_opts.beta */
@@ -378,13 +379,22 @@ typedef struct hc_tuning {
     int32_t mssp_switch_alpha;  /* hc_sssp_batched switch_alpha */
     int32_t trials;             /* candidates timed by the last hc_autotune */
     double tune_ms;             /* device time spent on them */
+    /* Per bottom-up BFS level granularity (HC_TUNE_BFS_LEVELS): bottom-up
+     * level k (0 = the first of a run) visits vertices [0, bfs_bu_split[k])
+     * warp per vertex and the rest thread per vertex (later levels use the
+     * last entry).  Used by hc_bfs when hc_bfs_opts.bu_variant is AUTO and
+     * bfs_bu_split_levels > 0; the candidates are equal-edge segment bounds
+     * (hc_equal_edge_ranges), 32-aligned. */
+    int32_t bfs_bu_split[HC_BFS_SPLIT_LEVELS];
+    int32_t bfs_bu_split_levels;
 } hc_tuning;
 
 #define HC_TUNE_BFS 1u
 #define HC_TUNE_SSSP 2u
 #define HC_TUNE_BFS_BATCHED 4u
 #define HC_TUNE_SSSP_BATCHED 8u
-#define HC_TUNE_ALL 15u
+#define HC_TUNE_BFS_LEVELS 16u
+#define HC_TUNE_ALL 31u
 
 /* Times candidate parameters on the sample sources (CUDA events, outputs
  * discarded) by coordinate descent, one parameter at a time from the current
@@ -408,6 +418,50 @@ hc_status hc_dev_memset(void *ptr, int32_t value, size_t bytes);
 hc_status hc_device_synchronize(void);
 /* Kernels launched by this library in this process so far. */
 int64_t hc_kernel_launches(void);
+
+/* ------------------------------------------------- segment profiling */
+/* Vertex ranges of about equal edge count, the reference's
+ * compute_equal_edge_ranges (src/graph.cuh:156-201): walking the vertices in
+ * order, a segment closes at the vertex whose degree brings its running sum to
+ * at least num_edges / num_segments (that vertex opens the next one); the
+ * last segment ends at num_nodes, and inner bounds are rounded to the nearest
+ * multiple of chunk_size.  ranges_out: num_segments + 1 entries.  Three
+ * departures keep every vertex in exactly one segment where the reference
+ * does not: closures past num_segments - 1 are dropped (the reference writes
+ * past its array when the edge total is not divisible by the count, or is
+ * below it), the last segment always ends at num_nodes (the reference's ends
+ * at the vertex that closed it when num_segments closures happen), and bounds
+ * never round past num_nodes.  index: host array. */
+hc_status hc_equal_edge_ranges(const int64_t *index, int32_t num_nodes, int32_t num_segments,
+                               int32_t chunk_size, int32_t *ranges_out);
+
+typedef enum hc_profile_algo {
+    HC_PROFILE_SSSP = 0,  /* epoch_sssp_pull_gpu_* (hc_epoch_sssp_pull) */
+    HC_PROFILE_PR = 1,    /* epoch_pr_pull_gpu_* (hc_epoch_pr_pull) */
+    HC_PROFILE_BFS = 2    /* epoch_bfs_pull_gpu_* / sync warp (hc_epoch_bfs_pull / _sync_pull) */
+} hc_profile_algo;
+
+/* segment_res_t (src/benchmarks/benchmark.cuh:36-47). */
+typedef struct hc_segment_result {
+    int32_t start_id, end_id;  /* [start_id, end_id) */
+    int64_t num_edges;
+    float avg_degree, min_degree, max_degree;
+    int32_t epoch;             /* BFS: the level profiled; -1 otherwise */
+    double millis;             /* mean over `iters` launches */
+    double gteps;              /* num_edges / 2 per second, the reference's formula */
+} hc_segment_result;
+
+/* The per-segment benchmark of the reference's TreeBenchmark
+ * (src/benchmarks/benchmark.cuh:87-309, gpu_benchmark.cuh:201-330): for each
+ * segment [ranges[s], ranges[s+1]) one epoch kernel launch of `variant`
+ * (sync_iters > 0: the sync-warp BFS kernel) with the given shape, timed with
+ * CUDA events over `iters` launches from the same initial state (SSSP / PR: a
+ * seeded random vector; BFS: the state before level `level` of a BFS from
+ * `source`).  out: num_segments results. */
+hc_status hc_profile_segments(hc_graph *g, hc_profile_algo algo, hc_variant variant, int32_t sync_iters,
+                              const int32_t *ranges, int32_t num_segments, int32_t source, int32_t level,
+                              int32_t block_count, int32_t thread_count, int32_t iters,
+                              hc_segment_result *out);
 
 /* ------------------------------------------------------- time limits */
 /* No counterpart in the reference, whose host loops wait without a bound.

@@ -156,3 +156,27 @@ def run_reference(algo, graph_path, nsrc, out_path, threads=None, timeout=None, 
     r = subprocess.run([REF_DRIVER, algo, graph_path, str(nsrc), out_path, str(repeats), str(warmup)],
                        capture_output=True, text=True, env=env, check=True, timeout=timeout)
     return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def equal_edge_ranges_reference(index, num_segments, chunk_size=1):
+    """compute_equal_edge_ranges (src/graph.cuh:156-201) step by step, with its array allowed to grow: returns
+    (bounds written, in order; closures).  bounds[0] = 0; a closure at vertex v writes v; after the walk, if
+    fewer than num_segments closures happened, num_nodes is written next; inner bounds 1 .. num_segments - 1
+    are rounded to chunk_size.  Entries the reference leaves unwritten are absent."""
+    n = len(index) - 1
+    avg = int(index[n] - index[0]) // num_segments
+    b = [0]
+    acc, closures = 0, 0
+    for v in range(n):
+        acc += int(index[v + 1] - index[v])
+        if acc >= avg:
+            b.append(v)
+            acc = 0
+            closures += 1
+    if closures != num_segments:
+        b.append(n)
+    for i in range(1, min(num_segments, len(b))):
+        r = b[i] % chunk_size
+        if r:
+            b[i] = b[i] - r if r < chunk_size // 2 else b[i] - r + chunk_size
+    return b, closures

@@ -26,6 +26,7 @@ def test_tuned_values_come_from_the_candidates(tuned):
     assert t["sssp_delta"] > 0 and (t["sssp_pull_alpha"] == -1 or 1 <= t["sssp_pull_alpha"] <= 12)
     assert t["mbfs_group"] in (64, 128, 256, 512) and t["mbfs_switch_alpha"] in (5, 10, 20, 40, -1)
     assert t["mssp_group"] in (64, 128, 256, 512) and t["mssp_switch_alpha"] in (1, 2, 4, -1)
+    assert 0 <= t["bfs_bu_split_levels"] <= 8 and len(t["bfs_bu_split"]) == t["bfs_bu_split_levels"]
     assert g.tuning == t
 
 
@@ -58,3 +59,31 @@ def test_set_tuning_round_trip_and_explicit_options_win(tuned):
     assert e.value.status == hc.INVALID_ARG
     g.set_tuning(saved)
     assert g.tuning == saved
+
+
+def test_per_level_split_table_exact_and_validated(tuned):
+    """The per-bottom-up-level warp/thread split (the per-epoch granularity selector): tuned splits come
+    from the equal-edge segment bounds, hand-set tables of every shape keep BFS exact, and bad tables are
+    refused."""
+    from hc import profile
+    host, g, src, t = tuned
+    bounds = set(profile.equal_edge_ranges(host.index[:g.info().num_active + 1], 16, 32).tolist())
+    n_active = g.info().num_active
+    for x in t["bfs_bu_split"]:
+        assert x in bounds or x % 32 == 0, x
+    saved = g.tuning
+    s = src[:5]
+    for table in ([0], [n_active], [n_active, 0, 1024], [64, 4096, 0, n_active]):
+        g.set_tuning(dict(saved, bfs_bu_split=table, bfs_bu_split_levels=len(table)))
+        depth, parent, st = g.bfs(s, stats=True)
+        assert st.bu_levels > 0
+        for i, v in enumerate(s):
+            d = oracle.bfs_depth(host.index, host.neighbors, v)
+            assert np.array_equal(depth[i], d)
+            assert oracle.verify_bfs_parents(host.index, host.neighbors, d, parent[i], v)[0] == 0
+    for bad in (dict(bfs_bu_split_levels=9), dict(bfs_bu_split=[-1], bfs_bu_split_levels=1),
+                dict(bfs_bu_split=[host.num_nodes + 1], bfs_bu_split_levels=1)):
+        with pytest.raises(hc.HCError) as e:
+            g.set_tuning(dict(saved, **bad))
+        assert e.value.status == hc.INVALID_ARG
+    g.set_tuning(saved)

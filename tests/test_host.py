@@ -144,7 +144,13 @@ def test_no_device_is_an_error_not_a_fallback():
 _STRUCTS = {"CSR": "hc_csr", "GraphInfo": "hc_graph_info", "BfsOpts": "hc_bfs_opts", "BfsStats": "hc_bfs_stats",
             "SsspOpts": "hc_sssp_opts", "SsspStats": "hc_sssp_stats", "PrOpts": "hc_pr_opts",
             "PrStats": "hc_pr_stats", "BatchOpts": "hc_batch_opts", "BatchStats": "hc_batch_stats",
-            "Tuning": "hc_tuning"}
+            "Tuning": "hc_tuning", "profile.SegmentResult": "hc_segment_result"}
+
+
+def _resolve(name):
+    import importlib
+    mod, _, attr = name.rpartition(".")
+    return getattr(importlib.import_module("hc." + mod) if mod else hc, attr)
 
 
 def test_ctypes_structs_match_the_c_header(tmp_path):
@@ -157,7 +163,7 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
         pytest.skip("gcc not found")
     lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "hc.h"', "int main(void) {"]
     for py, c in _STRUCTS.items():
-        cls = getattr(hc, py)
+        cls = _resolve(py)
         lines.append(f'printf("{py} size %zu\\n", sizeof({c}));')
         for name, _ in cls._fields_:
             lines.append(f'printf("{py} {name} %zu\\n", offsetof({c}, {name}));')
@@ -173,7 +179,7 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
             py, name, val = line.split()
             got[(py, name)] = int(val)
     for py in _STRUCTS:
-        cls = getattr(hc, py)
+        cls = _resolve(py)
         assert got[(py, "size")] == C.sizeof(cls), py
         for name, _ in cls._fields_:
             assert got[(py, name)] == getattr(cls, name).offset, (py, name)
