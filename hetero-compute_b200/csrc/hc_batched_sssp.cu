@@ -65,10 +65,17 @@ struct WideDist {
     static constexpr int kPer = 1;
     static constexpr W kInfWord = kInfDist;
     __device__ static W weight(int32_t w) { return w; }
+    // d + w clamped at INT32_MAX: for d, w in [0, INT32_MAX] the unsigned
+    // sum cannot wrap, and a clamped candidate lowers nothing (the transpose
+    // refuses a group whose distances come within w_max of the clamp).
+    __device__ static W sum(W d, W w) {
+        const uint32_t s = (uint32_t)d + (uint32_t)w;
+        return s < (uint32_t)kInfDist ? (W)s : kInfDist;
+    }
     // min(best, d + w) over the word's distances; an unreachable d changes nothing.
-    __device__ static W relax(W best, W d, W w) { return (d != kInfDist && d + w < best) ? d + w : best; }
+    __device__ static W relax(W best, W d, W w) { return min(best, sum(d, w)); }
     // Push candidate d + w (unreachable stays unreachable).
-    __device__ static W cand(W du, W w) { return du == kInfDist ? kInfDist : du + w; }
+    __device__ static W cand(W du, W w) { return sum(du, w); }
     __device__ static bool lowers(W nd, W d) { return nd < d; }
     __device__ static void atomic_lower(W *p, W nd, W) { atomicMin(p, nd); }
     __device__ static W lower_of(W a, W b) { return min(a, b); }
@@ -116,11 +123,10 @@ struct MsspCtl {
     int max_epochs;
     long long m;
     unsigned long long t0;
-    unsigned maxf;                  // largest finite distance of the group (narrow transpose)
+    unsigned maxf;                  // largest finite distance of the group (transpose)
     unsigned maxw;                  // largest finite distance written so far (narrow epochs)
     int w_max;                      // largest edge weight
     int narrow;                     // 16-bit distance words
-    int overflow;                   // 32-bit words: a distance wrapped past INT32_MAX (transpose)
 };
 
 __device__ __forceinline__ int ctl_queue(const MsspCtl *ctl, int c) { return ctl->stop ? 0 : ctl->qlen[c]; }
@@ -621,16 +627,13 @@ __global__ void mssp_transpose(const typename D::W *dist, int32_t n, int nsrc, i
     __shared__ int32_t tile[TV][K + 1];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
     unsigned mx = 0;
-    bool wrapped = false;
     for (int64_t vb = (int64_t)blockIdx.x * TV; vb < n; vb += (int64_t)gridDim.x * TV) {
         for (int r = ty; r < TV; r += 8) {
             const int64_t v = vb + r;
             for (int c = tx; c < KW; c += 32) {
                 const typename D::W x = v < n ? dist[(size_t)v * KW + c] : D::kInfWord;
                 if constexpr (D::kPer == 1) {
-                    // Sums of non-negative weights only fall, so a wrapped
-                    // one stays negative to the end.
-                    wrapped |= (int32_t)x < 0;
+                    if (x != kInfDist) mx = max(mx, (unsigned)x);
                     tile[r][c] = x;
                 } else {
 #pragma unroll
@@ -652,12 +655,8 @@ __global__ void mssp_transpose(const typename D::W *dist, int32_t n, int nsrc, i
         }
         __syncthreads();
     }
-    if constexpr (D::kPer == 2) {
-        mx = __reduce_max_sync(kFull, mx);
-        if (tx == 0 && mx) atomicMax(&ctl->maxf, mx);
-    } else {
-        if (__any_sync(kFull, wrapped) && tx == 0) ctl->overflow = 1;
-    }
+    mx = __reduce_max_sync(kFull, mx);
+    if (tx == 0 && mx) atomicMax(&ctl->maxf, mx);
 }
 
 template <class D>
@@ -789,13 +788,14 @@ hc_status run_group(hc_graph *g, const int32_t *h_src, int k, int32_t *dst, int 
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
         *fits = (int64_t)hctl->maxf + g->w_max < (int64_t)kInf16;
     } else if (dst && (int64_t)g->w_max * std::max<int64_t>(g->n_active - 1, 0) >= (int64_t)kInfDist) {
-        // A path of n_active - 1 largest weights could pass INT32_MAX: read
-        // the transpose's wrap flag.
+        // Candidates are clamped at INT32_MAX; when a path of n_active - 1
+        // largest weights could reach the clamp, the group's largest finite
+        // distance (from the transpose) must stay w_max below it.
         HC_CUDA_TRY(cudaMemcpyAsync(hctl, b.ctl, sizeof(MsspCtl), cudaMemcpyDeviceToHost, g->stream));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        if (hctl->overflow)
-            return fail(HC_ERR_UNSUPPORTED, "hc_sssp_batched: a distance exceeds INT32_MAX (largest weight %d)",
-                        g->w_max);
+        if ((int64_t)hctl->maxf + g->w_max >= (int64_t)kInfDist)
+            return fail(HC_ERR_UNSUPPORTED, "hc_sssp_batched: a distance comes within the largest weight (%d) of "
+                        "INT32_MAX: int32 distances cannot hold it", g->w_max);
     }
     return HC_OK;
 }

@@ -121,11 +121,24 @@ __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
                 const int32_t x = a.order[i];
                 const int64_t b = a.index[x], e = a.index[x + 1];
                 float sum = 0.0f;
-                for (int64_t c = b; c < e; c += 32) {
-                    float t = 0.0f;
-                    if (c + lane < e) t = __ldcg(&a.gv[a.nbr[c + lane]]);
-                    const int k = (int)min((int64_t)32, e - c);
-                    for (int q = 0; q < k; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t, q));
+                // Full 32-term chunks: the shuffles take constant lanes and
+                // issue ahead of the add chain, so a chunk costs its 32
+                // dependent adds; the next chunk's gathers are issued before
+                // this one is summed.
+                const int64_t full_end = b + ((e - b) & ~(int64_t)31);
+                float t = 0.0f;
+                if (b < full_end) t = __ldcg(&a.gv[a.nbr[b + lane]]);
+                for (int64_t c = b; c < full_end; c += 32) {
+                    float tn = 0.0f;
+                    if (c + 32 < full_end) tn = __ldcg(&a.gv[a.nbr[c + 32 + lane]]);
+#pragma unroll
+                    for (int q = 0; q < 32; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t, q));
+                    t = tn;
+                }
+                if (full_end < e) {
+                    const float tr = full_end + lane < e ? __ldcg(&a.gv[a.nbr[full_end + lane]]) : 0.0f;
+                    const int k = (int)(e - full_end);
+                    for (int q = 0; q < k; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, tr, q));
                 }
                 const float nv = __fadd_rn(base, __fmul_rn(a.damping, sum));
                 const float old = __ldcg(&a.score[x]);

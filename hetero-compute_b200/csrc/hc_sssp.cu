@@ -76,6 +76,15 @@ struct SsspArgs {
     int max_epochs;
 };
 
+// dist + w for a distance and a weight in [0, INT32_MAX], clamped at
+// INT32_MAX (unreachable): the sum never wraps, and a candidate that reaches
+// the clamp lowers nothing.  Callers check afterwards that no distance came
+// within the largest weight of the clamp.
+__device__ __forceinline__ int32_t sat_add(int32_t d, int32_t w) {
+    const uint32_t s = (uint32_t)d + (uint32_t)w;
+    return s < (uint32_t)kInfDist ? (int32_t)s : kInfDist;
+}
+
 // Push relaxation visitor: nd = dist[u] + w; lower dist[v] with atomicMin and
 // queue v once per epoch (near) or once per phase (far), by raising a stamp.
 struct RelaxVisit {
@@ -96,7 +105,7 @@ struct RelaxVisit {
     };
     __device__ __forceinline__ void load(Item &it, int32_t u, int64_t e) {
         it.v = nbr[e];
-        it.nd = __ldcg(dist + u) + w[e];
+        it.nd = sat_add(__ldcg(dist + u), w[e]);
     }
     __device__ __forceinline__ void probe(Item &it) { it.dv = __ldcg(dist + it.v); }
     // Stages across the round's items: all atomicMins in flight, then all
@@ -136,8 +145,7 @@ struct RelaxVisit {
 // and the row that lowered it is marked changed and relaxed again next epoch;
 // the grid barrier's fence invalidates L1 between epochs.
 __device__ __forceinline__ int32_t pull_val(const SsspArgs &a, int64_t e) {
-    const int32_t du = __ldca(a.dist + a.nbr[e]);
-    return du == kInfDist ? kInfDist : du + a.w[e];
+    return sat_add(__ldca(a.dist + a.nbr[e]), a.w[e]);
 }
 
 // One Bellman-Ford pull over every row with edges (the reference's epoch,
@@ -586,7 +594,7 @@ __global__ void sssp_parents_fill(const int64_t *index, const int32_t *nbr, cons
         const int64_t b = index[u], e = index[u + 1];
         for (int64_t i = b + lane; i < e; i += 32) {
             const int32_t v = nbr[i];
-            if (v != src && du + w[i] == dist[v]) parent[v] = u;
+            if (v != src && sat_add(du, w[i]) == dist[v]) parent[v] = u;
         }
     }
 }
@@ -600,13 +608,18 @@ __global__ void count_finite(const int32_t *dist, int32_t n, unsigned long long 
     if (threadIdx.x == 0 && c) atomicAdd(out, c);
 }
 
-// Distances are int32 sums of non-negative weights.  A sum past INT32_MAX
-// wraps to a negative value, and a relaxation only ever lowers a distance, so
-// the run overflowed exactly when some final distance is negative.
-__global__ void any_negative(const int32_t *dist, int32_t n, int *flag) {
-    bool neg = false;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) neg |= dist[i] < 0;
-    if (__any_sync(kFull, neg) && (threadIdx.x & 31) == 0) *flag = 1;
+// Candidates are clamped at INT32_MAX (sat_add).  When every finite
+// distance plus the largest weight stays below the clamp, no candidate
+// reached it, so the clamp changed nothing; otherwise some distance may lie
+// beyond int32 and the run is refused.  Sets *flag when a finite distance
+// exceeds `limit` (INT32_MAX - 1 - largest weight).
+__global__ void any_above(const int32_t *dist, int32_t n, int32_t limit, int *flag) {
+    bool hi = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t d = dist[i];
+        hi |= d != kInfDist && d > limit;
+    }
+    if (__any_sync(kFull, hi) && (threadIdx.x & 31) == 0) *flag = 1;
 }
 
 // Whether any weight is negative (flags[0]), the largest weight (flags[1])
@@ -794,12 +807,14 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
 
     HC_TRY(g->pinned.ensure(sizeof(SsspCtl)));
     volatile int *h_flags = g->pinned.as<int>();
-    // Overflow is possible only when a path of n_active - 1 edges of the
-    // largest weight can pass INT32_MAX; then each source's distances are
-    // checked after its run (a flag in the control block's spare half).
+    // Candidates can reach the INT32_MAX clamp only when a path of
+    // n_active - 1 edges of the largest weight can; then each source's
+    // distances are checked after its run (a flag in the control block's
+    // spare half).
     static_assert(sizeof(SsspCtl) <= 2048, "SsspCtl overlaps its spare slots");
-    const bool check_overflow = (int64_t)g->w_max * std::max<int64_t>(g->n_active - 1, 0) >= (int64_t)kInfDist;
-    int *neg_flag = (int *)((char *)a.ctl + 2056);
+    const bool check_range = (int64_t)g->w_max * std::max<int64_t>(g->n_active - 1, 0) >= (int64_t)kInfDist;
+    const int32_t range_limit = kInfDist - 1 - g->w_max;
+    int *range_flag = (int *)((char *)a.ctl + 2056);
     double total_ms = 0;
     for (int32_t i = 0; i < num_sources; i++) {
         a.src = src[i];
@@ -822,11 +837,11 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
             HC_TRY(pipe.release(i, dst));
         }
         SsspCtl c;
-        int negative = 0;
-        if (check_overflow) {
-            HC_CUDA_TRY(cudaMemsetAsync(neg_flag, 0, sizeof(int), g->stream));
-            { any_negative<<<g->sm_count * 4, 256, 0, g->stream>>>(a.dist, g->N, neg_flag); ::hc::count_launch(); }
-            HC_CUDA_TRY(cudaMemcpyAsync(&negative, neg_flag, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+        int out_of_range = 0;
+        if (check_range) {
+            HC_CUDA_TRY(cudaMemsetAsync(range_flag, 0, sizeof(int), g->stream));
+            { any_above<<<g->sm_count * 4, 256, 0, g->stream>>>(a.dist, g->N, range_limit, range_flag); ::hc::count_launch(); }
+            HC_CUDA_TRY(cudaMemcpyAsync(&out_of_range, range_flag, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
         }
         HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
         if (o.collect_stats && stats) {
@@ -841,9 +856,9 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
         if (c.gs.err) return fail((hc_status)c.gs.err, "hc_sssp: device run from source %d ended with status %d",
                                   src[i], c.gs.err);
-        if (negative)
-            return fail(HC_ERR_UNSUPPORTED, "hc_sssp: a distance from source %d exceeds INT32_MAX (int32 "
-                        "distances; largest weight %d)", src[i], g->w_max);
+        if (out_of_range)
+            return fail(HC_ERR_UNSUPPORTED, "hc_sssp: a distance from source %d comes within the largest weight "
+                        "(%d) of INT32_MAX: int32 distances cannot hold it", src[i], g->w_max);
         float ms = 0;
         HC_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_start, g->ev_stop));
         total_ms += ms;

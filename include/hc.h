@@ -231,12 +231,14 @@ typedef struct hc_sssp_stats {
 
 /* Single-source shortest paths over int32 weights (graph wtype HC_W_I32).
  * dist_out: [num_sources][num_nodes] int32, INT32_MAX = unreachable.
- * Distances are int32: when a path of num_active - 1 edges of the largest
- * weight could pass INT32_MAX, each source's distances are checked after its
- * run: a distance above INT32_MAX returns HC_ERR_UNSUPPORTED (one of exactly
- * INT32_MAX reads as unreachable).  The reference's float distances lose
- * integer exactness above 2^24 instead (src/kernels/gpu/sssp.cuh:120-281).
- * hc_sssp_batched checks its 32-bit groups the same way.
+ * Distances are int32 and every candidate dist + w is clamped at INT32_MAX:
+ * when a path of num_active - 1 edges of the largest weight could reach the
+ * clamp, each source's distances are checked after its run, and a finite
+ * distance within the largest weight of INT32_MAX (where a clamped candidate
+ * could have hidden a longer one) returns HC_ERR_UNSUPPORTED.  The
+ * reference's float distances lose integer exactness above 2^24 instead
+ * (src/kernels/gpu/sssp.cuh:120-281).  hc_sssp_batched checks its 32-bit
+ * groups the same way.
  * parent_out (optional): a shortest-path tree, parent[src] = src.
  * Replaces sssp_pull_gpu (src/kernels/gpu/sssp.cuh:42-100). */
 hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_sources,

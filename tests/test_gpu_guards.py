@@ -27,25 +27,30 @@ def _path(weights):
 
 
 def test_sssp_int32_overflow_is_reported():
-    index, nbr, w = _path([2**30, 2**30])  # distance 2^31 does not fit
+    """Candidates clamp at INT32_MAX; a run whose distances come within the largest weight of it is refused
+    (there a clamped candidate may have hidden a longer distance), one that stays below is exact."""
+    for weights in ([2**30, 2**30], [2**30 - 1, 2**30 - 1, 1], [2**29, 2**29, 2**29, 2**29]):
+        index, nbr, w = _path(weights)
+        g = hc.Graph(index, nbr, w)
+        with pytest.raises(hc.HCError) as e:
+            g.sssp([0])
+        assert e.value.status == hc.UNSUPPORTED
+        with pytest.raises(hc.HCError) as e:
+            g.sssp_batched(np.array([0, 1], dtype=np.int32))
+        assert e.value.status == hc.UNSUPPORTED
+    index, nbr, w = _path([2**29, 2**29, 2**28, 5])  # largest distance 2^30 + 2^28 + 5, + 2^29 < INT32_MAX
     g = hc.Graph(index, nbr, w)
-    with pytest.raises(hc.HCError) as e:
-        g.sssp([0])
-    assert e.value.status == hc.UNSUPPORTED
-    with pytest.raises(hc.HCError) as e:
-        g.sssp_batched(np.array([0, 1], dtype=np.int32))
-    assert e.value.status == hc.UNSUPPORTED
-    index, nbr, w = _path([2**30 - 1, 2**30 - 1, 1])  # 2^31 - 1 = INT32_MAX: reads as unreachable
-    g = hc.Graph(index, nbr, w)
-    d, _, _ = g.sssp([0])
-    assert list(d[0]) == [0, 2**30 - 1, 2**31 - 2, INT32_MAX]
-    db, _ = g.sssp_batched(np.array([0], dtype=np.int32))
-    assert np.array_equal(db[0], d[0])
+    d, _, _ = g.sssp([0, 4])
+    far = 2**30 + 2**28 + 5
+    assert list(d[0]) == [0, 2**29, 2**30, 2**30 + 2**28, far]
+    assert list(d[1]) == [far, 2**29 + 2**28 + 5, 2**28 + 5, 5, 0]
+    db, _ = g.sssp_batched(np.array([0, 4], dtype=np.int32))
+    assert np.array_equal(db, d)
 
 
 def test_sssp_large_weights_below_the_limit_are_exact():
     host = hc.gen_kronecker(10, 8, 5, wtype=hc.W_I32)
-    w = (host.weights.astype(np.int64) * 2**22).astype(np.int32)  # up to 255 * 2^22 < 2^30
+    w = (host.weights.astype(np.int64) * 2**20).astype(np.int32)  # up to 255 * 2^20: the range check runs
     g = hc.Graph(host.index, host.neighbors, w)
     src = hc.pick_sources(host, 3)
     d, _, _ = g.sssp(src)  # the overflow check runs (w_max * (n - 1) >= INT32_MAX) and finds nothing
