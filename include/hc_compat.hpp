@@ -49,6 +49,10 @@ struct wnode_t {
 };
 
 namespace hc_compat {
+inline void check(hc_status s, const char *what);
+}
+inline void hc_compat_dev_alloc(void **p, size_t bytes);
+namespace hc_compat {
 inline void check(hc_status s, const char *what) {
     if (s != HC_OK) {
         std::cerr << "[" << what << "] " << hc_status_string(s) << ": " << hc_last_error() << std::endl;
@@ -62,6 +66,10 @@ inline nid_t target<nid_t>(const nid_t &x) { return x; }
 template <>
 inline nid_t target<wnode_t>(const wnode_t &x) { return x.v; }
 }  // namespace hc_compat
+
+inline void hc_compat_dev_alloc(void **p, size_t bytes) {
+    hc_compat::check(hc_dev_malloc(p, bytes, 0), "hc_dev_malloc");
+}
 
 template <typename NeighborT>
 class GenericCSRGraph {
@@ -86,6 +94,14 @@ public:
         delete[] index;
         delete[] neighbors;
     }
+    // The range of nid's neighbours, iterable as the reference's
+    // (src/graph.cuh:60-80: `for (wnode_t nei : g.get_neighbors(v))`).
+    struct Neighborhood {
+        const NeighborT *first, *last;
+        const NeighborT *begin() const { return first; }
+        const NeighborT *end() const { return last; }
+    };
+    Neighborhood get_neighbors(nid_t nid) const { return {neighbors + index[nid], neighbors + index[nid + 1]}; }
     offset_t get_degree(nid_t nid) const { return index[nid + 1] - index[nid]; }
     bool has_self_cycle(nid_t nid) const {
         for (offset_t i = index[nid]; i < index[nid + 1]; i++)
@@ -143,48 +159,245 @@ private:
     std::uniform_int_distribution<nid_t> dist_;
 };
 
-// ---------------------------------------------------------------- kernels
-
-struct hc_epoch_kernel {
-    hc_variant variant;
-    bool engine;  // true: this library's device-driven path
-    const char *name;
-    int sync_iters;  // > 0: the sync-warp BFS epoch probing that many chunks per vote
+// ----------------------------------------------------------------- Bitmap
+// The reference's Bitmap (src/bitmap.cuh:14-191): the struct layout and the
+// functions epoch kernels and drivers call.  Host functions are plain C++ over
+// the C ABI's memory helpers; get_bit / set_bit are host-and-device and
+// cu_set_bit_atomic device-only under nvcc, so epoch kernels a caller writes
+// against the reference's API compile unchanged.
+#ifdef __CUDACC__
+#define HC_COMPAT_HD __host__ __device__
+#else
+#define HC_COMPAT_HD
+#endif
+namespace Bitmap {
+using data_t = int;
+const std::size_t data_size = sizeof(data_t) * 8;
+HC_COMPAT_HD inline std::size_t data_offset(std::size_t n) { return n / data_size; }
+HC_COMPAT_HD inline std::size_t bit_offset(std::size_t n) { return n & (data_size - 1); }
+struct Bitmap {
+    data_t *buffer;
+    bool using_cuda;
+    std::size_t size;  // words
 };
-using bfs_gpu_epoch_func = const hc_epoch_kernel *;
-using sssp_gpu_epoch_func = const hc_epoch_kernel *;
-using pr_gpu_epoch_func = const hc_epoch_kernel *;
+HC_COMPAT_HD inline void set_bit(Bitmap *const b, const std::size_t idx) {
+    b->buffer[data_offset(idx)] |= static_cast<data_t>(1) << bit_offset(idx);
+}
+HC_COMPAT_HD inline bool get_bit(const Bitmap *const b, const std::size_t idx) {
+    return (b->buffer[data_offset(idx)] >> bit_offset(idx)) & static_cast<data_t>(1);
+}
+#ifdef __CUDACC__
+__device__ inline void cu_set_bit_atomic(Bitmap *const b, const std::size_t idx) {
+    atomicOr(b->buffer + data_offset(idx), static_cast<data_t>(1) << bit_offset(idx));
+}
+#endif
+inline void set_bit_atomic(Bitmap *const b, const std::size_t idx) {
+    __atomic_fetch_or(&b->buffer[data_offset(idx)], static_cast<data_t>(1) << bit_offset(idx), __ATOMIC_RELAXED);
+}
+inline void reset(Bitmap *const b) { std::fill(b->buffer, b->buffer + b->size, 0); }
+inline bool copy(const Bitmap *const from, Bitmap *const to) {
+    if (from->size != to->size) return false;
+    std::copy(from->buffer, from->buffer + from->size, to->buffer);
+    return true;
+}
+// Host bitmap (use_cuda: its buffer in device memory instead, as the
+// reference's pinned-or-device variants are used by its drivers).
+inline Bitmap *constructor(const std::size_t num_elements, const bool use_cuda = false) {
+    Bitmap *b = new Bitmap{nullptr, use_cuda, (num_elements + data_size - 1) / data_size};
+    if (use_cuda) {
+        hc_compat_dev_alloc((void **)&b->buffer, b->size * sizeof(data_t));
+        hc_dev_memset(b->buffer, 0, b->size * sizeof(data_t));
+    } else {
+        b->buffer = new data_t[b->size];
+        reset(b);
+    }
+    return b;
+}
+inline void destructor(Bitmap **const b) {
+    if ((*b)->using_cuda) hc_dev_free((*b)->buffer);
+    else delete[] (*b)->buffer;
+    delete *b;
+    *b = nullptr;
+}
+// Host proxy of a device buffer (src/bitmap.cuh:122-160).
+inline Bitmap *cu_cpu_constructor(const std::size_t num_elements) { return constructor(num_elements, true); }
+inline void cu_cpu_destructor(Bitmap **const b) { destructor(b); }
+inline void cu_cpu_reset(Bitmap *const b) { hc_dev_memset(b->buffer, 0, b->size * sizeof(data_t)); }
+inline void cu_cpu_set_bit(Bitmap *const b, const std::size_t idx) {
+    data_t w = 0;
+    hc_memcpy(&w, b->buffer + data_offset(idx), sizeof(w));
+    w |= static_cast<data_t>(1) << bit_offset(idx);
+    hc_memcpy(b->buffer + data_offset(idx), &w, sizeof(w));
+}
+// The struct itself in device memory (src/bitmap.cuh:165-183).
+inline Bitmap *cu_constructor(const Bitmap *const b) {
+    Bitmap *d = nullptr;
+    hc_compat_dev_alloc((void **)&d, sizeof(Bitmap));
+    hc_memcpy(d, b, sizeof(Bitmap));
+    return d;
+}
+inline void cu_destructor(Bitmap **const d) {
+    hc_dev_free(*d);
+    *d = nullptr;
+}
+}  // namespace Bitmap
 
-inline const hc_epoch_kernel hc_k_bfs_one[] = {{HC_VARIANT_THREAD, false, "bfs_gpu_onetoone"}};
-inline const hc_epoch_kernel hc_k_bfs_warp[] = {{HC_VARIANT_WARP, false, "bfs_gpu_warp"}};
-inline const hc_epoch_kernel hc_k_bfs_auto[] = {{HC_VARIANT_AUTO, true, "bfs_gpu_auto"}};
-inline const hc_epoch_kernel hc_k_sssp_one[] = {{HC_VARIANT_THREAD, false, "sssp_gpu_onetoone"}};
-inline const hc_epoch_kernel hc_k_sssp_warp[] = {{HC_VARIANT_WARP, false, "sssp_gpu_warp_red"}};
-inline const hc_epoch_kernel hc_k_sssp_block[] = {{HC_VARIANT_BLOCK, false, "sssp_gpu_block_red"}};
-inline const hc_epoch_kernel hc_k_sssp_auto[] = {{HC_VARIANT_AUTO, true, "sssp_gpu_auto"}};
-inline const hc_epoch_kernel hc_k_pr_one[] = {{HC_VARIANT_THREAD, false, "pr_gpu_onetoone"}};
-inline const hc_epoch_kernel hc_k_pr_warp[] = {{HC_VARIANT_WARP, false, "pr_gpu_warp_red"}};
-inline const hc_epoch_kernel hc_k_pr_block[] = {{HC_VARIANT_BLOCK, false, "pr_gpu_block_red"}};
-inline const hc_epoch_kernel hc_k_pr_auto[] = {{HC_VARIANT_AUTO, true, "pr_gpu_auto"}};
+// ---------------------------------------------------------------- kernels
+// Epoch-kernel types with the reference's signatures
+// (src/kernels/kernel_types.cuh:36-63).
+typedef void (*sssp_gpu_epoch_func)(const offset_t *, const wnode_t *, const nid_t, const nid_t, weight_t *, nid_t *);
+typedef void (*pr_gpu_epoch_func)(const offset_t *, const wnode_t *, const nid_t, const nid_t, weight_t *, nid_t *,
+                                  int, offset_t *);
+typedef void (*bfs_gpu_epoch_func)(const offset_t *const, const nid_t *const, nid_t *const, const nid_t,
+                                   const nid_t, const Bitmap::Bitmap *const, Bitmap::Bitmap *const, nid_t *const);
 
-// Reference kernel names (src/kernels/gpu/*.cuh).
-inline const bfs_gpu_epoch_func epoch_bfs_pull_gpu_one_to_one = hc_k_bfs_one;
-inline const bfs_gpu_epoch_func epoch_bfs_pull_gpu_warp = hc_k_bfs_warp;
-// epoch_bfs_sync_pull_gpu_warp<sync_iters> (src/kernels/gpu/bfs.cuh:234-288),
-// spelled as the reference's callers spell it (`epoch_bfs_sync_pull_gpu_warp<2>`).
+// The reference's kernel names are functions of those types.  A driver given
+// one runs this library's epoch of that granularity (hc_epoch_*), in the
+// reference's host loop; the *_auto names run this engine's device-driven
+// paths.  Called directly (device pointers, Bitmap structs in host or device
+// memory), a name runs one epoch with the drivers' default launch shape.
+// Any other function of the same type is taken to be the caller's own
+// __global__ epoch kernel: under nvcc the drivers launch it with <<<...>>>
+// exactly as the reference's drivers do; elsewhere it is refused.
+namespace hc_compat {
+constexpr int kDefaultBlocks = 64, kDefaultThreads = 1024;
+inline Bitmap::Bitmap read_bitmap(const Bitmap::Bitmap *b) {
+    Bitmap::Bitmap h{};
+    check(hc_memcpy(&h, b, sizeof(h)), "hc_memcpy");
+    return h;
+}
+inline void bfs_epoch(hc_variant v, int sync_iters, const offset_t *index, const nid_t *nbr, nid_t *parents,
+                      nid_t start, nid_t end, const Bitmap::Bitmap *f, Bitmap::Bitmap *nf, nid_t *count) {
+    const Bitmap::Bitmap hf = read_bitmap(f), hnf = read_bitmap(nf);
+    if (sync_iters > 0)
+        check(hc_epoch_bfs_sync_pull(index, nbr, parents, start, end, (const uint32_t *)hf.buffer,
+                                     (uint32_t *)hnf.buffer, count, sync_iters, kDefaultBlocks, kDefaultThreads,
+                                     nullptr), "hc_epoch_bfs_sync_pull");
+    else
+        check(hc_epoch_bfs_pull(index, nbr, parents, start, end, (const uint32_t *)hf.buffer, (uint32_t *)hnf.buffer,
+                                count, v, kDefaultBlocks, kDefaultThreads, nullptr), "hc_epoch_bfs_pull");
+}
+}  // namespace hc_compat
+
+inline void epoch_sssp_pull_gpu_one_to_one(const offset_t *i, const wnode_t *n, const nid_t s, const nid_t e,
+                                           weight_t *d, nid_t *u) {
+    hc_compat::check(hc_epoch_sssp_pull(i, n, s, e, d, u, HC_VARIANT_THREAD, 64, 1024, nullptr), "hc_epoch_sssp_pull");
+}
+inline void epoch_sssp_pull_gpu_warp_red(const offset_t *i, const wnode_t *n, const nid_t s, const nid_t e,
+                                         weight_t *d, nid_t *u) {
+    hc_compat::check(hc_epoch_sssp_pull(i, n, s, e, d, u, HC_VARIANT_WARP, 64, 1024, nullptr), "hc_epoch_sssp_pull");
+}
+inline void epoch_sssp_pull_gpu_block_red(const offset_t *i, const wnode_t *n, const nid_t s, const nid_t e,
+                                          weight_t *d, nid_t *u) {
+    hc_compat::check(hc_epoch_sssp_pull(i, n, s, e, d, u, HC_VARIANT_BLOCK, 64, 256, nullptr), "hc_epoch_sssp_pull");
+}
+inline void epoch_sssp_auto(const offset_t *i, const wnode_t *n, const nid_t s, const nid_t e, weight_t *d,
+                            nid_t *u) {
+    epoch_sssp_pull_gpu_warp_red(i, n, s, e, d, u);  // as an epoch: the warp variant
+}
+inline void epoch_pr_pull_gpu_one_to_one(const offset_t *i, const wnode_t *n, const nid_t s, const nid_t e,
+                                         weight_t *x, nid_t *u, int nn, offset_t *deg) {
+    hc_compat::check(hc_epoch_pr_pull(i, n, s, e, x, u, nn, deg, HC_VARIANT_THREAD, 64, 1024, nullptr),
+                     "hc_epoch_pr_pull");
+}
+inline void epoch_pr_pull_gpu_warp_red(const offset_t *i, const wnode_t *n, const nid_t s, const nid_t e,
+                                       weight_t *x, nid_t *u, int nn, offset_t *deg) {
+    hc_compat::check(hc_epoch_pr_pull(i, n, s, e, x, u, nn, deg, HC_VARIANT_WARP, 64, 1024, nullptr),
+                     "hc_epoch_pr_pull");
+}
+inline void epoch_pr_pull_gpu_block_red(const offset_t *i, const wnode_t *n, const nid_t s, const nid_t e,
+                                        weight_t *x, nid_t *u, int nn, offset_t *deg) {
+    hc_compat::check(hc_epoch_pr_pull(i, n, s, e, x, u, nn, deg, HC_VARIANT_BLOCK, 64, 256, nullptr),
+                     "hc_epoch_pr_pull");
+}
+inline void epoch_pr_auto(const offset_t *i, const wnode_t *n, const nid_t s, const nid_t e, weight_t *x, nid_t *u,
+                          int nn, offset_t *deg) {
+    epoch_pr_pull_gpu_one_to_one(i, n, s, e, x, u, nn, deg);
+}
+inline void epoch_bfs_pull_gpu_one_to_one(const offset_t *const i, const nid_t *const n, nid_t *const p,
+                                          const nid_t s, const nid_t e, const Bitmap::Bitmap *const f,
+                                          Bitmap::Bitmap *const nf, nid_t *const c) {
+    hc_compat::bfs_epoch(HC_VARIANT_THREAD, 0, i, n, p, s, e, f, nf, c);
+}
+inline void epoch_bfs_pull_gpu_warp(const offset_t *const i, const nid_t *const n, nid_t *const p, const nid_t s,
+                                    const nid_t e, const Bitmap::Bitmap *const f, Bitmap::Bitmap *const nf,
+                                    nid_t *const c) {
+    hc_compat::bfs_epoch(HC_VARIANT_WARP, 0, i, n, p, s, e, f, nf, c);
+}
+// epoch_bfs_sync_pull_gpu_warp<sync_iters> (src/kernels/gpu/bfs.cuh:234-288):
+// callers name it with or without the template argument, as the reference's do
+// (tests/bfs/bfs_verify.cu, profile/bfs/benchmark_bfs.cu:242-260).
 template <offset_t sync_iters = 1>
-inline const hc_epoch_kernel hc_k_bfs_sync[] = {{HC_VARIANT_WARP, false, "bfs_gpu_sync_warp", (int)sync_iters}};
-template <offset_t sync_iters = 1>
-inline const bfs_gpu_epoch_func epoch_bfs_sync_pull_gpu_warp = hc_k_bfs_sync<sync_iters>;
-inline const bfs_gpu_epoch_func epoch_bfs_auto = hc_k_bfs_auto;
-inline const sssp_gpu_epoch_func epoch_sssp_pull_gpu_one_to_one = hc_k_sssp_one;
-inline const sssp_gpu_epoch_func epoch_sssp_pull_gpu_warp_red = hc_k_sssp_warp;
-inline const sssp_gpu_epoch_func epoch_sssp_pull_gpu_block_red = hc_k_sssp_block;
-inline const sssp_gpu_epoch_func epoch_sssp_auto = hc_k_sssp_auto;
-inline const pr_gpu_epoch_func epoch_pr_pull_gpu_one_to_one = hc_k_pr_one;
-inline const pr_gpu_epoch_func epoch_pr_pull_gpu_warp_red = hc_k_pr_warp;
-inline const pr_gpu_epoch_func epoch_pr_pull_gpu_block_red = hc_k_pr_block;
-inline const pr_gpu_epoch_func epoch_pr_auto = hc_k_pr_auto;
+inline void epoch_bfs_sync_pull_gpu_warp(const offset_t *const i, const nid_t *const n, nid_t *const p,
+                                         const nid_t s, const nid_t e, const Bitmap::Bitmap *const f,
+                                         Bitmap::Bitmap *const nf, nid_t *const c) {
+    static_assert(sync_iters >= 1, "sync_iters must be at least 1");
+    hc_compat::bfs_epoch(HC_VARIANT_WARP, (int)sync_iters, i, n, p, s, e, f, nf, c);
+}
+inline void epoch_bfs_auto(const offset_t *const i, const nid_t *const n, nid_t *const p, const nid_t s,
+                           const nid_t e, const Bitmap::Bitmap *const f, Bitmap::Bitmap *const nf, nid_t *const c) {
+    hc_compat::bfs_epoch(HC_VARIANT_THREAD, 0, i, n, p, s, e, f, nf, c);
+}
+
+namespace hc_compat {
+// What a driver does with a kernel name: this library's epoch of a
+// granularity, the engine path, or (not found) the caller's own kernel.
+struct KernelInfo {
+    hc_variant variant;
+    bool engine;
+    int sync_iters;
+    const char *name;
+};
+constexpr int kMaxSyncIters = 8;
+template <int K>
+inline void add_sync(std::vector<std::pair<bfs_gpu_epoch_func, KernelInfo>> &v) {
+    if constexpr (K >= 1) {
+        add_sync<K - 1>(v);
+        static const std::string name = "bfs_gpu_sync_warp_" + std::to_string(K);
+        v.push_back({&epoch_bfs_sync_pull_gpu_warp<K>, {HC_VARIANT_WARP, false, K, name.c_str()}});
+    }
+}
+inline const KernelInfo *lookup(bfs_gpu_epoch_func f) {
+    static const std::vector<std::pair<bfs_gpu_epoch_func, KernelInfo>> table = [] {
+        std::vector<std::pair<bfs_gpu_epoch_func, KernelInfo>> v = {
+            {&epoch_bfs_pull_gpu_one_to_one, {HC_VARIANT_THREAD, false, 0, "bfs_gpu_onetoone"}},
+            {&epoch_bfs_pull_gpu_warp, {HC_VARIANT_WARP, false, 0, "bfs_gpu_warp"}},
+            {&epoch_bfs_auto, {HC_VARIANT_AUTO, true, 0, "bfs_gpu_auto"}}};
+        add_sync<kMaxSyncIters>(v);
+        return v;
+    }();
+    for (auto &e : table)
+        if (e.first == f) return &e.second;
+    return nullptr;
+}
+inline const KernelInfo *lookup(sssp_gpu_epoch_func f) {
+    static const std::pair<sssp_gpu_epoch_func, KernelInfo> table[] = {
+        {&epoch_sssp_pull_gpu_one_to_one, {HC_VARIANT_THREAD, false, 0, "sssp_gpu_onetoone"}},
+        {&epoch_sssp_pull_gpu_warp_red, {HC_VARIANT_WARP, false, 0, "sssp_gpu_warp_red"}},
+        {&epoch_sssp_pull_gpu_block_red, {HC_VARIANT_BLOCK, false, 0, "sssp_gpu_block_red"}},
+        {&epoch_sssp_auto, {HC_VARIANT_AUTO, true, 0, "sssp_gpu_auto"}}};
+    for (auto &e : table)
+        if (e.first == f) return &e.second;
+    return nullptr;
+}
+inline const KernelInfo *lookup(pr_gpu_epoch_func f) {
+    static const std::pair<pr_gpu_epoch_func, KernelInfo> table[] = {
+        {&epoch_pr_pull_gpu_one_to_one, {HC_VARIANT_THREAD, false, 0, "pr_gpu_onetoone"}},
+        {&epoch_pr_pull_gpu_warp_red, {HC_VARIANT_WARP, false, 0, "pr_gpu_warp_red"}},
+        {&epoch_pr_pull_gpu_block_red, {HC_VARIANT_BLOCK, false, 0, "pr_gpu_block_red"}},
+        {&epoch_pr_auto, {HC_VARIANT_AUTO, true, 0, "pr_gpu_auto"}}};
+    for (auto &e : table)
+        if (e.first == f) return &e.second;
+    return nullptr;
+}
+// A caller's own kernel (not one of the names above): launched as the
+// reference's drivers launch theirs, when compiled by nvcc.
+[[noreturn]] inline void no_user_kernels(const char *who) {
+    std::cerr << "[" << who << "] the epoch kernel is not one of this library's names; a kernel of your own "
+              << "needs this header compiled by nvcc" << std::endl;
+    std::exit(EXIT_FAILURE);
+}
+}  // namespace hc_compat
 
 enum class BFSGPU { one_to_one, warp, automatic, undefined };
 enum class SSSPGPU { one_to_one, warp_red, block_red, automatic, undefined };
@@ -227,12 +440,13 @@ inline pr_gpu_epoch_func get_kernel(PRGPU k) {
 template <class E>
 inline std::string to_repr(E k) {
     auto f = get_kernel(k);
-    return f ? f->name : "";
+    const hc_compat::KernelInfo *i = f ? hc_compat::lookup(f) : nullptr;
+    return i ? i->name : "";
 }
 template <class E>
 inline std::string to_string(E k) {
-    auto f = get_kernel(k);
-    return f ? std::string("GPU ") + f->name : "undefined GPU kernel";
+    const std::string r = to_repr(k);
+    return r.empty() ? "undefined GPU kernel" : "GPU " + r;
 }
 
 // ---------------------------------------------------------------- drivers
@@ -255,9 +469,13 @@ inline double bfs_gpu(const CSRUWGraph &g, const nid_t source_id, nid_t **const 
                       bfs_gpu_epoch_func epoch_kernel, int block_count = 64, int thread_count = 1024) {
     using namespace hc_compat;
     if (!epoch_kernel) check(HC_ERR_INVALID_ARG, "bfs_gpu: null epoch kernel");
+    const KernelInfo *ki = lookup(epoch_kernel);
+#ifndef __CUDACC__
+    if (!ki) no_user_kernels("bfs_gpu");
+#endif
     nid_t *parents = new nid_t[g.num_nodes];
     double ms = 0;
-    if (epoch_kernel->engine) {
+    if (ki && ki->engine) {
         hc_graph *hg = nullptr;
         check(hc_graph_create(g.index, g.neighbors, nullptr, HC_W_NONE, g.num_nodes, g.num_edges, 0, &hg),
               "hc_graph_create");
@@ -278,26 +496,39 @@ inline double bfs_gpu(const CSRUWGraph &g, const nid_t source_id, nid_t **const 
         check(hc_dev_memset(f0.p, 0, 4 * words), "hc_dev_memset");
         uint32_t bit = 1u << (source_id & 31);
         check(hc_memcpy(f0.as<uint32_t>() + (source_id >> 5), &bit, 4), "hc_memcpy");
-        uint32_t *cur = f0.as<uint32_t>(), *next = f1.as<uint32_t>();
+        // Device Bitmap structs over the two frontier buffers, as the
+        // reference's driver builds them (src/bitmap.cuh:165-183).
+        Bitmap::Bitmap hb[2] = {{f0.as<int>(), true, words}, {f1.as<int>(), true, words}};
+        Bitmap::Bitmap *cb[2] = {Bitmap::cu_constructor(&hb[0]), Bitmap::cu_constructor(&hb[1])};
+        int cur = 0;
         auto t0 = std::chrono::steady_clock::now();
         nid_t found = 0;
         do {
             check(hc_dev_memset(cnt.p, 0, 4), "hc_dev_memset");
-            check(hc_dev_memset(next, 0, 4 * words), "hc_dev_memset");
-            if (epoch_kernel->sync_iters > 0)
+            check(hc_dev_memset(hb[1 - cur].buffer, 0, 4 * words), "hc_dev_memset");
+            if (!ki) {
+#ifdef __CUDACC__
+                (*epoch_kernel)<<<block_count, thread_count>>>(idx.as<offset_t>(), nbr.as<nid_t>(), par.as<nid_t>(), 0,
+                                                              g.num_nodes, cb[cur], cb[1 - cur], cnt.as<nid_t>());
+                check(cudaGetLastError() == cudaSuccess ? HC_OK : HC_ERR_CUDA, "bfs_gpu: epoch launch");
+#endif
+            } else if (ki->sync_iters > 0) {
                 check(hc_epoch_bfs_sync_pull(idx.as<int64_t>(), nbr.as<int32_t>(), par.as<int32_t>(), 0, g.num_nodes,
-                                             cur, next, cnt.as<int32_t>(), epoch_kernel->sync_iters, block_count,
-                                             thread_count, nullptr),
+                                             (const uint32_t *)hb[cur].buffer, (uint32_t *)hb[1 - cur].buffer,
+                                             cnt.as<int32_t>(), ki->sync_iters, block_count, thread_count, nullptr),
                       "hc_epoch_bfs_sync_pull");
-            else
-                check(hc_epoch_bfs_pull(idx.as<int64_t>(), nbr.as<int32_t>(), par.as<int32_t>(), 0, g.num_nodes, cur,
-                                        next, cnt.as<int32_t>(), epoch_kernel->variant, block_count, thread_count,
-                                        nullptr),
+            } else {
+                check(hc_epoch_bfs_pull(idx.as<int64_t>(), nbr.as<int32_t>(), par.as<int32_t>(), 0, g.num_nodes,
+                                        (const uint32_t *)hb[cur].buffer, (uint32_t *)hb[1 - cur].buffer,
+                                        cnt.as<int32_t>(), ki->variant, block_count, thread_count, nullptr),
                       "hc_epoch_bfs_pull");
+            }
             check(hc_memcpy(&found, cnt.p, 4), "hc_memcpy");
-            std::swap(cur, next);
+            cur = 1 - cur;
         } while (found != 0);
         ms = ms_since(t0);
+        Bitmap::cu_destructor(&cb[0]);
+        Bitmap::cu_destructor(&cb[1]);
         check(hc_memcpy(parents, par.p, 4 * (size_t)g.num_nodes), "hc_memcpy");
     }
     *ret_parents = parents;
@@ -309,12 +540,16 @@ inline double sssp_pull_gpu(const CSRWGraph &g, sssp_gpu_epoch_func epoch_kernel
                             weight_t **const ret_dist, int block_count = 64, int thread_count = 1024) {
     using namespace hc_compat;
     if (!epoch_kernel) check(HC_ERR_INVALID_ARG, "sssp_pull_gpu: null epoch kernel");
+    const KernelInfo *ki = lookup(epoch_kernel);
+#ifndef __CUDACC__
+    if (!ki) no_user_kernels("sssp_pull_gpu");
+#endif
     weight_t *dist = new weight_t[g.num_nodes];
     double ms = 0;
     // The engine path needs one source (a single 0, the rest inf) and
     // integer weights; anything else runs the epoch loop.
     nid_t src = -1;
-    bool single = epoch_kernel->engine;
+    bool single = ki && ki->engine;
     for (nid_t i = 0; single && i < g.num_nodes; i++) {
         if (init_dist[i] == 0.0f && src < 0) src = i;
         else if (!std::isinf(init_dist[i])) single = false;
@@ -351,10 +586,18 @@ inline double sssp_pull_gpu(const CSRWGraph &g, sssp_gpu_epoch_func epoch_kernel
         nid_t updated = 1;
         while (updated != 0) {
             check(hc_dev_memset(cnt.p, 0, 4), "hc_dev_memset");
-            check(hc_epoch_sssp_pull(idx.as<int64_t>(), nb.p, 0, g.num_nodes, dd.as<float>(), cnt.as<int32_t>(),
-                                     epoch_kernel->variant == HC_VARIANT_AUTO ? HC_VARIANT_WARP : epoch_kernel->variant,
-                                     block_count, thread_count, nullptr),
-                  "hc_epoch_sssp_pull");
+            if (!ki) {
+#ifdef __CUDACC__
+                (*epoch_kernel)<<<block_count, thread_count>>>(idx.as<offset_t>(), nb.as<wnode_t>(), 0, g.num_nodes,
+                                                              dd.as<weight_t>(), cnt.as<nid_t>());
+                check(cudaGetLastError() == cudaSuccess ? HC_OK : HC_ERR_CUDA, "sssp_pull_gpu: epoch launch");
+#endif
+            } else {
+                check(hc_epoch_sssp_pull(idx.as<int64_t>(), nb.p, 0, g.num_nodes, dd.as<float>(), cnt.as<int32_t>(),
+                                         ki->variant == HC_VARIANT_AUTO ? HC_VARIANT_WARP : ki->variant, block_count,
+                                         thread_count, nullptr),
+                      "hc_epoch_sssp_pull");
+            }
             check(hc_memcpy(&updated, cnt.p, 4), "hc_memcpy");
         }
         ms = ms_since(t0);
@@ -374,9 +617,13 @@ inline double pr_pull_gpu(const CSRWGraph &g, pr_gpu_epoch_func epoch_kernel, we
                           weight_t **const ret_score, int block_count = 64, int thread_count = 1024) {
     using namespace hc_compat;
     if (!epoch_kernel) check(HC_ERR_INVALID_ARG, "pr_pull_gpu: null epoch kernel");
+    const KernelInfo *ki = lookup(epoch_kernel);
+#ifndef __CUDACC__
+    if (!ki) no_user_kernels("pr_pull_gpu");
+#endif
     weight_t *score = new weight_t[g.num_nodes];
     double ms = 0;
-    if (epoch_kernel->engine) {
+    if (ki && ki->engine) {
         std::vector<int32_t> nbr((size_t)g.num_edges);
         for (offset_t i = 0; i < g.num_edges; i++) nbr[i] = g.neighbors[i].v;
         hc_graph *hg = nullptr;
@@ -404,10 +651,18 @@ inline double pr_pull_gpu(const CSRWGraph &g, pr_gpu_epoch_func epoch_kernel, we
         nid_t updated = 1;
         for (int it = 0; updated != 0 && it <= 200; it++) {
             check(hc_dev_memset(cnt.p, 0, 4), "hc_dev_memset");
-            check(hc_epoch_pr_pull(idx.as<int64_t>(), nb.p, 0, g.num_nodes, sc.as<float>(), cnt.as<int32_t>(),
-                                   g.num_nodes, dg.as<int64_t>(), epoch_kernel->variant, block_count, thread_count,
-                                   nullptr),
-                  "hc_epoch_pr_pull");
+            if (!ki) {
+#ifdef __CUDACC__
+                (*epoch_kernel)<<<block_count, thread_count>>>(idx.as<offset_t>(), nb.as<wnode_t>(), 0, g.num_nodes,
+                                                              sc.as<weight_t>(), cnt.as<nid_t>(), g.num_nodes,
+                                                              dg.as<offset_t>());
+                check(cudaGetLastError() == cudaSuccess ? HC_OK : HC_ERR_CUDA, "pr_pull_gpu: epoch launch");
+#endif
+            } else {
+                check(hc_epoch_pr_pull(idx.as<int64_t>(), nb.p, 0, g.num_nodes, sc.as<float>(), cnt.as<int32_t>(),
+                                       g.num_nodes, dg.as<int64_t>(), ki->variant, block_count, thread_count, nullptr),
+                      "hc_epoch_pr_pull");
+            }
             check(hc_memcpy(&updated, cnt.p, 4), "hc_memcpy");
         }
         ms = ms_since(t0);
@@ -415,6 +670,22 @@ inline double pr_pull_gpu(const CSRWGraph &g, pr_gpu_epoch_func epoch_kernel, we
     }
     *ret_score = score;
     return ms;
+}
+
+// The reference's heterogeneous drivers (src/kernels/heterogeneous/*.cuh,
+// generated code that splits vertex segments over CPUs and GPUs and exchanges
+// them peer to peer): here the split collapses to one GPU, and each runs the
+// engine path of its algorithm.  enable_all_peer_access* have nothing to do.
+inline void enable_all_peer_access() {}
+inline void enable_all_peer_access_pr() {}
+inline double bfs_do_heterogeneous(const CSRUWGraph &g, const nid_t source_id, nid_t **const ret_parents) {
+    return bfs_gpu(g, source_id, ret_parents, epoch_bfs_auto);
+}
+inline double sssp_pull_heterogeneous(const CSRWGraph &g, const weight_t *init_dist, weight_t **const ret_dist) {
+    return sssp_pull_gpu(g, epoch_sssp_auto, init_dist, ret_dist);
+}
+inline double pr_pull_heterogeneous(const CSRWGraph &g, const weight_t *init_score, weight_t **const ret_score) {
+    return pr_pull_gpu(g, epoch_pr_auto, const_cast<weight_t *>(init_score), ret_score);
 }
 
 template <class E, class = typename std::enable_if<std::is_enum<E>::value>::type>

@@ -34,3 +34,31 @@ def test_compat_drivers_verify(tmp_path):
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count("success") == 3 + 3 + 4 + 4
+
+
+REF_TESTS = {name: os.path.join(ROOT, "oracle", "_ref", f"{name}_verify") for name in ("bfs", "sssp", "pr")}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["bfs", "sssp", "pr"])
+def test_reference_verify_programs_pass(tmp_path, name):
+    """The reference's own tests/{bfs,sssp,pr}/*_verify.cu, compiled unchanged against include/hc_compat.hpp
+    (oracle/Makefile `compat`: its GPU driver headers replaced, its CPU kernels as they are), run on a Kronecker
+    graph: every kernel they exercise -- the CPU ones, bfs_gpu / sssp_pull_gpu / pr_pull_gpu with each named
+    epoch kernel (the sync-warp BFS kernel named without its template argument), and the heterogeneous drivers,
+    which run on one GPU here -- must report success."""
+    exe = REF_TESTS[name]
+    if not os.path.exists(exe):
+        pytest.skip("the reference's test programs were not built (oracle/_ref)")
+    g = hc.gen_kronecker(12, 16, 4, wtype=hc.W_I32)
+    path = str(tmp_path / ("g.sg" if name == "bfs" else "g.wsg"))
+    hc.write_graph(path, hc.HostCSR(g.index, g.neighbors) if name == "bfs" else g)
+    r = subprocess.run([exe, path], capture_output=True, text=True, timeout=600)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    verified = r.stdout.count("Verifying ")
+    assert verified == {"bfs": 8, "sssp": 5, "pr": 5}[name], r.stdout
+    if name == "bfs":
+        assert r.stdout.count("Verification success!") == verified, r.stdout
+    else:
+        assert r.stdout.count("Verification succeeded!") == verified and "failed" not in r.stdout, r.stdout
