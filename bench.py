@@ -496,8 +496,9 @@ def cpu_leg(host, a, gpu):
         par["bfs"] = {"sources": kp, "ok": bool(ok),
                       "check": "depths == serial BFS; GPU parents and the reference's bfs_do_cpu parents valid trees"}
         ref = oracle.run_reference("sssp", wsg, kp, out, threads=threads)
-        ref_d = np.fromfile(out, dtype=np.float32).reshape(kp, n)
-        want = np.where(np.isinf(ref_d), 0x7FFFFFFF, ref_d).astype(np.int64)
+        ref_d = np.fromfile(out, dtype=np.float32).reshape(kp, n).astype(np.float64)
+        ref_d[np.isinf(ref_d)] = 0x7FFFFFFF  # the reference's inf is this engine's INT32_MAX
+        want = ref_d.astype(np.int64)
         ok = bool(np.array_equal(gpu["dist"][:kp].astype(np.int64), want))
         par["sssp"] = {"sources": kp, "ok": ok, "check": "bit-exact vs the reference's sssp_pull_cpu"}
         ref = oracle.run_reference("pr", wsg, 0, out, threads=1)

@@ -27,19 +27,6 @@ namespace {
 
 constexpr int kPrThreads = 256;
 constexpr int kMaxIterSlots = 4096;
-// The sweep's block size and the shared-memory copy of the gathered vector's
-// hub prefix (bytes per block): on a degree-sorted graph most gathers read
-// the first few thousand entries (at Kronecker scale 22, 40 % of the edges
-// point at the first 16384 vertices); a Jacobi sweep reads only the previous
-// iterate, so a per-block copy taken at the start of the sweep is exact.
-#ifndef HC_PR_SWEEP_THREADS
-#define HC_PR_SWEEP_THREADS 512
-#endif
-#ifndef HC_PR_HUB_BYTES
-#define HC_PR_HUB_BYTES (48 * 1024)
-#endif
-constexpr int kSweepThreads = HC_PR_SWEEP_THREADS;
-constexpr int kHubBytes = HC_PR_HUB_BYTES;
 
 struct IterState {
     double l1[kMaxIterSlots];
@@ -72,7 +59,6 @@ struct SweepArgs {
     float tol_l1, eps;
     int max_iters;
     int32_t n_active;
-    int32_t hub_n;          // gin[0, hub_n) is read from the block's shared copy
 };
 
 template <bool kEW, bool kRS, bool kPS, bool kBaseVec, bool kCG = false>
@@ -106,34 +92,19 @@ __device__ __forceinline__ void finish_row(const SweepArgs &a, int32_t r, float 
     chg += dl > a.eps;
 }
 
-// Gathered value of neighbour u: from the block's shared copy for a hub, else
-// through L1.  Both loads issue (the global one at entry 0 for a hub, a line
-// every warp shares) and a select picks one, so a warp's gathers stay
-// independent and in flight together.
-__device__ __forceinline__ float gather(const SweepArgs &a, const float *s_hub, int32_t u) {
-    const bool hub = u < a.hub_n;
-    const float gg = __ldg(a.gin + (hub ? 0 : u));
-    const float gh = s_hub[hub ? u : 0];
-    return hub ? gh : gg;
-}
-
 template <bool kEW>
-__device__ __forceinline__ float edge_val(const SweepArgs &a, const float *s_hub, int64_t e) {
-    const float g = gather(a, s_hub, a.nbr[e]);
+__device__ __forceinline__ float edge_val(const SweepArgs &a, int64_t e) {
+    const float g = __ldg(a.gin + a.nbr[e]);
     return kEW ? g * a.ew[e] : g;
 }
 
 template <bool kEW, bool kRS, bool kPS, bool kBaseVec, bool kCG = false>
-__global__ void __launch_bounds__(kSweepThreads) pr_sweep(SweepArgs a, PrPlanDev plan) {
-    __shared__ float s_acc[kSweepThreads / 32][32];
+__global__ void __launch_bounds__(kPrThreads) pr_sweep(SweepArgs a, PrPlanDev plan) {
+    __shared__ float s_acc[kPrThreads / 32][32];
     __shared__ double s_l1[32];
     __shared__ int s_chg[32];
     __shared__ int s_last;
-    extern __shared__ float s_hub[];  // max(hub_n, 1) entries
     if (*(volatile int *)&a.st->done) return;
-    // The previous iterate is read-only during the sweep: copy its hub prefix.
-    for (int i = threadIdx.x; i < a.hub_n; i += blockDim.x) s_hub[i] = __ldg(a.gin + i);
-    __syncthreads();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -153,12 +124,12 @@ __global__ void __launch_bounds__(kSweepThreads) pr_sweep(SweepArgs a, PrPlanDev
             float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
             int64_t i = b + lane;
             for (; i + 96 < e; i += 128) {
-                s0 += edge_val<kEW>(a, s_hub, i);
-                s1 += edge_val<kEW>(a, s_hub, i + 32);
-                s2 += edge_val<kEW>(a, s_hub, i + 64);
-                s3 += edge_val<kEW>(a, s_hub, i + 96);
+                s0 += edge_val<kEW>(a, i);
+                s1 += edge_val<kEW>(a, i + 32);
+                s2 += edge_val<kEW>(a, i + 64);
+                s3 += edge_val<kEW>(a, i + 96);
             }
-            for (; i < e; i += 32) s0 += edge_val<kEW>(a, s_hub, i);
+            for (; i < e; i += 32) s0 += edge_val<kEW>(a, i);
             float s = warp_sum((s0 + s1) + (s2 + s3));
             int last = 0;
             if (lane == 0) {
@@ -183,20 +154,19 @@ __global__ void __launch_bounds__(kSweepThreads) pr_sweep(SweepArgs a, PrPlanDev
             float s = 0.f;
             // Scalar head up to a 16-byte boundary, then 128-bit neighbour loads.
             const int64_t ab = min(e, (b + 3) & ~(int64_t)3);
-            if (b + lane < ab) s += edge_val<kEW>(a, s_hub, b + lane);
+            if (b + lane < ab) s += edge_val<kEW>(a, b + lane);
             for (int64_t i = ab + 4 * lane; i + 3 < e; i += 128) {
                 const int4 v4 = *reinterpret_cast<const int4 *>(a.nbr + i);
-                const float g0 = gather(a, s_hub, v4.x), g1 = gather(a, s_hub, v4.y);
-                const float g2 = gather(a, s_hub, v4.z), g3 = gather(a, s_hub, v4.w);
                 if (kEW) {
                     const float4 w4 = *reinterpret_cast<const float4 *>(a.ew + i);
-                    s += g0 * w4.x + g1 * w4.y + g2 * w4.z + g3 * w4.w;
+                    s += __ldg(a.gin + v4.x) * w4.x + __ldg(a.gin + v4.y) * w4.y +
+                         __ldg(a.gin + v4.z) * w4.z + __ldg(a.gin + v4.w) * w4.w;
                 } else {
-                    s += (g0 + g1) + (g2 + g3);
+                    s += (__ldg(a.gin + v4.x) + __ldg(a.gin + v4.y)) + (__ldg(a.gin + v4.z) + __ldg(a.gin + v4.w));
                 }
             }
             const int64_t tail = ab + ((e - ab) & ~(int64_t)3);
-            if (tail + lane < e) s += edge_val<kEW>(a, s_hub, tail + lane);
+            if (tail + lane < e) s += edge_val<kEW>(a, tail + lane);
             s = warp_sum(s);
             if (lane == 0) finish_row<kEW, kRS, kPS, kBaseVec, kCG>(a, r, s, l1, chg);
         } else {
@@ -217,7 +187,7 @@ __global__ void __launch_bounds__(kSweepThreads) pr_sweep(SweepArgs a, PrPlanDev
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const int k = k0 + 32 * j + lane;
-                    vals[j] = k < gend ? edge_val<kEW>(a, s_hub, s0 + k) : 0.f;
+                    vals[j] = k < gend ? edge_val<kEW>(a, s0 + k) : 0.f;
                 }
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
@@ -672,20 +642,14 @@ PrPlanDev plan_view(hc_graph *g, int *partial_slots) {
 }
 
 template <bool kEW, bool kRS, bool kPS, bool kBaseVec, bool kCG = false>
-hc_status launch_sweep(hc_graph *g, const SweepArgs &args, const PrPlanDev &plan) {
+hc_status launch_sweep(hc_graph *g, const SweepArgs &a, const PrPlanDev &plan) {
     static int bps = 0;
-    constexpr int hub_cap = kHubBytes / 4;
-    const size_t smem = sizeof(float) * (size_t)std::max(hub_cap, 1);
     if (bps == 0) {
-        HC_CUDA_TRY(cudaFuncSetAttribute(pr_sweep<kEW, kRS, kPS, kBaseVec, kCG>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         HC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pr_sweep<kEW, kRS, kPS, kBaseVec, kCG>,
-                                                                  kSweepThreads, smem));
+                                                                  kPrThreads, 0));
         bps = std::max(bps, 1);
     }
-    SweepArgs a = args;
-    a.hub_n = std::min(hub_cap, a.n_active);
-    { pr_sweep<kEW, kRS, kPS, kBaseVec, kCG><<<g->sm_count * bps, kSweepThreads, smem, g->stream>>>(a, plan); ::hc::count_launch(); }
+    { pr_sweep<kEW, kRS, kPS, kBaseVec, kCG><<<g->sm_count * bps, kPrThreads, 0, g->stream>>>(a, plan); ::hc::count_launch(); }
     HC_CUDA_TRY(cudaGetLastError());
     return HC_OK;
 }

@@ -24,10 +24,11 @@
 // once per graph by Kahn's algorithm on the device: count each vertex's lower
 // neighbours, start from the vertices with none, and release a vertex when its
 // last lower neighbour has been placed.  A cooperative persistent kernel then
-// runs the sweeps: a warp per row (its lanes gather 32 terms at a time and
-// every lane adds them in row order from shuffles, so the sum is the
-// sequential one), a grid barrier after each level, and the per-sweep update
-// count read after the last barrier.
+// runs the sweeps with a grid barrier after each level and the per-sweep
+// update count read after the last barrier.  A lane sums a short row by
+// itself; the warp sums a long row together (its lanes gather 32 terms at a
+// time and every lane adds them in row order from shuffles).  Either way each
+// sum is the sequential one.
 #include <algorithm>
 #include <vector>
 
@@ -38,6 +39,8 @@ namespace {
 
 constexpr int kOrdThreads = 256;
 constexpr int kSweepsPerLaunch = 8;
+// Rows up to this many edges are summed by one lane, longer ones by the warp.
+constexpr int kShortRow = 64;
 
 // cnt[x] = neighbours u < x in x's row; vertices with none open level 0.
 __global__ void ord_count_lower(const int64_t *index, const int32_t *nbr, int32_t n, int32_t *cnt,
@@ -105,6 +108,17 @@ struct OrdArgs {
     OrdCtl *ctl;
 };
 
+// The reference's update of row x from its in-order sum: stored only when it
+// moves the score by more than eps; returns 1 when stored.
+__device__ __forceinline__ int update_row(const OrdArgs &a, float base, int32_t x, float sum) {
+    const float nv = __fadd_rn(base, __fmul_rn(a.damping, sum));
+    const float old = __ldcg(&a.score[x]);
+    if (!(fabsf(__fsub_rn(nv, old)) > a.eps)) return 0;
+    __stcg(&a.score[x], nv);
+    __stcg(&a.gv[x], __fdiv_rn(nv, a.degf[x]));
+    return 1;
+}
+
 __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -117,40 +131,62 @@ __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
         int local = 0;
         for (int l = 0; l < a.levels; l++) {
             const int lo = a.level_off[l], hi = a.level_off[l + 1];
-            for (int i = lo + warp; i < hi; i += nw) {
-                const int32_t x = a.order[i];
-                const int64_t b = a.index[x], e = a.index[x + 1];
-                float sum = 0.0f;
-                // Full 32-term chunks: the shuffles take constant lanes and
-                // issue ahead of the add chain, so a chunk costs its 32
-                // dependent adds; the next chunk's gathers are issued before
-                // this one is summed.
-                const int64_t full_end = b + ((e - b) & ~(int64_t)31);
-                float t = 0.0f;
-                if (b < full_end) t = __ldcg(&a.gv[a.nbr[b + lane]]);
-                for (int64_t c = b; c < full_end; c += 32) {
-                    float tn = 0.0f;
-                    if (c + 32 < full_end) tn = __ldcg(&a.gv[a.nbr[c + 32 + lane]]);
-#pragma unroll
-                    for (int q = 0; q < 32; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t, q));
-                    t = tn;
+            // A warp takes 32 rows of the level: a lane sums a short row alone
+            // (four gathers in flight ahead of its add chain); the warp then
+            // sums the long rows among the 32 together, one at a time.
+            for (int g0 = lo + warp * 32; g0 < hi; g0 += nw * 32) {
+                const int i = g0 + lane;
+                int32_t x = -1;
+                int64_t b = 0, e = 0;
+                if (i < hi) {
+                    x = a.order[i];
+                    b = a.index[x];
+                    e = a.index[x + 1];
                 }
-                if (full_end < e) {
-                    const float tr = full_end + lane < e ? __ldcg(&a.gv[a.nbr[full_end + lane]]) : 0.0f;
-                    const int k = (int)(e - full_end);
-                    for (int q = 0; q < k; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, tr, q));
-                }
-                const float nv = __fadd_rn(base, __fmul_rn(a.damping, sum));
-                const float old = __ldcg(&a.score[x]);
-                if (fabsf(__fsub_rn(nv, old)) > a.eps) {
-                    if (lane == 0) {
-                        __stcg(&a.score[x], nv);
-                        __stcg(&a.gv[x], __fdiv_rn(nv, a.degf[x]));
+                const bool is_long = x >= 0 && e - b > kShortRow;
+                if (x >= 0 && !is_long) {
+                    float sum = 0.0f;
+                    int64_t j = b;
+                    for (; j + 3 < e; j += 4) {
+                        const float t0 = __ldcg(&a.gv[a.nbr[j]]), t1 = __ldcg(&a.gv[a.nbr[j + 1]]);
+                        const float t2 = __ldcg(&a.gv[a.nbr[j + 2]]), t3 = __ldcg(&a.gv[a.nbr[j + 3]]);
+                        sum = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(sum, t0), t1), t2), t3);
                     }
-                    local++;
+                    for (; j < e; j++) sum = __fadd_rn(sum, __ldcg(&a.gv[a.nbr[j]]));
+                    local += update_row(a, base, x, sum);
+                }
+                for (unsigned lm = __ballot_sync(kFull, is_long); lm; lm &= lm - 1) {
+                    const int src = __ffs(lm) - 1;
+                    const int32_t xr = __shfl_sync(kFull, x, src);
+                    const int64_t br = __shfl_sync(kFull, b, src), er = __shfl_sync(kFull, e, src);
+                    float sum = 0.0f;
+                    // Full 32-term chunks: the shuffles take constant lanes
+                    // and issue ahead of the add chain; the next chunk's
+                    // gathers are issued before this one is summed.
+                    const int64_t full_end = br + ((er - br) & ~(int64_t)31);
+                    float t = 0.0f;
+                    if (br < full_end) t = __ldcg(&a.gv[a.nbr[br + lane]]);
+                    for (int64_t c = br; c < full_end; c += 32) {
+                        float tn = 0.0f;
+                        if (c + 32 < full_end) tn = __ldcg(&a.gv[a.nbr[c + 32 + lane]]);
+#pragma unroll
+                        for (int q = 0; q < 32; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t, q));
+                        t = tn;
+                    }
+                    if (full_end < er) {
+                        const float tr = full_end + lane < er ? __ldcg(&a.gv[a.nbr[full_end + lane]]) : 0.0f;
+                        const int k = (int)(er - full_end);
+                        for (int q = 0; q < k; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, tr, q));
+                    }
+                    int stored = 0;
+                    if (lane == src) stored = update_row(a, base, xr, sum);
+                    local += stored;
                 }
             }
-            if (l == a.levels - 1 && lane == 0 && local) atomicAdd(&a.ctl->updated[s % 3], local);
+            if (l == a.levels - 1) {
+                const int w = warp_sum(local);
+                if (lane == 0 && w) atomicAdd(&a.ctl->updated[s % 3], w);
+            }
             if (!grid_barrier(&a.ctl->gs)) return;
         }
         const int u = ld_cg(&a.ctl->updated[s % 3]);
