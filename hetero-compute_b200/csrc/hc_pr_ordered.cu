@@ -39,8 +39,12 @@ namespace {
 
 constexpr int kOrdThreads = 256;
 constexpr int kSweepsPerLaunch = 8;
-// Rows up to this many edges are summed by one lane, longer ones by the warp.
-constexpr int kShortRow = 64;
+// Rows up to this many edges are summed by one lane from terms the warp
+// gathered into shared memory (32 rows' worth at most kShortRow * 32 terms);
+// longer ones by the whole warp, kLongDepth 32-term chunks in flight.
+constexpr int kShortRow = 32;
+constexpr int kGatherUnroll = 4;
+constexpr int kLongDepth = 8;
 
 // cnt[x] = neighbours u < x in x's row; vertices with none open level 0.
 __global__ void ord_count_lower(const int64_t *index, const int32_t *nbr, int32_t n, int32_t *cnt,
@@ -120,6 +124,8 @@ __device__ __forceinline__ int update_row(const OrdArgs &a, float base, int32_t 
 }
 
 __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
+    __shared__ float s_terms[kOrdThreads / 32][kShortRow * 32];
+    const int wib = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -131,9 +137,12 @@ __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
         int local = 0;
         for (int l = 0; l < a.levels; l++) {
             const int lo = a.level_off[l], hi = a.level_off[l + 1];
-            // A warp takes 32 rows of the level: a lane sums a short row alone
-            // (four gathers in flight ahead of its add chain); the warp then
-            // sums the long rows among the 32 together, one at a time.
+            // A warp takes 32 rows of the level.  Short rows (<= kShortRow
+            // edges): the warp gathers all their terms at once, coalesced
+            // over the rows' concatenated edge ranges, into its shared
+            // buffer, then each lane adds its own row's terms in row order.
+            // Long rows: the whole warp, one row at a time, kLongDepth
+            // 32-term chunks in flight ahead of the add chain.
             for (int g0 = lo + warp * 32; g0 < hi; g0 += nw * 32) {
                 const int i = g0 + lane;
                 int32_t x = -1;
@@ -144,39 +153,67 @@ __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
                     e = a.index[x + 1];
                 }
                 const bool is_long = x >= 0 && e - b > kShortRow;
+                const int dshort = (x >= 0 && !is_long) ? (int)(e - b) : 0;
+                int total = 0;
+                const int pre = warp_exclusive_scan(dshort, &total);
+                for (int k0 = 0; k0 < total; k0 += 32 * kGatherUnroll) {
+                    int32_t u[kGatherUnroll];
+#pragma unroll
+                    for (int j = 0; j < kGatherUnroll; j++) {
+                        const int k = k0 + 32 * j + lane;
+                        const int kk = min(k, total - 1);
+                        // Term kk's row: the last lane whose prefix is <= kk
+                        // (every lane takes part in the shuffles).
+                        int lo_l = 0;
+#pragma unroll
+                        for (int st = 16; st > 0; st >>= 1) {
+                            const int c = __shfl_sync(kFull, pre, lo_l + st);
+                            if (c <= kk) lo_l += st;
+                        }
+                        const int64_t ob = __shfl_sync(kFull, b, lo_l);
+                        const int op = __shfl_sync(kFull, pre, lo_l);
+                        u[j] = k < total ? a.nbr[ob + (kk - op)] : -1;
+                    }
+#pragma unroll
+                    for (int j = 0; j < kGatherUnroll; j++) {
+                        const int k = k0 + 32 * j + lane;
+                        if (k < total) s_terms[wib][k] = __ldcg(&a.gv[u[j]]);
+                    }
+                }
+                __syncwarp();
                 if (x >= 0 && !is_long) {
                     float sum = 0.0f;
-                    int64_t j = b;
-                    for (; j + 3 < e; j += 4) {
-                        const float t0 = __ldcg(&a.gv[a.nbr[j]]), t1 = __ldcg(&a.gv[a.nbr[j + 1]]);
-                        const float t2 = __ldcg(&a.gv[a.nbr[j + 2]]), t3 = __ldcg(&a.gv[a.nbr[j + 3]]);
-                        sum = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(sum, t0), t1), t2), t3);
-                    }
-                    for (; j < e; j++) sum = __fadd_rn(sum, __ldcg(&a.gv[a.nbr[j]]));
+                    for (int k = pre; k < pre + dshort; k++) sum = __fadd_rn(sum, s_terms[wib][k]);
                     local += update_row(a, base, x, sum);
                 }
+                __syncwarp();
                 for (unsigned lm = __ballot_sync(kFull, is_long); lm; lm &= lm - 1) {
                     const int src = __ffs(lm) - 1;
                     const int32_t xr = __shfl_sync(kFull, x, src);
                     const int64_t br = __shfl_sync(kFull, b, src), er = __shfl_sync(kFull, e, src);
                     float sum = 0.0f;
-                    // Full 32-term chunks: the shuffles take constant lanes
-                    // and issue ahead of the add chain; the next chunk's
-                    // gathers are issued before this one is summed.
-                    const int64_t full_end = br + ((er - br) & ~(int64_t)31);
-                    float t = 0.0f;
-                    if (br < full_end) t = __ldcg(&a.gv[a.nbr[br + lane]]);
-                    for (int64_t c = br; c < full_end; c += 32) {
-                        float tn = 0.0f;
-                        if (c + 32 < full_end) tn = __ldcg(&a.gv[a.nbr[c + 32 + lane]]);
+                    // kLongDepth chunks per round: their gathers are issued
+                    // together, then summed 32 at a time from shuffles with
+                    // constant lanes (the add chain is the only wait).
+                    for (int64_t c0 = br; c0 < er; c0 += 32 * kLongDepth) {
+                        float t[kLongDepth];
 #pragma unroll
-                        for (int q = 0; q < 32; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t, q));
-                        t = tn;
-                    }
-                    if (full_end < er) {
-                        const float tr = full_end + lane < er ? __ldcg(&a.gv[a.nbr[full_end + lane]]) : 0.0f;
-                        const int k = (int)(er - full_end);
-                        for (int q = 0; q < k; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, tr, q));
+                        for (int j = 0; j < kLongDepth; j++) {
+                            const int64_t c = c0 + 32 * j + lane;
+                            t[j] = c < er ? __ldcg(&a.gv[a.nbr[c]]) : 0.0f;
+                        }
+#pragma unroll
+                        for (int j = 0; j < kLongDepth; j++) {
+                            const int64_t cb = c0 + 32 * j;
+                            if (cb >= er) break;
+                            if (er - cb >= 32) {
+#pragma unroll
+                                for (int q = 0; q < 32; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t[j], q));
+                            } else {
+                                const int k = (int)(er - cb);
+                                for (int q = 0; q < k; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t[j], q));
+                            }
+                        }
                     }
                     int stored = 0;
                     if (lane == src) stored = update_row(a, base, xr, sum);
