@@ -67,7 +67,8 @@ struct hc_graph {
     int32_t pr_partial_slots = 0;
     hc::DevBuf pr_plan_huge_rows;
     // level schedule of the reference-order PageRank sweep (hc_pr_ordered.cu):
-    // order[N] | level_off[levels + 1] | deg as fp32 [N]; levels -1 = not built
+    // order[N] | level_off[levels + 1] | level_long[levels] | deg as fp32 [N];
+    // levels -1 = not built
     hc::DevBuf pr_ord;
     int32_t pr_ord_levels = -1;
 

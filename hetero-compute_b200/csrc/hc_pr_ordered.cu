@@ -104,6 +104,7 @@ struct OrdArgs {
     const int32_t *nbr;
     const int32_t *order;
     const int32_t *level_off;
+    const int32_t *level_long;  // rows of more than kShortRow edges at the head of each level
     int32_t levels, n;
     float *score, *gv;
     const float *degf;
@@ -137,13 +138,44 @@ __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
         int local = 0;
         for (int l = 0; l < a.levels; l++) {
             const int lo = a.level_off[l], hi = a.level_off[l + 1];
-            // A warp takes 32 rows of the level.  Short rows (<= kShortRow
-            // edges): the warp gathers all their terms at once, coalesced
-            // over the rows' concatenated edge ranges, into its shared
-            // buffer, then each lane adds its own row's terms in row order.
-            // Long rows: the whole warp, one row at a time, kLongDepth
-            // 32-term chunks in flight ahead of the add chain.
-            for (int g0 = lo + warp * 32; g0 < hi; g0 += nw * 32) {
+            // Each level lists its long rows (> kShortRow edges) first.  A long
+            // row is summed by one warp (kLongDepth 32-term chunks in flight,
+            // summed 32 at a time from shuffles with constant lanes: the add
+            // chain is the only wait), one row per warp so that long rows run
+            // side by side.  Short rows go 32 to a warp: the warp gathers all
+            // their terms at once, coalesced over the rows' concatenated edge
+            // ranges, into its shared buffer, and each lane adds its own row's
+            // terms in row order.
+            const int mid = lo + a.level_long[l];
+            for (int i = lo + warp; i < mid; i += nw) {
+                const int32_t x = a.order[i];
+                const int64_t br = a.index[x], er = a.index[x + 1];
+                float sum = 0.0f;
+                for (int64_t c0 = br; c0 < er; c0 += 32 * kLongDepth) {
+                    float t[kLongDepth];
+#pragma unroll
+                    for (int j = 0; j < kLongDepth; j++) {
+                        const int64_t c = c0 + 32 * j + lane;
+                        t[j] = c < er ? __ldcg(&a.gv[a.nbr[c]]) : 0.0f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < kLongDepth; j++) {
+                        const int64_t cb = c0 + 32 * j;
+                        if (cb >= er) break;
+                        if (er - cb >= 32) {
+#pragma unroll
+                            for (int q = 0; q < 32; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t[j], q));
+                        } else {
+                            const int k = (int)(er - cb);
+                            for (int q = 0; q < k; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t[j], q));
+                        }
+                    }
+                }
+                int stored = 0;
+                if (lane == 0) stored = update_row(a, base, x, sum);
+                local += stored;
+            }
+            for (int g0 = mid + warp * 32; g0 < hi; g0 += nw * 32) {
                 const int i = g0 + lane;
                 int32_t x = -1;
                 int64_t b = 0, e = 0;
@@ -152,8 +184,7 @@ __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
                     b = a.index[x];
                     e = a.index[x + 1];
                 }
-                const bool is_long = x >= 0 && e - b > kShortRow;
-                const int dshort = (x >= 0 && !is_long) ? (int)(e - b) : 0;
+                const int dshort = x >= 0 ? (int)(e - b) : 0;
                 int total = 0;
                 const int pre = warp_exclusive_scan(dshort, &total);
                 for (int k0 = 0; k0 < total; k0 += 32 * kGatherUnroll) {
@@ -181,44 +212,12 @@ __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
                     }
                 }
                 __syncwarp();
-                if (x >= 0 && !is_long) {
+                if (x >= 0) {
                     float sum = 0.0f;
                     for (int k = pre; k < pre + dshort; k++) sum = __fadd_rn(sum, s_terms[wib][k]);
                     local += update_row(a, base, x, sum);
                 }
                 __syncwarp();
-                for (unsigned lm = __ballot_sync(kFull, is_long); lm; lm &= lm - 1) {
-                    const int src = __ffs(lm) - 1;
-                    const int32_t xr = __shfl_sync(kFull, x, src);
-                    const int64_t br = __shfl_sync(kFull, b, src), er = __shfl_sync(kFull, e, src);
-                    float sum = 0.0f;
-                    // kLongDepth chunks per round: their gathers are issued
-                    // together, then summed 32 at a time from shuffles with
-                    // constant lanes (the add chain is the only wait).
-                    for (int64_t c0 = br; c0 < er; c0 += 32 * kLongDepth) {
-                        float t[kLongDepth];
-#pragma unroll
-                        for (int j = 0; j < kLongDepth; j++) {
-                            const int64_t c = c0 + 32 * j + lane;
-                            t[j] = c < er ? __ldcg(&a.gv[a.nbr[c]]) : 0.0f;
-                        }
-#pragma unroll
-                        for (int j = 0; j < kLongDepth; j++) {
-                            const int64_t cb = c0 + 32 * j;
-                            if (cb >= er) break;
-                            if (er - cb >= 32) {
-#pragma unroll
-                                for (int q = 0; q < 32; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t[j], q));
-                            } else {
-                                const int k = (int)(er - cb);
-                                for (int q = 0; q < k; q++) sum = __fadd_rn(sum, __shfl_sync(kFull, t[j], q));
-                            }
-                        }
-                    }
-                    int stored = 0;
-                    if (lane == src) stored = update_row(a, base, xr, sum);
-                    local += stored;
-                }
             }
             if (l == a.levels - 1) {
                 const int w = warp_sum(local);
@@ -244,7 +243,8 @@ __global__ void __launch_bounds__(kOrdThreads) pr_ordered_sweeps(OrdArgs a) {
 }
 
 // Builds the level schedule once per graph: g->pr_ord holds
-// order[N] | level_off[levels + 1] | degf[N], g->pr_ord_levels the count.
+// order[N] (each level's long rows first) | level_off[levels + 1] |
+// level_long[levels] | degf[N], g->pr_ord_levels the count.
 hc_status ensure_order(hc_graph *g) {
     if (g->pr_ord_levels >= 0) return HC_OK;
     bool sym = false;
@@ -283,13 +283,34 @@ hc_status ensure_order(hc_graph *g) {
     if (lo != n)
         return fail(HC_ERR_INVALID_ARG, "hc_pr_pull_ordered: level schedule placed %d of %d vertices", lo, n);
     const int32_t levels = (int32_t)off.size() - 1;
+    // Within a level any order is exact; long rows go first (descending
+    // degree, then id), and each level records how many there are.
+    std::vector<int32_t> h_order((size_t)n);
+    std::vector<int64_t> h_index((size_t)n + 1);
+    HC_CUDA_TRY(cudaMemcpyAsync(h_order.data(), order.ptr, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost,
+                                g->stream));
+    HC_CUDA_TRY(cudaMemcpyAsync(h_index.data(), g->index.ptr, sizeof(int64_t) * ((size_t)n + 1),
+                                cudaMemcpyDeviceToHost, g->stream));
+    HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    std::vector<int32_t> nlong((size_t)levels);
+    for (int32_t l = 0; l < levels; l++) {
+        auto deg = [&](int32_t v) { return h_index[v + 1] - h_index[v]; };
+        std::sort(h_order.begin() + off[l], h_order.begin() + off[l + 1], [&](int32_t p, int32_t q) {
+            return deg(p) != deg(q) ? deg(p) > deg(q) : p < q;
+        });
+        int32_t c = 0;
+        while (off[l] + c < off[l + 1] && deg(h_order[off[l] + c]) > kShortRow) c++;
+        nlong[l] = c;
+    }
     const size_t order_b = (sizeof(int32_t) * (size_t)n + 255) / 256 * 256;
-    const size_t off_b = (sizeof(int32_t) * (off.size()) + 255) / 256 * 256;
+    const size_t off_b = (sizeof(int32_t) * (2 * (size_t)levels + 1) + 255) / 256 * 256;
     HC_TRY(g->pr_ord.ensure(order_b + off_b + sizeof(float) * (size_t)n));
-    HC_CUDA_TRY(cudaMemcpyAsync(g->pr_ord.ptr, order.ptr, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToDevice,
+    HC_CUDA_TRY(cudaMemcpyAsync(g->pr_ord.ptr, h_order.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice,
                                 g->stream));
     HC_CUDA_TRY(cudaMemcpyAsync(g->pr_ord.as<char>() + order_b, off.data(), sizeof(int32_t) * off.size(),
                                 cudaMemcpyHostToDevice, g->stream));
+    HC_CUDA_TRY(cudaMemcpyAsync(g->pr_ord.as<char>() + order_b + sizeof(int32_t) * off.size(), nlong.data(),
+                                sizeof(int32_t) * nlong.size(), cudaMemcpyHostToDevice, g->stream));
     HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
     g->pr_ord_levels = levels;
     return HC_OK;
@@ -317,7 +338,7 @@ extern "C" hc_status hc_pr_pull_ordered(hc_graph *g, const float *init_scores, f
     HC_TRY(ensure_order(g));
 
     const size_t order_b = (sizeof(int32_t) * (size_t)n + 255) / 256 * 256;
-    const size_t off_b = (sizeof(int32_t) * ((size_t)g->pr_ord_levels + 1) + 255) / 256 * 256;
+    const size_t off_b = (sizeof(int32_t) * (2 * (size_t)g->pr_ord_levels + 1) + 255) / 256 * 256;
     HC_TRY(g->ws_pr.ensure(2 * ((sizeof(float) * (size_t)n + 255) / 256 * 256) + 256));
     HC_TRY(g->ws_ctl.ensure(4096));
     float *score = g->ws_pr.as<float>();
@@ -353,6 +374,7 @@ extern "C" hc_status hc_pr_pull_ordered(hc_graph *g, const float *init_scores, f
     a.nbr = g->nbr.as<int32_t>();
     a.order = g->pr_ord.as<int32_t>();
     a.level_off = reinterpret_cast<const int32_t *>(g->pr_ord.as<char>() + order_b);
+    a.level_long = a.level_off + g->pr_ord_levels + 1;
     a.levels = g->pr_ord_levels;
     a.n = n;
     a.score = score;
