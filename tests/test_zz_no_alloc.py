@@ -50,3 +50,32 @@ def test_noalloc_bfs_rejects_what_does_not_fit():
     st = hc.lib().hc_bfs_noalloc(host_idx.ctypes.data, nbr.data_ptr(), 3, 0, 0, out.data_ptr(), out.data_ptr(),
                                  None)
     assert st == hc.INVALID_ARG
+
+
+@pytest.mark.parametrize("kind", ["near_limit", "grid", "isolated_source"])
+def test_noalloc_bfs_near_its_limits_and_odd_graphs(kind):
+    """Near the fixed working set's limits (Kronecker scale 20, edge factor 8: 2^20 vertices, under 2^24
+    edges), on a graph without degree ordering (a grid), and from a source without edges."""
+    torch = pytest.importorskip("torch")
+    if kind == "near_limit":
+        host = hc.gen_kronecker(20, 8, 4)
+        assert host.num_nodes == 1 << 20 and host.num_edges <= 1 << 24
+        srcs = hc.pick_sources(host, 2)
+    elif kind == "grid":
+        host = hc.gen_grid(64, 48, 2)
+        srcs = np.array([0, 1234], dtype=np.int32)
+    else:
+        host = hc.gen_kronecker(12, 4, 6)
+        srcs = np.array([int(np.flatnonzero(host.degrees() == 0)[0])], dtype=np.int32)
+    n, m = host.num_nodes, host.num_edges
+    g = hc.Graph.from_host(host)
+    idx = torch.from_numpy(host.index).cuda()
+    nbr = torch.from_numpy(host.neighbors).cuda()
+    for s in srcs:
+        depth = torch.empty((n,), dtype=torch.int32, device="cuda")
+        parent = torch.empty((n,), dtype=torch.int32, device="cuda")
+        assert _call(idx, nbr, n, m, s, depth, parent) == hc.OK, hc.lib().hc_last_error().decode()
+        d = depth.cpu().numpy()
+        ref, _, _ = g.bfs(np.array([s], dtype=np.int32))
+        assert np.array_equal(d, ref[0]) and np.array_equal(d, oracle.bfs_depth(host.index, host.neighbors, s))
+        assert oracle.verify_bfs_parents(host.index, host.neighbors, d, parent.cpu().numpy(), s)[0] == 0
