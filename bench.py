@@ -851,10 +851,11 @@ def main():
     parity = None
     if rank == 0 and world == 1:
         kp = min(4, k)
-        ordered, ost = g.pagerank_ordered()
         gpu_out = {"sources": src[:kp].tolist(), "depth": depth[:kp].cpu().numpy(), "parent": h_parent[:kp].copy(),
-                   "dist": h_dist[:kp].copy(), "pr": h_scores.copy(), "pr_ordered": ordered,
-                   "pr_ordered_sweeps": int(ost.iterations), "pr_ordered_ms": ost.ms}
+                   "dist": h_dist[:kp].copy(), "pr": h_scores.copy()}
+        if not a.no_cpu_baseline:  # the reference-order PageRank is checked against the reference's run
+            ordered, ost = g.pagerank_ordered()
+            gpu_out.update(pr_ordered=ordered, pr_ordered_sweeps=int(ost.iterations), pr_ordered_ms=ost.ms)
         del depth, parent, dist_o, flush
         torch.cuda.empty_cache()
         if not a.no_extras:

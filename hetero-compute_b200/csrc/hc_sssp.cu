@@ -653,7 +653,8 @@ hc_status launch_sssp(hc_graph *g, const SsspArgs &args) {
         HC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, sssp_persistent<kStats>, kSsspThreads, 0));
         if (bps < 1) return fail(HC_ERR_CUDA, "SSSP kernel cannot be resident");
     }
-    dim3 grid(g->sm_count * bps), block(kSsspThreads);
+    const int use = g->tune.sssp_blocks_per_sm > 0 ? std::min(bps, g->tune.sssp_blocks_per_sm) : bps;
+    dim3 grid(g->sm_count * use), block(kSsspThreads);
     SsspArgs a = args;
     void *params[] = {&a};
     ::hc::count_launch();

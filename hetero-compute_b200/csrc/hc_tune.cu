@@ -196,6 +196,14 @@ hc_status tune_sssp(Tuner &tu, hc_tuning &out) {
     }
     out.sssp_delta = o.delta;
     out.sssp_pull_alpha = o.pull_alpha;
+    // Blocks per SM of the persistent kernel (read from the handle by the
+    // launch; the trials set it there).
+    g->tune.sssp_blocks_per_sm = 0;
+    int32_t bps = 0;
+    descend(o, &g->tune.sssp_blocks_per_sm, {1}, best, run);
+    bps = g->tune.sssp_blocks_per_sm;
+    g->tune.sssp_blocks_per_sm = 0;
+    out.sssp_blocks_per_sm = bps;
     return HC_OK;
 }
 
@@ -296,6 +304,7 @@ extern "C" hc_status hc_set_tuning(hc_graph *g, const hc_tuning *t) {
         return fail(HC_ERR_INVALID_ARG, "hc_set_tuning: bad BFS variant %d", t->bfs_bu_variant);
     if (t->bfs_alpha < 0 || t->bfs_beta < 0 || t->mbfs_group < 0 || t->mssp_group < 0)
         return fail(HC_ERR_INVALID_ARG, "hc_set_tuning: negative threshold or group");
+    if (t->sssp_blocks_per_sm < 0) return fail(HC_ERR_INVALID_ARG, "hc_set_tuning: negative blocks per SM");
     if (t->bfs_bu_split_levels < 0 || t->bfs_bu_split_levels > HC_BFS_SPLIT_LEVELS)
         return fail(HC_ERR_INVALID_ARG, "hc_set_tuning: bad split level count %d", t->bfs_bu_split_levels);
     for (int l = 0; l < t->bfs_bu_split_levels; l++)

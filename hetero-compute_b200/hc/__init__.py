@@ -91,7 +91,7 @@ class Tuning(C.Structure):
                 ("sssp_delta", C.c_int32), ("sssp_pull_alpha", C.c_int32), ("mbfs_group", C.c_int32),
                 ("mbfs_switch_alpha", C.c_int32), ("mssp_group", C.c_int32), ("mssp_switch_alpha", C.c_int32),
                 ("trials", C.c_int32), ("tune_ms", C.c_double), ("bfs_bu_split", C.c_int32 * 8),
-                ("bfs_bu_split_levels", C.c_int32)]
+                ("bfs_bu_split_levels", C.c_int32), ("sssp_blocks_per_sm", C.c_int32)]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_}

@@ -389,6 +389,10 @@ typedef struct hc_tuning {
      * (hc_equal_edge_ranges), 32-aligned. */
     int32_t bfs_bu_split[HC_BFS_SPLIT_LEVELS];
     int32_t bfs_bu_split_levels;
+    /* Blocks per SM of the persistent SSSP kernel (its push epochs): fewer
+     * blocks make each grid barrier cheaper, more give large frontiers more
+     * warps.  0 = as many as fit (2). */
+    int32_t sssp_blocks_per_sm;
 } hc_tuning;
 
 #define HC_TUNE_BFS 1u
