@@ -80,7 +80,6 @@ struct hc_graph {
     int wstats_done = 0;
     int w_negative = 0;
     int32_t w_max = 0;         // largest weight (0 when none is positive)
-    int32_t w_min = 0;         // smallest weight
     double w_mean = 0.0;
     int w_symmetric = 0;       // w(u->v) == w(v->u) for every edge (rows sorted)
 

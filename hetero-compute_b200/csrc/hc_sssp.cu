@@ -50,7 +50,6 @@ struct SsspCtl {
     unsigned long long mf[3];  // degree sum of each near queue
     int far_len[2];
     int min_far;
-    int pull_min;  // smallest distance in the queue a pull epoch relaxes (see pull_sweep)
     int epochs, phases, pulls;
     unsigned long long vproc, erelax;
     struct {
@@ -73,7 +72,6 @@ struct SsspArgs {
     PrPlanDev plan;
     int32_t src;
     int32_t delta;  // <= 0: no far pile (plain frontier Bellman-Ford)
-    int32_t w_min;  // smallest edge weight
     int pull_alpha;  // <= 0: push only
     int max_epochs;
 };
@@ -155,20 +153,9 @@ __device__ __forceinline__ int32_t pull_val(const SsspArgs &a, int64_t e) {
 // long rows reduce with a warp min and lower dist by atomicMin; stream groups
 // (32 rows, one warp) reduce with a segmented warp min and own their rows and
 // their changed-bitmap word.  Lowered vertices are marked in `changed`.
-//
-// Rows that cannot improve are skipped.  Every vertex whose edges have not
-// been relaxed since its distance last fell is in the epoch's queue or in the
-// far pile, and the far pile's distances are not below the queue's, so no
-// candidate this epoch is below pull_min + w_min (pull_min: the queue's
-// smallest distance).  A vertex lowered during the sweep itself is marked
-// changed and relaxes its edges in a later epoch, and its candidates lie
-// higher still.  So a row whose distance is at most that bound keeps it: its
-// edges need not be read.  On degree-sorted Kronecker graphs the hub rows,
-// which hold most edges, settle first, so later pull epochs skip most of the
-// edge stream.
 template <bool kStats>
-__device__ __forceinline__ void pull_sweep(const SsspArgs &a, int32_t bound, int gwarp, int nwarps,
-                                           int32_t (*s_acc)[32], unsigned long long &my_e) {
+__device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwarps, int32_t (*s_acc)[32],
+                                           unsigned long long &my_e) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const PrPlanDev &p = a.plan;
     const int total = p.n_tasks + p.n_long + p.n_stream;
@@ -187,7 +174,6 @@ __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int32_t bound, int
                 b = a.index[r];
                 e = a.index[r + 1];
             }
-            if (__ldcg(a.dist + r) <= bound) continue;  // the row cannot improve
             int32_t m0 = kInfDist, m1 = kInfDist, m2 = kInfDist, m3 = kInfDist;
             int64_t i = b + lane;
             for (; i + 96 < e; i += 128) {
@@ -207,60 +193,57 @@ __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int32_t bound, int
             const int32_t r0 = p.stream[item - p.n_tasks - p.n_long] * 32;
             const int32_t r = r0 + lane;
             const int32_t rc = min(r, a.n_active);
-            const bool live = r < a.n_active && __ldcg(a.dist + r) > bound;
-            const unsigned live_mask = __ballot_sync(kFull, live);
-            if (!live_mask) continue;  // no row of the group can improve
             const int64_t s0 = a.index[r0];
             const int32_t rel = (int32_t)(a.index[rc] - s0);
             const int32_t gend = (int32_t)(a.index[min(r0 + 32, a.n_active)] - s0);
             s_acc[wib][lane] = kInfDist;
             __syncwarp();
-            // Four 32-edge chunks per pass: each edge's row (owner) first, then
-            // the loads and gathers of the live rows' edges, issued together,
-            // then each chunk reduced by its segmented scan.
+            // Four 32-edge chunks per pass: their loads and gathers are issued
+            // together, then each chunk is reduced by its segmented scan.
             for (int k0 = 0; k0 < gend; k0 += 128) {
                 int32_t vals[4];
-                int owner[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const int k = k0 + 32 * j + lane;
+                    vals[j] = k < gend ? pull_val(a, s0 + k) : kInfDist;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int kb = k0 + 32 * j;
+                    if (kb >= gend) break;
+                    const int k = kb + lane;
+                    const bool act = k < gend;
                     int lo = 0;
 #pragma unroll
                     for (int st = 16; st > 0; st >>= 1) {
                         const int c = __shfl_sync(kFull, rel, lo + st);
                         if (c <= k) lo += st;
                     }
-                    owner[j] = k < gend ? lo : 32;
-                    const bool use = k < gend && ((live_mask >> lo) & 1u);
-                    vals[j] = use ? pull_val(a, s0 + k) : kInfDist;
-                    if (kStats && use) my_e++;
-                }
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int kb = k0 + 32 * j;
-                    if (kb >= gend) break;
-                    const bool act = kb + lane < gend;
+                    const int owner = act ? lo : 32;
                     int32_t v = vals[j];
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
                         const int32_t y = __shfl_up_sync(kFull, v, o);
-                        const int ow = __shfl_up_sync(kFull, owner[j], o);
-                        if (lane >= o && ow == owner[j]) v = min(v, y);
+                        const int ow = __shfl_up_sync(kFull, owner, o);
+                        if (lane >= o && ow == owner) v = min(v, y);
                     }
-                    const int next_owner = __shfl_down_sync(kFull, owner[j], 1);
-                    if (act && (lane == 31 || next_owner != owner[j]))
-                        s_acc[wib][owner[j]] = min(s_acc[wib][owner[j]], v);
+                    const int next_owner = __shfl_down_sync(kFull, owner, 1);
+                    if (act && (lane == 31 || next_owner != owner))
+                        s_acc[wib][owner] = min(s_acc[wib][owner], v);
                     __syncwarp();
                 }
             }
             const int32_t m = s_acc[wib][lane];
             bool ch = false;
-            if (live && m < __ldcg(a.dist + r)) {
+            if (r < a.n_active && m < __ldcg(a.dist + r)) {
                 a.dist[r] = m;  // the group is the only writer of its rows
                 ch = true;
             }
             const unsigned bal = __ballot_sync(kFull, ch);
-            if (lane == 0 && bal) a.changed[r0 >> 5] = bal;
+            if (lane == 0) {
+                if (bal) a.changed[r0 >> 5] = bal;
+                if (kStats) my_e += (unsigned long long)gend;
+            }
             __syncwarp();
         }
     }
@@ -303,7 +286,6 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
             ctl->qlen[0] = 1;
             ctl->mf[0] = (unsigned long long)(a.index[a.src + 1] - a.index[a.src]);
             ctl->min_far = kInfDist;
-            ctl->pull_min = kInfDist;
         }
         if (!grid_barrier(&ctl->gs)) return;
     } else {
@@ -313,10 +295,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
         T = __ldcg(&ctl->saved_T);
         t_start = __ldcg(&ctl->t_start);
         if (!grid_barrier(&ctl->gs)) return;  // everyone has read the saved state
-        if (gtid == 0) {
-            ctl->need_pull = 0;
-            ctl->pull_min = kInfDist;  // the next pull epoch's queue minimum starts afresh
-        }
+        if (gtid == 0) ctl->need_pull = 0;
     }
     bool after_pull = resumed;  // epoch E's pull sweep ran in sssp_pull_kernel
 
@@ -535,13 +514,6 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
         }
         if (kStats && gtid == 0) my_v += nq;
         if (pull) {
-            // The queue's smallest distance bounds what the pull can lower
-            // (pull_sweep); every block folds in its share before this
-            // launch ends, so the pull kernel reads the final minimum.
-            int qm = kInfDist;
-            for (int i = gtid; i < nq; i += nthreads) qm = min(qm, __ldcg(a.dist + __ldcg(qcur + i)));
-            qm = warp_min(qm);
-            if (lane == 0 && qm < kInfDist) atomicMin(&ctl->pull_min, qm);
             // Hand the epoch to sssp_pull_kernel and resume after it.
             if (gtid == 0) {
                 ctl->saved_E = E;
@@ -597,10 +569,7 @@ __global__ void __launch_bounds__(kPullThreads) sssp_pull_kernel(SsspArgs a) {
     if (!__ldcg(&a.ctl->need_pull) || __ldcg(&a.ctl->gs.err)) return;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long my_e = 0;
-    // Rows at or below the bound cannot improve this epoch (see pull_sweep).
-    const int32_t qmin = __ldcg(&a.ctl->pull_min);
-    const int32_t bound = qmin == kInfDist ? -1 : sat_add(qmin, a.w_min) - 1;
-    pull_sweep<kStats>(a, bound, gtid >> 5, (gridDim.x * blockDim.x) >> 5, s_acc, my_e);
+    pull_sweep<kStats>(a, gtid >> 5, (gridDim.x * blockDim.x) >> 5, s_acc, my_e);
     if (kStats) {
         const unsigned long long e = block_sum(my_e, s_red);
         if (threadIdx.x == 0 && e) atomicAdd(&a.ctl->erelax, e);
@@ -660,7 +629,7 @@ __global__ void weight_stats(const int64_t *index, const int32_t *w, int32_t n, 
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     unsigned long long s = 0;
-    int32_t mx = 0, mn = kInfDist;
+    int32_t mx = 0;
     for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
         const int64_t b = index[v], e = index[v + 1];
         for (int64_t i = b + lane; i < e; i += 32) {
@@ -668,13 +637,10 @@ __global__ void weight_stats(const int64_t *index, const int32_t *w, int32_t n, 
             if (x < 0) flags[0] = 1;
             s += (unsigned long long)max(x, 0);
             mx = max(mx, x);
-            mn = min(mn, max(x, 0));
         }
     }
     mx = __reduce_max_sync(kFull, mx);
     if (lane == 0 && mx > 0) atomicMax(flags + 1, mx);
-    mn = __reduce_min_sync(kFull, mn);
-    if (lane == 0 && mn < kInfDist) atomicMin(flags + 2, mn);
     s = block_sum(s, s_red);
     if (threadIdx.x == 0 && s) atomicAdd(sum, s);
 }
@@ -745,8 +711,6 @@ hc_status ensure_weight_stats(hc_graph *g) {
     HC_TRY(buf.ensure(64));
     HC_CUDA_TRY(cudaMemsetAsync(buf.ptr, 0, 64, g->stream));
     int *flags = buf.as<int>();
-    const int inf = kInfDist;
-    HC_CUDA_TRY(cudaMemcpyAsync(flags + 2, &inf, sizeof(int), cudaMemcpyHostToDevice, g->stream));
     unsigned long long *sum = reinterpret_cast<unsigned long long *>(buf.as<char>() + 16);
     {
         weight_stats<<<g->sm_count * 8, 256, 0, g->stream>>>(g->index.as<int64_t>(), g->wgt.as<int32_t>(), g->N,
@@ -754,14 +718,13 @@ hc_status ensure_weight_stats(hc_graph *g) {
         ::hc::count_launch();
     }
     HC_CUDA_TRY(cudaGetLastError());
-    int hf[3] = {0, 0, 0};
+    int hf[2] = {0, 0};
     unsigned long long hsum = 0;
-    HC_CUDA_TRY(cudaMemcpyAsync(hf, flags, 12, cudaMemcpyDeviceToHost, g->stream));
+    HC_CUDA_TRY(cudaMemcpyAsync(hf, flags, 8, cudaMemcpyDeviceToHost, g->stream));
     HC_CUDA_TRY(cudaMemcpyAsync(&hsum, sum, 8, cudaMemcpyDeviceToHost, g->stream));
     HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
     g->w_negative = hf[0];
     g->w_max = hf[1];
-    g->w_min = hf[2] == kInfDist ? 0 : hf[2];
     // Symmetric weights (w(u->v) == w(v->u) for every edge): one hashing pass.
     bool st = false, ws = false;
     HC_TRY(edge_symmetry(g, reinterpret_cast<const uint32_t *>(g->wgt.ptr), &st, &ws));
@@ -823,7 +786,6 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
     a.ctl = g->ws_ctl.as<SsspCtl>();
     a.plan = g->pr_view;
     a.max_epochs = o.max_epochs > 0 ? o.max_epochs : 0x7fffffff;
-    a.w_min = g->w_min;
     // The pull sweep reads w(u->v) from v's row: only valid when weights are symmetric.
     // Zero fields: the handle's tuned values, else the defaults.
     if (o.pull_alpha == 0) o.pull_alpha = g->tune.sssp_pull_alpha;
