@@ -392,7 +392,7 @@ hc_status ensure_pr_derived(hc_graph *g, bool weighted) {
 int64_t hc_graph::bytes_held() const {
     const hc::DevBuf *bufs[] = {&index, &nbr, &wgt, &inv_deg, &inv_wsum, &wtn, &wf32, &pr_plan,
                                 &pr_plan_huge_rows, &pr_ord, &ws_bfs, &ws_sssp, &ws_pr, &ws_batch,
-                                &ws_out0, &ws_out1, &ws_ctl, &ws_plan_ms, &ws_plan_mssp, &ws_src};
+                                &ws_out0, &ws_out1, &ws_ctl, &ws_plan_ms, &ws_plan_mssp, &ws_src, &sssp_adj};
     int64_t t = 0;
     for (auto *b : bufs) t += (int64_t)b->bytes;
     for (int s = 0; s < 2; s++)

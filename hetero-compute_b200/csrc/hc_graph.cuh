@@ -82,6 +82,10 @@ struct hc_graph {
     int32_t w_max = 0;         // largest weight (0 when none is positive)
     double w_mean = 0.0;
     int w_symmetric = 0;       // w(u->v) == w(v->u) for every edge (rows sorted)
+    // SSSP pull sweeps: int2[M + 64] (neighbour, weight) pairs of each row in
+    // weight-bucket order (stable), built on the first pull-enabled call
+    hc::DevBuf sssp_adj;
+    int sssp_adj_ready = 0;
 
     // batched-BFS hub plan (rows above its split threshold, (row, chunk) tasks)
     hc::DevBuf ws_plan_ms;

@@ -44,6 +44,7 @@ struct SsspCtl {
     int need_pull, resume;
     int finished;  // the run is over: later launches of the chain return at once
     int saved_E, saved_phase, saved_pulls, saved_T;
+    int saved_fgen;  // the far-pile claim the resumed launch uses
     unsigned long long t_start;
     int qlen[3];
     int tasks[3];
@@ -70,6 +71,8 @@ struct SsspArgs {
     int2 *tasks;
     SsspCtl *ctl;
     PrPlanDev plan;
+    const int2 *adj;  // pull sweeps: (neighbour, weight) pairs of each row in weight-bucket order
+    int ws;           // bucket shift: bucket(w) = w >> ws < 256
     int32_t src;
     int32_t delta;  // <= 0: no far pile (plain frontier Bellman-Ford)
     int pull_alpha;  // <= 0: push only
@@ -139,20 +142,34 @@ struct RelaxVisit {
     }
 };
 
+// Weight buckets of the pull sweeps' pair array: bucket(w) = w >> ws, ws the
+// shift that brings the largest weight below 256, non-decreasing along each
+// row.  Every pair at or after one of bucket b has weight >= b << ws.
+__device__ __forceinline__ int wbucket(int32_t w, int ws) { return w >> ws; }
+__device__ __forceinline__ int32_t wbucket_floor(int bk, int ws) { return bk << ws; }
+
+// dist[u] + w for a pair whose weight is below `bound`, else INT32_MAX
+// without touching dist: a candidate is at least its weight, so a pair with
+// w >= bound cannot lower a row whose best so far is `bound`.
 // The gather goes through L1 (.ca): most edges point at a few thousand hub
 // rows, whose distances then stay on the SM.  A value cached earlier in the
 // same sweep can be stale, but distances only fall, so it is an upper bound,
 // and the row that lowered it is marked changed and relaxed again next epoch;
-// the grid barrier's fence invalidates L1 between epochs.
-__device__ __forceinline__ int32_t pull_val(const SsspArgs &a, int64_t e) {
-    return sat_add(__ldca(a.dist + a.nbr[e]), a.w[e]);
+// kernel boundaries and the grid barrier's fence invalidate L1 between epochs.
+__device__ __forceinline__ int32_t pull_cand(const SsspArgs &a, int2 p, int32_t bound) {
+    return p.y < bound ? sat_add(__ldca(a.dist + p.x), p.y) : kInfDist;
 }
 
 // One Bellman-Ford pull over every row with edges (the reference's epoch,
-// src/kernels/gpu/sssp.cuh:120-281), on the shared row plan: hub chunks and
-// long rows reduce with a warp min and lower dist by atomicMin; stream groups
-// (32 rows, one warp) reduce with a segmented warp min and own their rows and
-// their changed-bitmap word.  Lowered vertices are marked in `changed`.
+// src/kernels/gpu/sssp.cuh:120-281), on the shared row plan, over the rows'
+// pairs in weight-bucket order.  Hub chunks and long rows walk their range
+// 128 pairs at a time with a running bound (the row's distance, then the best
+// candidate): pairs at or above it gather nothing, and the walk stops at the
+// first window whose leading bucket floor reaches it.  They lower dist by
+// atomicMin.  Stream groups (32 rows, one warp) read every pair, gather only
+// those below their row's bound and keep each row's minimum in shared memory;
+// they own their rows and their changed-bitmap word.  Lowered vertices are marked
+// in `changed`.
 template <bool kStats>
 __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwarps, int32_t (*s_acc)[32],
                                            unsigned long long &my_e) {
@@ -163,31 +180,47 @@ __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwa
         if (item < p.n_tasks + p.n_long) {
             int32_t r;
             int64_t b, e;
+            // The leading weight of the next window, read one window ahead so
+            // that the stop test comes before the window's loads.  A long row
+            // always takes its first window; a hub row's later chunk tests its
+            // first one too (it starts among the row's heavier pairs).
+            const int32_t *wcol = reinterpret_cast<const int32_t *>(a.adj) + 1;
+            bool test_first = false;
             if (item < p.n_tasks) {
                 const int2 tk = p.tasks[item];
                 r = p.hubs[tk.x].row;
                 const int64_t rb = a.index[r], re = a.index[r + 1];
                 b = rb + (int64_t)tk.y * kHubChunk;
                 e = min(re, b + (int64_t)kHubChunk);
+                test_first = tk.y > 0;
             } else {
                 r = p.longrows[item - p.n_tasks];
                 b = a.index[r];
                 e = a.index[r + 1];
             }
-            int32_t m0 = kInfDist, m1 = kInfDist, m2 = kInfDist, m3 = kInfDist;
-            int64_t i = b + lane;
-            for (; i + 96 < e; i += 128) {
-                m0 = min(m0, pull_val(a, i));
-                m1 = min(m1, pull_val(a, i + 32));
-                m2 = min(m2, pull_val(a, i + 64));
-                m3 = min(m3, pull_val(a, i + 96));
+            int32_t wnext = test_first ? wcol[2 * b] : 0;
+            const int32_t d0 = __shfl_sync(kFull, __ldcg(a.dist + r), 0);
+            int32_t bound = d0;
+            int64_t i0 = b;
+            for (; i0 < e; i0 += 128) {
+                // Pair i0 carries the smallest bucket of the rest of the range.
+                if ((i0 > b || test_first) && wbucket_floor(wbucket(wnext, a.ws), a.ws) >= bound) break;
+                int2 q[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int64_t i = i0 + 32 * j + lane;
+                    q[j] = i < e ? a.adj[i] : make_int2(0, kInfDist);
+                }
+                if (i0 + 128 < e) wnext = wcol[2 * (i0 + 128)];
+                int32_t m = kInfDist;
+#pragma unroll
+                for (int j = 0; j < 4; j++) m = min(m, pull_cand(a, q[j], bound));
+                bound = min(bound, warp_min(m));
             }
-            for (; i < e; i += 32) m0 = min(m0, pull_val(a, i));
-            const int32_t m = warp_min(min(min(m0, m1), min(m2, m3)));
             if (lane == 0) {
-                if (m < __ldcg(a.dist + r) && m < atomicMin(a.dist + r, m))
+                if (bound < d0 && bound < __ldcg(a.dist + r) && bound < atomicMin(a.dist + r, bound))
                     atomicOr(a.changed + (r >> 5), 1u << (r & 31));
-                if (kStats) my_e += (unsigned long long)(e - b);
+                if (kStats) my_e += (unsigned long long)(min(i0, e) - b);
             }
         } else {
             const int32_t r0 = p.stream[item - p.n_tasks - p.n_long] * 32;
@@ -196,47 +229,48 @@ __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwa
             const int64_t s0 = a.index[r0];
             const int32_t rel = (int32_t)(a.index[rc] - s0);
             const int32_t gend = (int32_t)(a.index[min(r0 + 32, a.n_active)] - s0);
+            // This lane's row: its distance at the start, then the best found.
+            int32_t rbound = r < a.n_active ? __ldcg(a.dist + r) : kInfDist;
+            const int32_t rd0 = rbound;
             s_acc[wib][lane] = kInfDist;
             __syncwarp();
-            // Four 32-edge chunks per pass: their loads and gathers are issued
-            // together, then each chunk is reduced by its segmented scan.
+            // Four 32-pair chunks per pass: the pair loads go out first, then
+            // each pair finds its row among the group's offsets, then the
+            // gathers below the row's bound.
             for (int k0 = 0; k0 < gend; k0 += 128) {
+                int2 q[4];
+                int owner[4];
                 int32_t vals[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const int k = k0 + 32 * j + lane;
-                    vals[j] = k < gend ? pull_val(a, s0 + k) : kInfDist;
+                    q[j] = k < gend ? a.adj[s0 + k] : make_int2(0, kInfDist);
                 }
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
-                    const int kb = k0 + 32 * j;
-                    if (kb >= gend) break;
-                    const int k = kb + lane;
-                    const bool act = k < gend;
+                    const int k = k0 + 32 * j + lane;
                     int lo = 0;
 #pragma unroll
                     for (int st = 16; st > 0; st >>= 1) {
                         const int c = __shfl_sync(kFull, rel, lo + st);
                         if (c <= k) lo += st;
                     }
-                    const int owner = act ? lo : 32;
-                    int32_t v = vals[j];
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int32_t y = __shfl_up_sync(kFull, v, o);
-                        const int ow = __shfl_up_sync(kFull, owner, o);
-                        if (lane >= o && ow == owner) v = min(v, y);
-                    }
-                    const int next_owner = __shfl_down_sync(kFull, owner, 1);
-                    if (act && (lane == 31 || next_owner != owner))
-                        s_acc[wib][owner] = min(s_acc[wib][owner], v);
-                    __syncwarp();
+                    owner[j] = k < gend ? lo : 32;
+                    const int32_t ob = __shfl_sync(kFull, rbound, lo);
+                    vals[j] = pull_cand(a, q[j], ob);
                 }
+                // Most pairs sit at or above their row's bound and bring no
+                // candidate: the few that do go to the row's slot by a
+                // shared-memory atomic minimum.
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (vals[j] < kInfDist) atomicMin(&s_acc[wib][owner[j]], vals[j]);
+                __syncwarp();
+                rbound = min(rbound, s_acc[wib][lane]);
             }
-            const int32_t m = s_acc[wib][lane];
             bool ch = false;
-            if (r < a.n_active && m < __ldcg(a.dist + r)) {
-                a.dist[r] = m;  // the group is the only writer of its rows
+            if (r < a.n_active && rbound < rd0 && rbound < __ldcg(a.dist + r)) {
+                a.dist[r] = rbound;  // the group is the only writer of its rows
                 ch = true;
             }
             const unsigned bal = __ballot_sync(kFull, ch);
@@ -264,6 +298,8 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
     const bool use_far = a.delta > 0;
     int32_t T = use_far ? a.delta : kInfDist;
     int E = 0, phase = 0, pulls = 0;
+    // Far-pile claim: a vertex is in the current pile when fstamp[v] == fgen.
+    int fgen = 1;
     unsigned long long my_v = 0, my_e = 0;
     // Every block reads the same control words (written before this launch).
     if (__ldcg(&ctl->finished) || __ldcg(&ctl->gs.err)) return;  // a speculative launch past the end
@@ -293,6 +329,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
         phase = __ldcg(&ctl->saved_phase);
         pulls = __ldcg(&ctl->saved_pulls);
         T = __ldcg(&ctl->saved_T);
+        fgen = __ldcg(&ctl->saved_fgen);
         t_start = __ldcg(&ctl->t_start);
         if (!grid_barrier(&ctl->gs)) return;  // everyone has read the saved state
         if (gtid == 0) ctl->need_pull = 0;
@@ -354,8 +391,8 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
                                 near = sp[k] < next_e;
                                 if (near) a.stamp[v] = next_e;
                             } else {
-                                far = sp[k] < phase + 1;
-                                if (far) a.fstamp[v] = phase + 1;
+                                far = sp[k] < fgen;
+                                if (far) a.fstamp[v] = fgen;
                             }
                             if (near) mf_next += (unsigned long long)(a.index[v + 1] - a.index[v]);
                         }
@@ -450,7 +487,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
                         bool to_near = false, to_far = false;
                         if (v[k] >= 0) {
                             if (d[k] >= T_old && d[k] < T) to_near = atomicMax(a.stamp + v[k], E) < E;
-                            else if (d[k] >= T) to_far = atomicMax(a.fstamp + v[k], phase + 2) < phase + 2;
+                            else if (d[k] >= T) to_far = atomicMax(a.fstamp + v[k], fgen + 1) < fgen + 1;
                             if (to_near) mf_split += (unsigned long long)(a.index[v[k] + 1] - a.index[v[k]]);
                         }
                         const uint32_t nm = __ballot_sync(kFull, to_near), fm = __ballot_sync(kFull, to_far);
@@ -490,6 +527,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
                 ctl->min_far = kInfDist;
             }
             phase++;
+            fgen++;
             nq = __ldcg(&ctl->qlen[cur]);
             if (nq == 0) continue;
         }
@@ -520,13 +558,17 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
                 ctl->saved_phase = phase;
                 ctl->saved_pulls = pulls + 1;
                 ctl->saved_T = T;
+                // The pull sweep propagates every distance it starts from, so
+                // the pull launch empties the far pile; the rows it lowers
+                // rejoin under a new claim.
+                ctl->saved_fgen = fgen + 1;
                 ctl->resume = 1;
                 ctl->need_pull = 1;
             }
             break;
         } else {
             RelaxVisit relax{a.index, a.nbr, a.w, a.dist, a.stamp, a.fstamp, qnext, &ctl->qlen[nxt], fpile,
-                             fpile_len, T, next_e, phase + 1, use_far, 0ull, 0ull};
+                             fpile_len, T, next_e, fgen, use_far, 0ull, 0ull};
             expand_small(a.index, qcur, nq, a.tasks, &ctl->tasks[cur], gwarp, nwarps, relax);
             unsigned long long mfb = block_sum(relax.mf, s_red);
             if (threadIdx.x == 0 && mfb) atomicAdd(&ctl->mf[nxt], mfb);
@@ -562,12 +604,17 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
 // that it runs at the occupancy of a small kernel instead of the persistent
 // kernel's; lowered rows are marked in `changed`.
 template <bool kStats>
-__global__ void __launch_bounds__(kPullThreads) sssp_pull_kernel(SsspArgs a) {
+__global__ void __launch_bounds__(kPullThreads, 6) sssp_pull_kernel(SsspArgs a) {
     __shared__ int32_t s_acc[kPullThreads / 32][32];
     __shared__ unsigned long long s_red[32];
     // A speculative launch with no pull epoch pending returns at once.
     if (!__ldcg(&a.ctl->need_pull) || __ldcg(&a.ctl->gs.err)) return;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    // Every distance this sweep starts from reaches all its neighbours' rows
+    // (a value that falls during the sweep marks its row changed), so the far
+    // pile's entries need no later relaxation: drop them.  The resumed launch
+    // re-queues the lowered rows under a new far claim.
+    if (gtid == 0) a.ctl->far_len[__ldcg(&a.ctl->saved_phase) & 1] = 0;
     unsigned long long my_e = 0;
     pull_sweep<kStats>(a, gtid >> 5, (gridDim.x * blockDim.x) >> 5, s_acc, my_e);
     if (kStats) {
@@ -645,6 +692,65 @@ __global__ void weight_stats(const int64_t *index, const int32_t *w, int32_t n, 
     if (threadIdx.x == 0 && s) atomicAdd(sum, s);
 }
 
+// The pull sweeps' pair array: each row's (neighbour, weight) pairs ordered
+// by weight bucket, stable within a bucket (CSR order), so the result is the
+// same on every run.  One warp per row: a bucket histogram in shared memory,
+// its exclusive scan, then a stable scatter 32 pairs at a time (lanes of one
+// bucket take consecutive slots in lane order).
+constexpr int kOrderThreads = 256;
+__global__ void __launch_bounds__(kOrderThreads) weight_order_rows(const int64_t *index, const int32_t *nbr,
+                                                                   const int32_t *w, int32_t n, int ws,
+                                                                   int2 *adj) {
+    __shared__ int s_cnt[kOrderThreads / 32][256];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int *cnt = s_cnt[wib];
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const int64_t b = index[v], e = index[v + 1];
+        if (e - b <= 1) {
+            if (e > b && lane == 0) adj[b] = make_int2(nbr[b], w[b]);
+            continue;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) cnt[lane * 8 + k] = 0;
+        __syncwarp();
+        for (int64_t i = b + lane; i < e; i += 32) atomicAdd(&cnt[wbucket(w[i], ws)], 1);
+        __syncwarp();
+        int loc[8], tot = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            loc[k] = tot;
+            tot += cnt[lane * 8 + k];
+        }
+        int incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < 8; k++) cnt[lane * 8 + k] = incl - tot + loc[k];
+        __syncwarp();
+        for (int64_t i0 = b; i0 < e; i0 += 32) {
+            const int64_t i = i0 + lane;
+            const bool act = i < e;
+            int2 q = make_int2(0, 0);
+            int bk = -1;
+            if (act) {
+                q = make_int2(nbr[i], w[i]);
+                bk = wbucket(q.y, ws);
+            }
+            const unsigned peers = __match_any_sync(kFull, bk);
+            if (act) adj[b + cnt[bk] + __popc(peers & ((1u << lane) - 1u))] = q;
+            __syncwarp();
+            if (act && (peers >> lane) == 1u) cnt[bk] += __popc(peers);  // the bucket's highest lane
+            __syncwarp();
+        }
+        __syncwarp();
+    }
+}
+
 template <bool kStats>
 hc_status launch_sssp(hc_graph *g, const SsspArgs &args) {
     static int blocks_per_sm[2] = {0, 0};
@@ -704,6 +810,29 @@ hc_status run_source(hc_graph *g, const SsspArgs &a, volatile int *h_flags) {
 }
 
 }  // namespace
+
+// The bucket shift for weights in [0, w_max]: the smallest ws with w_max >> ws < 256.
+int weight_shift(int32_t w_max) {
+    int ws = 0;
+    while ((w_max >> ws) > 255) ws++;
+    return ws;
+}
+
+// Builds the pull sweeps' weight-ordered pair array once per graph (after the
+// weight statistics, which give the bucket shift).
+hc_status ensure_weight_order(hc_graph *g) {
+    if (g->sssp_adj_ready) return HC_OK;
+    HC_TRY(g->sssp_adj.ensure(sizeof(int2) * ((size_t)g->M + 64)));
+    {
+        weight_order_rows<<<g->sm_count * 8, kOrderThreads, 0, g->stream>>>(
+            g->index.as<int64_t>(), g->nbr.as<int32_t>(), g->wgt.as<int32_t>(), g->N, weight_shift(g->w_max),
+            g->sssp_adj.as<int2>());
+        ::hc::count_launch();
+    }
+    HC_CUDA_TRY(cudaGetLastError());
+    g->sssp_adj_ready = 1;
+    return HC_OK;
+}
 
 hc_status ensure_weight_stats(hc_graph *g) {
     if (g->wstats_done) return HC_OK;
@@ -791,6 +920,11 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
     if (o.pull_alpha == 0) o.pull_alpha = g->tune.sssp_pull_alpha;
     if (o.delta == 0) o.delta = g->tune.sssp_delta;
     a.pull_alpha = !g->w_symmetric ? 0 : (o.pull_alpha == 0 ? kDefaultPullAlpha : std::max(o.pull_alpha, 0));
+    if (a.pull_alpha > 0) {
+        HC_TRY(ensure_weight_order(g));
+        a.adj = g->sssp_adj.as<int2>();
+        a.ws = weight_shift(g->w_max);
+    }
     if (o.delta == 0) {
         const double davg = g->n_active ? (double)g->M / (double)g->n_active : 1.0;
         a.delta = (int32_t)std::max(1.0, std::min(1e9, g->w_mean * 32.0 / std::max(davg, 1.0)));

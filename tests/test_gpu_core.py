@@ -193,6 +193,39 @@ def test_sssp_pull_on_unsorted_rows():
         assert np.array_equal(dist[i], oracle.sssp_dijkstra(host.index, nbr, w, s)), i
 
 
+def _sym_weights(host, kind):
+    """Symmetric weights (a hash of the unordered pair) of a chosen distribution."""
+    row = np.repeat(np.arange(host.num_nodes, dtype=np.int64), np.diff(host.index))
+    col = host.neighbors.astype(np.int64)
+    lo, hi = np.minimum(row, col), np.maximum(row, col)
+    h = (lo * 1000003 + hi * 7919) % 2147483629
+    h = (h * 48271) % 2147483647
+    if kind == "zeros":
+        return (h % 3).astype(np.int32)  # 0, 1, 2
+    if kind == "wide":
+        return (h % (1 << 20)).astype(np.int32)
+    if kind == "equal":
+        return np.full(host.num_edges, 7, dtype=np.int32)
+    # skewed: mostly 1, one in 50 near the top of a wide range
+    return np.where(h % 50 == 0, (1 << 18) + h % 1000, 1).astype(np.int32)
+
+
+@pytest.mark.parametrize("kind", ["zeros", "wide", "equal", "skewed"])
+def test_sssp_weight_ordered_pulls_exact(kind):
+    """Pull sweeps read each row's pairs in weight-bucket order and stop a row once the bucket floor reaches its
+    best distance: exact for zero weights, a wide range, equal weights (one bucket) and a skewed mix."""
+    host = hc.gen_kronecker(12, 8, 11)
+    w = _sym_weights(host, kind)
+    g = hc.Graph(host.index, host.neighbors, w)
+    src = hc.pick_sources(host, 4)
+    for pull_alpha in (1000000, 0, 2):
+        dist, parent, _ = g.sssp(src, pull_alpha=pull_alpha, want_parent=True)
+        for i, s in enumerate(src):
+            d = oracle.sssp_dijkstra(host.index, host.neighbors, w, s)
+            assert np.array_equal(dist[i], d), (kind, pull_alpha, i)
+            assert oracle.verify_sp_tree(host.index, host.neighbors, w, d, parent[i], s) == 0
+
+
 def test_sssp_grid_against_dijkstra():
     host = hc.gen_grid(200, 300, 3, wtype=hc.W_I32)
     g = hc.Graph.from_host(host)
