@@ -53,6 +53,9 @@ struct SsspCtl {
     int min_far;
     int epochs, phases, pulls;
     unsigned long long vproc, erelax;
+    // Degree sum of the rows a pull sweep lowered below the near threshold:
+    // the next epoch's push-or-pull test, without building its queue.
+    unsigned long long pull_mf;
     struct {
         int nq, phase;
         unsigned long long t_ns;
@@ -172,7 +175,7 @@ __device__ __forceinline__ int32_t pull_cand(const SsspArgs &a, int2 p, int32_t 
 // in `changed`.
 template <bool kStats>
 __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwarps, int32_t (*s_acc)[32],
-                                           unsigned long long &my_e) {
+                                           unsigned long long &my_e, int32_t T, unsigned long long &my_mf) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const PrPlanDev &p = a.plan;
     const int total = p.n_tasks + p.n_long + p.n_stream;
@@ -218,8 +221,11 @@ __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwa
                 bound = min(bound, warp_min(m));
             }
             if (lane == 0) {
-                if (bound < d0 && bound < __ldcg(a.dist + r) && bound < atomicMin(a.dist + r, bound))
-                    atomicOr(a.changed + (r >> 5), 1u << (r & 31));
+                if (bound < d0 && bound < __ldcg(a.dist + r) && bound < atomicMin(a.dist + r, bound)) {
+                    const uint32_t bit = 1u << (r & 31);
+                    if (!(atomicOr(a.changed + (r >> 5), bit) & bit) && bound < T)
+                        my_mf += (unsigned long long)(a.index[r + 1] - a.index[r]);
+                }
                 if (kStats) my_e += (unsigned long long)(min(i0, e) - b);
             }
         } else {
@@ -269,9 +275,11 @@ __device__ __forceinline__ void pull_sweep(const SsspArgs &a, int gwarp, int nwa
                 rbound = min(rbound, s_acc[wib][lane]);
             }
             bool ch = false;
+            const int32_t rnext = __shfl_down_sync(kFull, rel, 1);
             if (r < a.n_active && rbound < rd0 && rbound < __ldcg(a.dist + r)) {
                 a.dist[r] = rbound;  // the group is the only writer of its rows
                 ch = true;
+                if (rbound < T) my_mf += (unsigned long long)((lane == 31 ? gend : rnext) - rel);
             }
             const unsigned bal = __ballot_sync(kFull, ch);
             if (lane == 0) {
@@ -305,6 +313,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
     if (__ldcg(&ctl->finished) || __ldcg(&ctl->gs.err)) return;  // a speculative launch past the end
     const bool resumed = __ldcg(&ctl->resume) != 0;
     unsigned long long t_start;
+    unsigned long long pull_mf = 0;  // read before the barrier below; block 0 may reset it after
     if (!resumed) {
         for (int i = gtid; i < a.n; i += nthreads) {
             a.dist[i] = kInfDist;
@@ -330,6 +339,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
         pulls = __ldcg(&ctl->saved_pulls);
         T = __ldcg(&ctl->saved_T);
         fgen = __ldcg(&ctl->saved_fgen);
+        pull_mf = __ldcg(&ctl->pull_mf);
         t_start = __ldcg(&ctl->t_start);
         if (!grid_barrier(&ctl->gs)) return;  // everyone has read the saved state
         if (gtid == 0) ctl->need_pull = 0;
@@ -343,6 +353,33 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
         const int next_e = E + 1;
         if (after_pull) {
             after_pull = false;
+            // When the rows the pull lowered already make the next epoch a
+            // pull, that sweep propagates their values anyway: clear the
+            // changed bitmap and hand over at once, without queueing them.
+            if (a.pull_alpha > 0 && (double)pull_mf * (double)a.pull_alpha > (double)a.m && E + 1 < a.max_epochs) {
+                for (int w = gtid; w < W_act; w += nthreads) a.changed[w] = 0;
+                E++;
+                if (gtid == 0) {
+                    const int old_slot = (E + 2) % 3;
+                    ctl->qlen[old_slot] = 0;
+                    ctl->tasks[old_slot] = 0;
+                    ctl->mf[old_slot] = 0;
+                    if (E < kTraceEpochs) {
+                        ctl->trace[E].nq = 0;
+                        ctl->trace[E].phase = -1 - phase;
+                        ctl->trace[E].t_ns = globaltimer_ns();
+                    }
+                    ctl->saved_E = E;
+                    ctl->saved_phase = phase;
+                    ctl->saved_pulls = pulls + 1;
+                    ctl->saved_T = T;
+                    ctl->saved_fgen = fgen + 1;
+                    ctl->pull_mf = 0;
+                    ctl->resume = 1;
+                    ctl->need_pull = 1;
+                }
+                break;
+            }
             int32_t *fpile = (phase & 1) ? a.far1 : a.far0;
             int *fpile_len = &ctl->far_len[phase & 1];
             // Lowered vertices back into the near queue / far pile.  A warp
@@ -562,6 +599,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
                 // the pull launch empties the far pile; the rows it lowers
                 // rejoin under a new claim.
                 ctl->saved_fgen = fgen + 1;
+                ctl->pull_mf = 0;
                 ctl->resume = 1;
                 ctl->need_pull = 1;
             }
@@ -615,9 +653,12 @@ __global__ void __launch_bounds__(kPullThreads, 6) sssp_pull_kernel(SsspArgs a) 
     // pile's entries need no later relaxation: drop them.  The resumed launch
     // re-queues the lowered rows under a new far claim.
     if (gtid == 0) a.ctl->far_len[__ldcg(&a.ctl->saved_phase) & 1] = 0;
-    unsigned long long my_e = 0;
-    pull_sweep<kStats>(a, gtid >> 5, (gridDim.x * blockDim.x) >> 5, s_acc, my_e);
+    unsigned long long my_e = 0, my_mf = 0;
+    pull_sweep<kStats>(a, gtid >> 5, (gridDim.x * blockDim.x) >> 5, s_acc, my_e, __ldcg(&a.ctl->saved_T), my_mf);
+    const unsigned long long mf = block_sum(my_mf, s_red);
+    if (threadIdx.x == 0 && mf) atomicAdd(&a.ctl->pull_mf, mf);
     if (kStats) {
+        __syncthreads();
         const unsigned long long e = block_sum(my_e, s_red);
         if (threadIdx.x == 0 && e) atomicAdd(&a.ctl->erelax, e);
     }
