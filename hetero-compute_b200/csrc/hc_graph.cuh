@@ -164,4 +164,8 @@ const float *pr_weights(const hc_graph *g);
 hc_status ensure_plan(hc_graph *g);
 // Computes w_negative, w_max, w_mean and w_symmetric once (int32 weights).
 hc_status ensure_weight_stats(hc_graph *g);
+// The pull sweeps' weight-ordered (neighbour, weight) pairs (hc_graph::sssp_adj),
+// after the weight statistics; bucket(w) = w >> weight_shift(w_max) < 256.
+hc_status ensure_weight_order(hc_graph *g);
+int weight_shift(int32_t w_max);
 }  // namespace hc

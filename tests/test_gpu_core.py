@@ -218,12 +218,17 @@ def test_sssp_weight_ordered_pulls_exact(kind):
     w = _sym_weights(host, kind)
     g = hc.Graph(host.index, host.neighbors, w)
     src = hc.pick_sources(host, 4)
+    ref = [oracle.sssp_dijkstra(host.index, host.neighbors, w, s) for s in src]
     for pull_alpha in (1000000, 0, 2):
         dist, parent, _ = g.sssp(src, pull_alpha=pull_alpha, want_parent=True)
         for i, s in enumerate(src):
-            d = oracle.sssp_dijkstra(host.index, host.neighbors, w, s)
-            assert np.array_equal(dist[i], d), (kind, pull_alpha, i)
-            assert oracle.verify_sp_tree(host.index, host.neighbors, w, d, parent[i], s) == 0
+            assert np.array_equal(dist[i], ref[i]), (kind, pull_alpha, i)
+            assert oracle.verify_sp_tree(host.index, host.neighbors, w, ref[i], parent[i], s) == 0
+    # Batched pulls skip a lane's words of a neighbour whose weight reaches the lane's largest distance.
+    for switch_alpha, bits in ((1000000, 0), (0, 0), (1000000, 32)):
+        db, _ = g.sssp_batched(src, switch_alpha=switch_alpha, dist_bits=bits)
+        for i in range(len(src)):
+            assert np.array_equal(db[i], ref[i]), (kind, "batched", switch_alpha, bits, i)
 
 
 def test_sssp_grid_against_dijkstra():
