@@ -600,6 +600,7 @@ extern "C" hc_status hc_bfs_batched(hc_graph *g, const int32_t *sources, int32_t
                                     const hc_batch_opts *opts, hc_batch_stats *stats) {
     clear_error();
     HC_TRY(activate(g));
+    ReclaimScope reclaim_scope(g, kKeepBatch);
     if (!sources || num_sources < 1) return fail(HC_ERR_INVALID_ARG, "hc_bfs_batched: bad source list");
     hc_batch_opts o{};
     if (opts) o = *opts;

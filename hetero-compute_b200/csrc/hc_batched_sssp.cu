@@ -828,6 +828,7 @@ extern "C" hc_status hc_sssp_batched(hc_graph *g, const int32_t *sources, int32_
                                      const hc_batch_opts *opts, hc_batch_stats *stats) {
     clear_error();
     HC_TRY(activate(g));
+    ReclaimScope reclaim_scope(g, kKeepBatch);
     if (!sources || num_sources < 1) return fail(HC_ERR_INVALID_ARG, "hc_sssp_batched: bad source list");
     if (g->wtype != HC_W_I32) return fail(HC_ERR_UNSUPPORTED, "hc_sssp_batched: graph needs int32 edge weights");
     hc_batch_opts o{};

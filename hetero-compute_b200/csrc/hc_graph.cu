@@ -21,11 +21,58 @@ bool is_device_pointer(const void *p) {
     return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
+namespace {
+// The graph whose derived arrays an allocation of this thread may release,
+// and what its running call needs (set by ReclaimScope).
+thread_local hc_graph *t_reclaim_g = nullptr;
+thread_local unsigned t_reclaim_keep = 0;
+
+// Releases what the running call does not need; true if anything was freed.
+bool reclaim(hc_graph *g, unsigned keep, const DevBuf *self) {
+    bool freed = false;
+    auto drop = [&](DevBuf &b) {
+        if (&b != self && b.ptr) {
+            b.release();
+            freed = true;
+        }
+    };
+    if (!(keep & kKeepAdj) && &g->sssp_adj != self) {
+        drop(g->sssp_adj);
+        g->sssp_adj_ready = 0;
+    }
+    if (!(keep & kKeepPrOrd) && &g->pr_ord != self) {
+        drop(g->pr_ord);
+        g->pr_ord_levels = -1;
+    }
+    if (!(keep & kKeepPrWeighted) && &g->wtn != self && &g->inv_wsum != self && &g->wf32 != self) {
+        drop(g->wtn);
+        drop(g->inv_wsum);
+        drop(g->wf32);
+    }
+    if (!(keep & kKeepBatch)) drop(g->ws_batch);
+    return freed;
+}
+}  // namespace
+
+ReclaimScope::ReclaimScope(hc_graph *g, unsigned keep) : prev_g(t_reclaim_g), prev_keep(t_reclaim_keep) {
+    t_reclaim_g = g;
+    t_reclaim_keep = keep;
+}
+
+ReclaimScope::~ReclaimScope() {
+    t_reclaim_g = prev_g;
+    t_reclaim_keep = prev_keep;
+}
+
 hc_status DevBuf::ensure(size_t want) {
     if (want <= bytes && ptr) return HC_OK;
     release();
     size_t b = std::max<size_t>(want, 256);
     cudaError_t e = cudaMalloc(&ptr, b);
+    if (e == cudaErrorMemoryAllocation && t_reclaim_g && reclaim(t_reclaim_g, t_reclaim_keep, this)) {
+        cudaGetLastError();
+        e = cudaMalloc(&ptr, b);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         ptr = nullptr;

@@ -164,6 +164,20 @@ const float *pr_weights(const hc_graph *g);
 hc_status ensure_plan(hc_graph *g);
 // Computes w_negative, w_max, w_mean and w_symmetric once (int32 weights).
 hc_status ensure_weight_stats(hc_graph *g);
+// Device memory pressure.  Derived arrays that can be built again (the
+// pull sweeps' pair array, the reference-order schedule, the weighted
+// PageRank arrays) and the batched workspace are released, when an
+// allocation fails, unless the running call needs them; the allocation is
+// then tried once more.  A call states what it needs for its lifetime.
+enum : unsigned { kKeepAdj = 1u, kKeepPrOrd = 2u, kKeepPrWeighted = 4u, kKeepBatch = 8u };
+struct ReclaimScope {
+    ReclaimScope(hc_graph *g, unsigned keep);
+    ~ReclaimScope();
+    ReclaimScope(const ReclaimScope &) = delete;
+    ReclaimScope &operator=(const ReclaimScope &) = delete;
+    hc_graph *prev_g;
+    unsigned prev_keep;
+};
 // The pull sweeps' weight-ordered (neighbour, weight) pairs (hc_graph::sssp_adj),
 // after the weight statistics; bucket(w) = w >> weight_shift(w_max) < 256.
 hc_status ensure_weight_order(hc_graph *g);

@@ -948,6 +948,7 @@ extern "C" hc_status hc_pr_forward(hc_graph *g, const float *teleport, int32_t n
                                    const hc_pr_opts *opts, hc_pr_stats *stats) {
     clear_error();
     HC_TRY(activate(g));
+    ReclaimScope reclaim_scope(g, kKeepPrWeighted);
     if (ncols < 1 || !scores_out) return fail(HC_ERR_INVALID_ARG, "hc_pr_forward: bad ncols / output");
     if (ncols > 1 && !teleport) return fail(HC_ERR_INVALID_ARG, "hc_pr_forward: ncols > 1 needs a teleport matrix");
     hc_pr_opts o;
@@ -1112,6 +1113,7 @@ extern "C" hc_status hc_pr_backward(hc_graph *g, const float *scores, const floa
                                     float *dL_dweights, const hc_pr_opts *opts, hc_pr_stats *stats) {
     clear_error();
     HC_TRY(activate(g));
+    ReclaimScope reclaim_scope(g, kKeepPrWeighted);
     if (!scores || !dL_dscores) return fail(HC_ERR_INVALID_ARG, "hc_pr_backward: scores and dL/dscores required");
     hc_pr_opts o;
     fill_opts(opts, &o);
@@ -1238,6 +1240,7 @@ extern "C" hc_status hc_ppr_batched(hc_graph *g, const int32_t *seed_offsets, co
                                     float *scores_out, const hc_pr_opts *opts, hc_pr_stats *stats) {
     clear_error();
     HC_TRY(activate(g));
+    ReclaimScope reclaim_scope(g, kKeepPrWeighted | kKeepBatch);
     if (ncols < 1 || ncols > 256 || !seed_offsets || !seeds || !scores_out)
         return fail(HC_ERR_INVALID_ARG, "hc_ppr_batched: bad arguments (1 <= ncols <= 256)");
     hc_pr_opts o;

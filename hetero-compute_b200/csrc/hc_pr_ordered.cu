@@ -325,6 +325,7 @@ extern "C" hc_status hc_pr_pull_ordered(hc_graph *g, const float *init_scores, f
                                         const hc_pr_opts *opts, hc_pr_stats *stats) {
     clear_error();
     HC_TRY(activate(g));
+    ReclaimScope reclaim_scope(g, kKeepPrOrd);
     if (!scores_out) return fail(HC_ERR_INVALID_ARG, "hc_pr_pull_ordered: null output");
     hc_pr_opts o{};
     if (opts) o = *opts;

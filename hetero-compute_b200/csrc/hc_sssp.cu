@@ -912,6 +912,7 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
                              int32_t *parent_out, const hc_sssp_opts *opts, hc_sssp_stats *stats) {
     clear_error();
     HC_TRY(activate(g));
+    ReclaimScope reclaim_scope(g, kKeepAdj);
     if (!sources || num_sources < 0) return fail(HC_ERR_INVALID_ARG, "hc_sssp: bad source list");
     if (g->wtype != HC_W_I32) return fail(HC_ERR_UNSUPPORTED, "hc_sssp: graph needs int32 edge weights");
     hc_sssp_opts o{};
