@@ -33,6 +33,12 @@ constexpr int kTraceLevels = 64;
 // (the 131072 highest-degree vertices of a degree-sorted graph, which most
 // edges point at) into shared memory and probe them there.
 constexpr int kHubWords = 4096;
+// Every frontier bitmap has a summary: bit i set when one of its words
+// [i << sum_shift, (i + 1) << sum_shift) is non-zero, at most kSumWords words,
+// so bottom-up levels keep it in shared memory and probe the bitmap in global
+// memory only for neighbours whose summary bit is set (on a sparse frontier,
+// few: most rows that find no parent stop reading global memory).
+constexpr int kSumWords = 4096;
 
 struct LevelCnt {
     int nf;                 // vertices in this frontier
@@ -59,6 +65,8 @@ struct BfsArgs {
     int64_t m;
     int32_t *depth, *parent;
     uint32_t *visited, *fb0, *fb1, *fb2;
+    uint32_t *sb0, *sb1, *sb2;  // the frontier bitmaps' summaries (sum_words words each)
+    int sum_shift, sum_words;
     int32_t *q0, *q1;
     int2 *tasks;
     BfsCtl *ctl;
@@ -75,6 +83,29 @@ struct BfsArgs {
 __device__ __forceinline__ uint32_t *fb_sel(const BfsArgs &a, int i) {
     return i == 0 ? a.fb0 : (i == 1 ? a.fb1 : a.fb2);
 }
+__device__ __forceinline__ uint32_t *sb_sel(const BfsArgs &a, int i) {
+    return i == 0 ? a.sb0 : (i == 1 ? a.sb1 : a.sb2);
+}
+
+// Sets vertex v's bit in a frontier bitmap and, when its word was empty, the
+// word's summary bit.
+__device__ __forceinline__ void frontier_add(uint32_t *fb, uint32_t *sb, int cs, int32_t v) {
+    const int w = v >> 5;
+    if (atomicOr(fb + w, 1u << (v & 31)) == 0u) atomicOr(sb + ((w >> cs) >> 5), 1u << ((w >> cs) & 31));
+}
+
+// Word of the frontier bitmap that holds vertex u's bit: the shared copy of
+// the hub prefix for u < hub_v, else 0 when u's summary bit (shared) is clear,
+// else the bitmap in global memory.  u < 0 (no edge) reads as 0.
+__device__ __forceinline__ uint32_t frontier_word_sum(const uint32_t *s_fb, int hub_v, const uint32_t *s_sum, int cs,
+                                                      const uint32_t *fb, int32_t u) {
+    const bool hub = u >= 0 && u < hub_v;
+    const int sw_i = (max(u, 0) >> 5) >> cs;
+    const bool need = u >= 0 && !hub && ((s_sum[sw_i >> 5] >> (sw_i & 31)) & 1u);
+    const uint32_t hw = s_fb[hub ? (u >> 5) : 0];
+    const uint32_t gw = need ? __ldcg(fb + (u >> 5)) : 0u;
+    return hub ? hw : gw;
+}
 
 // Top-down edge visitor: claim an unvisited neighbour with a CAS on its
 // parent, mark it visited and in the next frontier, queue it.
@@ -82,7 +113,8 @@ struct TopDownVisit {
     const int64_t *index;
     const int32_t *nbr;
     int32_t *parent, *depth;
-    uint32_t *visited, *fnext;
+    uint32_t *visited, *fnext, *snext;
+    int cs;
     int32_t *qnext;
     int *qlen;
     int next_depth;
@@ -114,7 +146,7 @@ struct TopDownVisit {
                 const uint32_t bit = 1u << (v[j] & 31);
                 depth[v[j]] = next_depth;
                 atomicOr(visited + (v[j] >> 5), bit);
-                atomicOr(fnext + (v[j] >> 5), bit);
+                frontier_add(fnext, snext, cs, v[j]);
                 mf += (unsigned long long)(index[v[j] + 1] - index[v[j]]);
             }
         }
@@ -126,6 +158,7 @@ template <bool kStats>
 __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
     __shared__ unsigned long long s_red[32];
     __shared__ uint32_t s_fb[kHubWords];
+    __shared__ uint32_t s_sum[kSumWords];
     BfsCtl *ctl = a.ctl;
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -144,6 +177,11 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
         a.fb1[i] = 0;
         a.fb2[i] = 0;
     }
+    for (int i = gtid; i < a.sum_words; i += nthreads) {
+        a.sb0[i] = 0;
+        a.sb1[i] = 0;
+        a.sb2[i] = 0;
+    }
     const unsigned long long t_start = globaltimer_ns();
     if (!grid_barrier(&ctl->gs)) return;
     if (gtid == 0) {
@@ -152,6 +190,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
         a.parent[s] = s;
         a.visited[s >> 5] = 1u << (s & 31);
         a.fb0[s >> 5] = 1u << (s & 31);
+        a.sb0[((s >> 5) >> a.sum_shift) >> 5] = 1u << (((s >> 5) >> a.sum_shift) & 31);
         a.q0[0] = s;
         ctl->cnt[0].nf = 1;
         ctl->cnt[0].mf = (unsigned long long)(a.index[s + 1] - a.index[s]);
@@ -181,7 +220,9 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
             ctl->cnt[old].mf = 0;
         }
         uint32_t *fcur = fb_sel(a, cur), *fnext = fb_sel(a, nxt), *fold = fb_sel(a, old);
+        uint32_t *scur = sb_sel(a, cur), *snext = sb_sel(a, nxt), *sold = sb_sel(a, old);
         for (int i = gtid; i < W_act; i += nthreads) fold[i] = 0;
+        for (int i = gtid; i < a.sum_words; i += nthreads) sold[i] = 0;
         int32_t *qcur = (L & 1) ? a.q1 : a.q0;
         int32_t *qnext = (L & 1) ? a.q0 : a.q1;
 
@@ -216,8 +257,8 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
             edges_to_check -= num_edges;
             td_levels++;
             const int next_depth = L + 1;
-            TopDownVisit visit{a.index, a.nbr, a.parent, a.depth, a.visited, fnext, qnext, &ctl->cnt[nxt].nf,
-                               next_depth, 0ull};
+            TopDownVisit visit{a.index, a.nbr, a.parent, a.depth, a.visited, fnext, snext, a.sum_shift, qnext,
+                               &ctl->cnt[nxt].nf, next_depth, 0ull};
             if (kStats) {
                 for (int i = gtid; i < nf; i += nthreads) {
                     const int32_t u = __ldcg(qcur + i);
@@ -245,7 +286,9 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
             const int hub_w = min(kHubWords, W_act);
             const int hub_v = hub_w << 5;
             for (int i = threadIdx.x; i < hub_w; i += blockDim.x) s_fb[i] = __ldcg(fcur + i);
+            for (int i = threadIdx.x; i < a.sum_words; i += blockDim.x) s_sum[i] = __ldcg(scur + i);
             __syncthreads();
+            const int cs = a.sum_shift;
             // Rows of degree >= 32: warp per vertex, 32 probes per step.
             // AUTO = thread granularity with four probes in flight: on the
             // degree-sorted Kronecker graphs it beats warp-per-row for the
@@ -271,7 +314,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
                     int32_t u = 0;
                     if (i < e) {
                         u = a.nbr[i];
-                        hit = (frontier_word(s_fb, hub_v, fcur, u) >> (u & 31)) & 1u;
+                        hit = (frontier_word_sum(s_fb, hub_v, s_sum, cs, fcur, u) >> (u & 31)) & 1u;
                     }
                     const unsigned bal = __ballot_sync(kFull, hit);
                     if (kStats) probes += bal ? (int64_t)__ffs(bal) : ((e - e0) < 32 ? (e - e0) : (int64_t)32);
@@ -288,7 +331,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
                     a.parent[v] = par;
                     a.depth[v] = next_depth;
                     atomicOr(a.visited + (v >> 5), bit);
-                    atomicOr(fnext + (v >> 5), bit);
+                    frontier_add(fnext, snext, cs, v);
                     found_local++;
                 }
             }
@@ -306,7 +349,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
 #pragma unroll
                         for (int j = 0; j < 4; j++) u[j] = i + j < e ? a.nbr[i + j] : -1;
 #pragma unroll
-                        for (int j = 0; j < 4; j++) wd[j] = frontier_word(s_fb, hub_v, fcur, u[j]);
+                        for (int j = 0; j < 4; j++) wd[j] = frontier_word_sum(s_fb, hub_v, s_sum, cs, fcur, u[j]);
 #pragma unroll
                         for (int j = 0; j < 4; j++)
                             if (par < 0 && u[j] >= 0 && ((wd[j] >> (u[j] & 31)) & 1u)) {
@@ -326,7 +369,10 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_persistent(BfsArgs a) {
                 }
                 if (lane == 0) {
                     fnext[w] = bal;
-                    if (bal) a.visited[w] = vis | bal;
+                    if (bal) {
+                        a.visited[w] = vis | bal;
+                        atomicOr(snext + ((w >> cs) >> 5), 1u << ((w >> cs) & 31));
+                    }
                     found_local += __popc(bal);
                 }
             }
@@ -418,7 +464,11 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
     const int64_t n = g->N;
     const int64_t W = (n + 31) / 32;
     const int64_t ntasks = max_expand_tasks(g->M, n);
-    const size_t bytes = sizeof(uint32_t) * 4 * W + sizeof(int32_t) * 2 * n + sizeof(int2) * ntasks + 1024;
+    int sum_shift = 0;
+    while (((W + (1ll << sum_shift) - 1) >> sum_shift) > (int64_t)kSumWords * 32) sum_shift++;
+    const int sum_words = (int)((((W + (1ll << sum_shift) - 1) >> sum_shift) + 31) / 32);
+    const size_t bytes = sizeof(uint32_t) * 4 * W + sizeof(int32_t) * 2 * n + sizeof(int2) * ntasks +
+                         3 * (sizeof(uint32_t) * (size_t)sum_words + 256) + 1024;
     HC_TRY(g->ws_bfs.ensure(bytes));
     HC_TRY(g->ws_ctl.ensure(4096));
     char *p = g->ws_bfs.as<char>();
@@ -438,6 +488,11 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
     a.fb0 = (uint32_t *)take(4 * W);
     a.fb1 = (uint32_t *)take(4 * W);
     a.fb2 = (uint32_t *)take(4 * W);
+    a.sb0 = (uint32_t *)take(4 * (size_t)sum_words);
+    a.sb1 = (uint32_t *)take(4 * (size_t)sum_words);
+    a.sb2 = (uint32_t *)take(4 * (size_t)sum_words);
+    a.sum_shift = sum_shift;
+    a.sum_words = sum_words;
     a.q0 = (int32_t *)take(4 * n);
     a.q1 = (int32_t *)take(4 * n);
     a.tasks = (int2 *)take(sizeof(int2) * ntasks);
@@ -546,8 +601,12 @@ constexpr int64_t kNoAllocMaxEdges = 1ll << 24;
 constexpr size_t na_align(size_t b) { return (b + 255) / 256 * 256; }
 constexpr size_t kNaWords = (size_t)kNoAllocMaxNodes / 32;
 constexpr size_t kNaTasks = (size_t)(kNoAllocMaxEdges / kTaskEdges + kNoAllocMaxEdges / (kSmallDeg + 1) + 64);
+// Frontier summaries: one bit per bitmap word (kNaWords <= 32 * kSumWords).
+constexpr size_t kNaSumWords = (kNaWords + 31) / 32;
+static_assert(kNaWords <= (size_t)kSumWords * 32, "summary of the fixed-size bitmaps needs a shift");
 constexpr size_t kNoAllocBytes = na_align(sizeof(BfsCtl)) + na_align(sizeof(int)) + 4 * na_align(4 * kNaWords) +
-                                 2 * na_align(4 * (size_t)kNoAllocMaxNodes) + na_align(sizeof(int2) * kNaTasks);
+                                 3 * na_align(4 * kNaSumWords) + 2 * na_align(4 * (size_t)kNoAllocMaxNodes) +
+                                 na_align(sizeof(int2) * kNaTasks);
 
 static __device__ __align__(256) unsigned char g_bfs_scratch[kNoAllocBytes];
 
@@ -625,6 +684,11 @@ extern "C" hc_status hc_bfs_noalloc(const int64_t *index, const int32_t *neighbo
     a.fb0 = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
     a.fb1 = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
     a.fb2 = reinterpret_cast<uint32_t *>(take(4 * kNaWords));
+    a.sb0 = reinterpret_cast<uint32_t *>(take(4 * kNaSumWords));
+    a.sb1 = reinterpret_cast<uint32_t *>(take(4 * kNaSumWords));
+    a.sb2 = reinterpret_cast<uint32_t *>(take(4 * kNaSumWords));
+    a.sum_shift = 0;
+    a.sum_words = (int)((((num_nodes + 31) / 32) + 31) / 32);
     a.q0 = reinterpret_cast<int32_t *>(take(4 * (size_t)kNoAllocMaxNodes));
     a.q1 = reinterpret_cast<int32_t *>(take(4 * (size_t)kNoAllocMaxNodes));
     a.tasks = reinterpret_cast<int2 *>(take(sizeof(int2) * kNaTasks));
