@@ -596,7 +596,8 @@ hc_status hc_graph_destroy(hc_graph *g) {
     if (g->stream && g->stream != g->own_stream) cudaStreamSynchronize(g->stream);
     DevBuf *bufs[] = {&g->index, &g->nbr, &g->wgt, &g->inv_deg, &g->inv_wsum, &g->wtn, &g->wf32, &g->pr_plan,
                       &g->pr_plan_huge_rows, &g->ws_bfs, &g->ws_sssp, &g->ws_pr, &g->ws_batch,
-                      &g->ws_out0, &g->ws_out1, &g->ws_ctl, &g->ws_plan_ms, &g->ws_plan_mssp, &g->ws_src};
+                      &g->ws_out0, &g->ws_out1, &g->ws_ctl, &g->ws_plan_ms, &g->ws_plan_mssp, &g->ws_src,
+                      &g->sssp_adj, &g->pr_ord};
     for (auto *b : bufs) b->release();
     if (g->copy_stream) cudaStreamSynchronize(g->copy_stream);
     for (int s = 0; s < 2; s++) {

@@ -240,6 +240,12 @@ typedef struct hc_sssp_stats {
  * (src/kernels/gpu/sssp.cuh:120-281).  hc_sssp_batched checks its 32-bit
  * groups the same way.
  * parent_out (optional): a shortest-path tree, parent[src] = src.
+ * With pull epochs enabled the first call builds, and the handle keeps, a
+ * second copy of the adjacency for the pull sweeps: each row's (neighbour,
+ * weight) pairs ordered by weight, 8 * (num_edges + 64) bytes.  When a later
+ * call of another kind cannot allocate what it needs, that copy (like the
+ * other arrays a handle derives and can rebuild) is released and built
+ * again by the next hc_sssp.
  * Replaces sssp_pull_gpu (src/kernels/gpu/sssp.cuh:42-100). */
 hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_sources,
                   int32_t *dist_out, int32_t *parent_out,
