@@ -67,24 +67,24 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     return t;
 }
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
-__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Grid-wide barrier for cooperative (co-resident) launches.  Arrival is an
-// atomic on `count`; the last block to arrive resets it and bumps `gen`.
-// Waiters poll `gen` with an acquire load and give up after the wait limit,
-// setting *err.  Once *err is set every later barrier returns at once, so a
-// failed run drains in bounded time.  Returns false when the run must stop.
+// Grid-wide barrier for cooperative (co-resident) launches.  `count` only
+// grows: every block adds one per barrier, so barrier k of a run is complete
+// when count reaches (k + 1) * gridDim.x, and a block computes that target
+// from the value its own arrival returned; no block resets anything, and the
+// waiters see the last arrival itself.  The control block must be zeroed
+// before a run, and every launch of a run must use the same grid size.
+// Waiters poll `count` with an acquire load and give up after the wait
+// limit, setting *err.  Once *err is set every later barrier returns at once,
+// so a failed run drains in bounded time.  Returns false when the run must
+// stop.
 struct GridSync {
-    unsigned count;
-    unsigned gen;
+    unsigned long long count;
     int err;
     int pad;
 };
@@ -97,23 +97,19 @@ __device__ __forceinline__ bool grid_barrier(GridSync *gs) {
         if (*(volatile int *)&gs->err) {
             ok = 0;
         } else {
-            unsigned my_gen = ld_acquire_u32(&gs->gen);
             __threadfence();
-            unsigned arrived = atomicAdd(&gs->count, 1u);
-            if (arrived == gridDim.x - 1) {
-                gs->count = 0;
-                __threadfence();
-                st_release_u32(&gs->gen, my_gen + 1);
-            } else {
+            const unsigned long long t = atomicAdd(&gs->count, 1ull);
+            const unsigned long long target = (t / gridDim.x + 1) * gridDim.x;
+            if (t + 1 != target) {
                 unsigned long long t0 = globaltimer_ns();
-                while (ld_acquire_u32(&gs->gen) == my_gen) {
+                while (ld_acquire_u64(&gs->count) < target) {
                     if (*(volatile int *)&gs->err) { ok = 0; break; }
                     if (globaltimer_ns() - t0 > c_limits.wait_ns) {
                         atomicExch(&gs->err, (int)HC_ERR_TIMEOUT);
                         ok = 0;
                         break;
                     }
-                    __nanosleep(64);
+                    __nanosleep(32);
                 }
             }
             __threadfence();

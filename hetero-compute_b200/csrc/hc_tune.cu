@@ -99,7 +99,14 @@ hc_status tune_bfs(Tuner &tu, hc_tuning &out) {
         }
         o.bu_variant = (hc_variant)var;
     }
-    descend(o, &o.alpha, {4, 8, 15, 30, 60}, best, run);
+    // Cheap sparse bottom-up levels (frontier summaries) make an early switch
+    // pay on large graphs: the range reaches well above the reference's 15.
+    descend(o, &o.alpha, {4, 8, 15, 30, 60, 120, 240}, best, run);
+    {
+        std::vector<int32_t> fine;
+        for (double f : {0.7, 1.4}) fine.push_back((int32_t)std::max(1.0, std::floor(o.alpha * f)));
+        descend(o, &o.alpha, fine, best, run);
+    }
     descend(o, &o.beta, {6, 12, 18, 36, 72}, best, run);
     out.bfs_alpha = o.alpha;
     out.bfs_beta = o.beta;
