@@ -34,7 +34,7 @@ namespace {
 constexpr int kSsspThreads = 512;
 constexpr int kPullThreads = 256;
 constexpr int kTraceEpochs = 96;
-constexpr int kDefaultPullAlpha = 4;
+constexpr int kDefaultPullAlpha = 8;
 // Far piles of at most this many entries end the near/far phases (one last
 // phase takes every remaining vertex).
 #ifndef HC_SSSP_TAIL_PILE

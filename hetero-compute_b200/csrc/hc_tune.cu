@@ -76,7 +76,7 @@ void descend(Opts &opts, int32_t *field, const std::vector<int32_t> &cands, doub
 }
 
 hc_status tune_bfs(Tuner &tu, hc_tuning &out) {
-    const int k = (int)std::min<size_t>(tu.src.size(), 16);
+    const int k = (int)std::min<size_t>(tu.src.size(), 32);
     hc_bfs_opts o{};
     o.alpha = out.bfs_alpha > 0 ? out.bfs_alpha : 15;
     o.beta = out.bfs_beta > 0 ? out.bfs_beta : 18;
@@ -101,7 +101,7 @@ hc_status tune_bfs(Tuner &tu, hc_tuning &out) {
     }
     // Cheap sparse bottom-up levels (frontier summaries) make an early switch
     // pay on large graphs: the range reaches well above the reference's 15.
-    descend(o, &o.alpha, {4, 8, 15, 30, 60, 120, 240}, best, run);
+    descend(o, &o.alpha, {4, 8, 15, 30, 45, 60, 90, 120, 240}, best, run);
     {
         std::vector<int32_t> fine;
         for (double f : {0.7, 1.4}) fine.push_back((int32_t)std::max(1.0, std::floor(o.alpha * f)));
@@ -176,13 +176,15 @@ hc_status tune_sssp(Tuner &tu, hc_tuning &out) {
     if (g->wtype != HC_W_I32) return HC_OK;  // no SSSP on this graph
     HC_TRY(ensure_weight_stats(g));
     if (g->w_negative) return HC_OK;
-    const int k = (int)std::min<size_t>(tu.src.size(), 8);
+    // 16 sample sources: the push/pull and delta choices move the time by a
+    // few percent, about what the spread between 8 sources is.
+    const int k = (int)std::min<size_t>(tu.src.size(), 16);
     // The built-in delta (hc_sssp): mean weight x 32 / mean degree.
     const double davg = g->n_active ? (double)g->M / (double)g->n_active : 1.0;
     const int32_t base = (int32_t)std::max(1.0, std::min(1e9, g->w_mean * 32.0 / std::max(davg, 1.0)));
     hc_sssp_opts o{};
     o.delta = out.sssp_delta > 0 ? out.sssp_delta : base;
-    o.pull_alpha = out.sssp_pull_alpha != 0 ? out.sssp_pull_alpha : 4;
+    o.pull_alpha = out.sssp_pull_alpha != 0 ? out.sssp_pull_alpha : 8;
     auto run = [&](const hc_sssp_opts &x) { return tu.sssp(x, k); };
     tu.sssp(o, 1);
     double best = run(o);
@@ -190,7 +192,7 @@ hc_status tune_sssp(Tuner &tu, hc_tuning &out) {
     std::vector<int32_t> deltas;
     for (double f : {0.25, 0.5, 1.0, 2.0, 4.0}) deltas.push_back((int32_t)std::max(1.0, std::floor(base * f)));
     descend(o, &o.delta, deltas, best, run);
-    if (g->w_symmetric) descend(o, &o.pull_alpha, {1, 2, 4, 8, -1}, best, run);
+    if (g->w_symmetric) descend(o, &o.pull_alpha, {2, 4, 8, 12, 16, -1}, best, run);
     // Second, finer pass around the winners.
     std::vector<int32_t> fine;
     for (double f : {0.7, 0.85, 1.2, 1.4}) fine.push_back((int32_t)std::max(1.0, std::floor(o.delta * f)));
