@@ -790,15 +790,20 @@ def main():
     h_dist = torch.empty((k, n), dtype=torch.int32).pin_memory().numpy()
     h_scores = torch.empty(n, dtype=torch.float32).pin_memory().numpy()
     e2e_ms = []
+    e2e_phase = []  # per step: BFS, SSSP, PageRank calls (host clock)
     for _ in range(max(1, a.steps)):
         flush.fill_(1)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         s_np = src_pin.numpy()
         g.bfs(s_np, None, h_parent, want_depth=False)
+        t1 = time.perf_counter()
         g.sssp(s_np, h_dist)
+        t2 = time.perf_counter()
         g.pagerank(None, h_scores, tol_l1=1e-4, max_iters=50)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        t3 = time.perf_counter()
+        e2e_ms.append((t3 - t0) * 1e3)
+        e2e_phase.append([(t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3])
     os.sched_setaffinity(0, saved_cpus)
     e2e_total = float(np.sum(e2e_ms))
     e2e_total = max_over_ranks(e2e_total, dev)
@@ -894,7 +899,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": int(src.nbytes),
                     "d2h_bytes_per_step": int(2 * k * n * 4 + n * 4),
                     "host_cpus": (f"{len(near)} of {len(saved_cpus)}, the GPU's NUMA node" if near
-                                  else f"all {len(saved_cpus)}")},
+                                  else f"all {len(saved_cpus)}"),
+                    "phase_ms": dict(zip(("bfs", "sssp", "pagerank"),
+                                         np.array(e2e_phase).mean(axis=0).round(3).tolist()))},
             "gpu_launches": launches, "clocks": clk.summary(), "parity": parity, "per_algo": per_algo,
             **extras, "tuning": tuning, "graph_gen_s": gen_s}), flush=True)
     g.close()
