@@ -35,8 +35,8 @@ constexpr int kSsspThreads = 512;
 constexpr int kPullThreads = 256;
 constexpr int kTraceEpochs = 96;
 constexpr int kDefaultPullAlpha = 8;
-// Far piles of at most this many entries end the near/far phases (one last
-// phase takes every remaining vertex).
+// After a pull epoch, far piles of at most this many entries end the near/far
+// phases (one last phase takes every remaining vertex).
 #ifndef HC_SSSP_TAIL_PILE
 #define HC_SSSP_TAIL_PILE 16384
 #endif
@@ -501,11 +501,15 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent(SsspArgs a) {
             const int32_t mfar = __ldcg(&ctl->min_far);
             if (mfar == kInfDist) break;
             const int32_t T_old = T;
-            // A small pile is finished in one last near phase: a phase costs
-            // a few grid barriers however few vertices it holds, and
-            // relaxing those few out of distance order costs little.
-            const long long tn = fl <= kTailPile ? (long long)kInfDist
-                                                 : ((long long)mfar / a.delta + 1) * (long long)a.delta;
+            // After a pull sweep (the dense part of a small-diameter graph is
+            // done) a small pile is finished in one last near phase: a phase
+            // costs a few grid barriers however few vertices it holds, and
+            // relaxing those few out of distance order costs little.  On a
+            // high-diameter graph (no pulls) the pile is the thin wavefront
+            // and keeps its distance order.
+            const long long tn = pulls > 0 && fl <= kTailPile
+                                     ? (long long)kInfDist
+                                     : ((long long)mfar / a.delta + 1) * (long long)a.delta;
             T = (int32_t)(tn < (long long)kInfDist ? tn : (long long)kInfDist);
             // Split: [T_old, T) joins the epoch-E queue, >= T stays far.  A
             // warp takes 1024 consecutive pile entries: pass 1 classifies them
