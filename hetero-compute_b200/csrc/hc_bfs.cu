@@ -16,6 +16,7 @@
 //   tasks          int2[]        (vertex, chunk) pieces of long rows
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <cstdlib>
 #include <mutex>
 #include <vector>
@@ -525,7 +526,7 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
         if (host_depth || host_parent) HC_TRY(pipe.acquire(i, stage));
         a.depth = dev_depth ? depth_out + (size_t)i * n : host_depth ? stage[0] : g->ws_out0.as<int32_t>();
         a.parent = dev_parent ? parent_out + (size_t)i * n : host_parent ? stage[1] : g->ws_out1.as<int32_t>();
-        HC_CUDA_TRY(cudaMemsetAsync(a.ctl, 0, sizeof(BfsCtl), g->stream));
+        HC_TRY(ctl_zero(g, a.ctl, sizeof(BfsCtl)));
         HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
         HC_TRY(o.collect_stats ? launch_bfs<true>(g, a) : launch_bfs<false>(g, a));
         HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
@@ -534,18 +535,23 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
                             host_parent ? (void *)(parent_out + (size_t)i * n) : nullptr};
             HC_TRY(pipe.release(i, dst));
         }
+        static_assert(sizeof(BfsCtl) <= kCtlSlotBytes, "BfsCtl exceeds a control-read slot");
         BfsCtl c;
-        HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
+        const void *h_ctl = nullptr, *h_cnt = nullptr;
+        HC_TRY(ctl_read(g, a.ctl, sizeof(c), 0, &h_ctl));
         if (o.collect_stats && stats) {
             unsigned long long *cnt = (unsigned long long *)((char *)a.ctl + 2048);
-            HC_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, g->stream));
+            HC_TRY(ctl_zero(g, cnt, 8));
             { count_reached<<<g->sm_count * 4, 256, 0, g->stream>>>(a.depth, g->N, cnt); ::hc::count_launch(); }
-            unsigned long long reached = 0;
-            HC_CUDA_TRY(cudaMemcpyAsync(&reached, cnt, 8, cudaMemcpyDeviceToHost, g->stream));
-            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-            stats->reached += (int32_t)reached;
+            HC_TRY(ctl_read(g, cnt, 8, 1, &h_cnt));
         }
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        std::memcpy(&c, h_ctl, sizeof(c));
+        if (h_cnt) {
+            unsigned long long reached = 0;
+            std::memcpy(&reached, h_cnt, 8);
+            stats->reached += (int32_t)reached;
+        }
         if (c.gs.err) return fail((hc_status)c.gs.err, "hc_bfs: device run from source %d ended with status %d",
                                   src[i], c.gs.err);
         float ms = 0;

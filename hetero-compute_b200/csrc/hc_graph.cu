@@ -172,6 +172,35 @@ hc_status OutPipe::finish() {
     return HC_OK;
 }
 
+namespace {
+__global__ void words_zero(uint32_t *p, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 0u;
+}
+__global__ void words_to_host(uint32_t *dst, const uint32_t *src, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+    __threadfence_system();
+}
+}  // namespace
+
+hc_status ctl_zero(hc_graph *g, void *dev, size_t bytes) {
+    { words_zero<<<1, 256, 0, g->stream>>>(reinterpret_cast<uint32_t *>(dev), (int)((bytes + 3) / 4)); count_launch(); }
+    HC_CUDA_TRY(cudaGetLastError());
+    return HC_OK;
+}
+
+hc_status ctl_read(hc_graph *g, const void *dev, size_t bytes, int slot, const void **host) {
+    if (bytes > kCtlSlotBytes || slot < 0 || slot >= kCtlSlots) return fail(HC_ERR_INVALID_ARG, "ctl_read: bad slot");
+    if (!g->ctl_host) {
+        HC_CUDA_TRY(cudaHostAlloc(&g->ctl_host, kCtlSlotBytes * kCtlSlots, cudaHostAllocMapped));
+        HC_CUDA_TRY(cudaHostGetDevicePointer(&g->ctl_host_dev, g->ctl_host, 0));
+    }
+    uint32_t *d = reinterpret_cast<uint32_t *>(static_cast<char *>(g->ctl_host_dev) + (size_t)slot * kCtlSlotBytes);
+    { words_to_host<<<1, 256, 0, g->stream>>>(d, reinterpret_cast<const uint32_t *>(dev), (int)((bytes + 3) / 4)); count_launch(); }
+    HC_CUDA_TRY(cudaGetLastError());
+    *host = static_cast<const char *>(g->ctl_host) + (size_t)slot * kCtlSlotBytes;
+    return HC_OK;
+}
+
 hc_status activate(hc_graph *g) {
     if (!g) return fail(HC_ERR_INVALID_ARG, "null graph handle");
     HC_CUDA_TRY(cudaSetDevice(g->device));
@@ -607,6 +636,7 @@ hc_status hc_graph_destroy(hc_graph *g) {
     }
     if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
     g->pinned.release();
+    if (g->ctl_host) cudaFreeHost(g->ctl_host);
     if (g->ev_start) cudaEventDestroy(g->ev_start);
     if (g->ev_stop) cudaEventDestroy(g->ev_stop);
     if (g->own_stream) cudaStreamDestroy(g->own_stream);

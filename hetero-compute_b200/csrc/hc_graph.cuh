@@ -106,6 +106,9 @@ struct hc_graph {
     // workspaces
     hc::DevBuf ws_bfs, ws_sssp, ws_pr, ws_batch, ws_out0, ws_out1, ws_ctl, ws_src;
     hc::PinnedBuf pinned;
+    // mapped pinned slots for control-block reads (ctl_read), and their device address
+    void *ctl_host = nullptr;
+    void *ctl_host_dev = nullptr;
 
     int bfs_grid = 0, sssp_grid = 0;
     int64_t bytes_held() const;
@@ -164,6 +167,18 @@ const float *pr_weights(const hc_graph *g);
 hc_status ensure_plan(hc_graph *g);
 // Computes w_negative, w_max, w_mean and w_symmetric once (int32 weights).
 hc_status ensure_weight_stats(hc_graph *g);
+// Per-run control traffic kept off the copy engines.  A host-output call
+// keeps a large copy on the copy stream while the next source runs; a small
+// cudaMemcpyAsync or cudaMemsetAsync of a control block on the compute stream
+// can queue on the same engine behind it and serialise the two.  ctl_zero
+// clears device words with a one-block kernel on the graph's stream; ctl_read
+// has a one-block kernel write `bytes` (at most kCtlSlotBytes) of device memory
+// into mapped pinned slot `slot` (0..kCtlSlots-1) and returns its host address,
+// valid once the stream has been synchronised.
+constexpr size_t kCtlSlotBytes = 4096;
+constexpr int kCtlSlots = 4;
+hc_status ctl_zero(hc_graph *g, void *dev, size_t bytes);
+hc_status ctl_read(hc_graph *g, const void *dev, size_t bytes, int slot, const void **host);
 // Device memory pressure.  Derived arrays that can be built again (the
 // pull sweeps' pair array, the reference-order schedule, the weighted
 // PageRank arrays) and the batched workspace are released, when an

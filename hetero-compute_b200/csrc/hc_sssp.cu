@@ -22,6 +22,7 @@
 #include <climits>
 #include <cstddef>
 #include <cstdio>
+#include <cstring>
 #include <cstdlib>
 #include <vector>
 
@@ -845,7 +846,7 @@ hc_status launch_pull(hc_graph *g, const SsspArgs &a) {
 constexpr int kSpeculate = 3;
 
 template <bool kStats>
-hc_status run_source(hc_graph *g, const SsspArgs &a, volatile int *h_flags) {
+hc_status run_source(hc_graph *g, const SsspArgs &a) {
     HC_TRY(launch_sssp<kStats>(g, a));
     if (a.pull_alpha <= 0) return HC_OK;  // no pull epochs: one launch
     for (int round = 0;; round++) {
@@ -854,11 +855,12 @@ hc_status run_source(hc_graph *g, const SsspArgs &a, volatile int *h_flags) {
             HC_TRY(launch_sssp<kStats>(g, a));
         }
         // gs.err, need_pull, resume and finished, at the head of SsspCtl.
-        HC_CUDA_TRY(cudaMemcpyAsync((void *)h_flags, a.ctl, offsetof(SsspCtl, finished) + sizeof(int),
-                                    cudaMemcpyDeviceToHost, g->stream));
+        const void *h_head = nullptr;
+        HC_TRY(ctl_read(g, a.ctl, offsetof(SsspCtl, finished) + sizeof(int), 3, &h_head));
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        const SsspCtl *hc = (const SsspCtl *)h_flags;
-        if (hc->gs.err || hc->finished) return HC_OK;
+        SsspCtl head;
+        std::memcpy(&head, h_head, offsetof(SsspCtl, finished) + sizeof(int));
+        if (head.gs.err || head.finished) return HC_OK;
         if ((int64_t)round * kSpeculate > a.max_epochs)
             return fail(HC_ERR_NOT_CONVERGED, "hc_sssp: pull rounds exceed the epoch cap");
     }
@@ -996,8 +998,6 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
     OutPipe pipe;
     if (host_dist || host_parent) HC_TRY(pipe.init(g, 2, 4 * n));
 
-    HC_TRY(g->pinned.ensure(sizeof(SsspCtl)));
-    volatile int *h_flags = g->pinned.as<int>();
     // Candidates can reach the INT32_MAX clamp only when a path of
     // n_active - 1 edges of the largest weight can; then each source's
     // distances are checked after its run (a flag in the control block's
@@ -1012,9 +1012,9 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
         int32_t *stage[2] = {nullptr, nullptr};
         if (host_dist || host_parent) HC_TRY(pipe.acquire(i, stage));
         a.dist = dev_dist ? dist_out + (size_t)i * n : host_dist ? stage[0] : g->ws_out0.as<int32_t>();
-        HC_CUDA_TRY(cudaMemsetAsync(a.ctl, 0, sizeof(SsspCtl), g->stream));
+        HC_TRY(ctl_zero(g, a.ctl, sizeof(SsspCtl)));
         HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
-        HC_TRY(o.collect_stats ? run_source<true>(g, a, h_flags) : run_source<false>(g, a, h_flags));
+        HC_TRY(o.collect_stats ? run_source<true>(g, a) : run_source<false>(g, a));
         HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
         if (parent_out) {
             int32_t *par = dev_parent ? parent_out + (size_t)i * n : stage[1];
@@ -1029,22 +1029,27 @@ extern "C" hc_status hc_sssp(hc_graph *g, const int32_t *sources, int32_t num_so
         }
         SsspCtl c;
         int out_of_range = 0;
+        const void *h_range = nullptr, *h_ctl = nullptr, *h_cnt = nullptr;
         if (check_range) {
-            HC_CUDA_TRY(cudaMemsetAsync(range_flag, 0, sizeof(int), g->stream));
+            HC_TRY(ctl_zero(g, range_flag, sizeof(int)));
             { any_above<<<g->sm_count * 4, 256, 0, g->stream>>>(a.dist, g->N, range_limit, range_flag); ::hc::count_launch(); }
-            HC_CUDA_TRY(cudaMemcpyAsync(&out_of_range, range_flag, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+            HC_TRY(ctl_read(g, range_flag, sizeof(int), 1, &h_range));
         }
-        HC_CUDA_TRY(cudaMemcpyAsync(&c, a.ctl, sizeof(c), cudaMemcpyDeviceToHost, g->stream));
+        HC_TRY(ctl_read(g, a.ctl, sizeof(c), 0, &h_ctl));
         if (o.collect_stats && stats) {
             unsigned long long *cnt = (unsigned long long *)((char *)a.ctl + 2048);
-            HC_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, g->stream));
+            HC_TRY(ctl_zero(g, cnt, 8));
             { count_finite<<<g->sm_count * 4, 256, 0, g->stream>>>(a.dist, g->N, cnt); ::hc::count_launch(); }
-            unsigned long long reached = 0;
-            HC_CUDA_TRY(cudaMemcpyAsync(&reached, cnt, 8, cudaMemcpyDeviceToHost, g->stream));
-            HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
-            stats->reached += (int32_t)reached;
+            HC_TRY(ctl_read(g, cnt, 8, 2, &h_cnt));
         }
         HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        std::memcpy(&c, h_ctl, sizeof(c));
+        if (h_range) std::memcpy(&out_of_range, h_range, sizeof(int));
+        if (h_cnt) {
+            unsigned long long reached = 0;
+            std::memcpy(&reached, h_cnt, 8);
+            stats->reached += (int32_t)reached;
+        }
         if (c.gs.err) return fail((hc_status)c.gs.err, "hc_sssp: device run from source %d ended with status %d",
                                   src[i], c.gs.err);
         if (out_of_range)
