@@ -10,14 +10,17 @@
 //         paths", IPDPS 2014);
 //   pull  when the frontier's edges exceed M / pull_alpha, sweep every row
 //         with the reference's own Bellman-Ford pull (min over neighbours of
-//         dist[u] + w), which streams the CSR without per-edge atomics, then
-//         turn the vertices it lowered back into the near queue / far pile.
+//         dist[u] + w) over each row's (neighbour, weight) pairs in weight
+//         order, stopping a row once no later pair can lower it, without
+//         per-edge atomics, then turn the vertices it lowered back into the
+//         near queue / far pile.
 // Distances are exact integers; unreachable = INT32_MAX.
 //
 // Working set (N vertices): dist int32[N]; near queues q[2] int32[N];
 // far piles far[2] int32[N]; stamp / fstamp int32[N] (queue dedup without
 // clearing: a vertex joins the epoch-E queue by raising stamp[v] to E);
 // changed bitmap uint32[N/32] (pull sweeps); tasks int2[] for long rows.
+// Per graph: the pull sweeps' pair array int2[M + 64] (weight_order_rows).
 #include <algorithm>
 #include <climits>
 #include <cstddef>
