@@ -328,8 +328,12 @@ def profile_case(a):
     capture of bfs_persistent / sssp_persistent / sssp_pull_kernel / pr_sweep
     selects.  With --suite batched: one 512-source batched BFS, one 512-source
     batched SSSP group on 16-bit distances and one 256-source group on int32
-    distances (device outputs)."""
+    distances (device outputs).  Under a profiler that replays each captured
+    launch dozens of times a whole persistent run takes far longer than it
+    does alone, so the run and loop limits are raised to 10 minutes here (the
+    per-barrier wait limit stays at its default)."""
     import hc
+    hc.set_time_limits(0, 0, 600 * 10**9, 600 * 10**9)
     if a.suite == "batched":
         import torch
         host = hc.gen_kronecker(a.scale, a.edge_factor, a.seed, hc.W_I32)
