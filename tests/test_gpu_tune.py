@@ -1,5 +1,7 @@
 """Autotuner: the tuned parameters come from the candidate sets, results stay
 exact under the tuned launch parameters, and explicit options still win."""
+import math
+
 import numpy as np
 import pytest
 
@@ -22,8 +24,12 @@ def test_tuned_values_come_from_the_candidates(tuned):
     host, g, src, t = tuned
     assert t["trials"] > 20 and t["tune_ms"] > 0
     assert t["bfs_bu_variant"] in (hc.VARIANT_THREAD, hc.VARIANT_WARP, hc.VARIANT_BLOCK)
-    assert t["bfs_alpha"] in (4, 8, 15, 30, 60) and t["bfs_beta"] in (6, 12, 18, 36, 72)
-    assert t["sssp_delta"] > 0 and (t["sssp_pull_alpha"] == -1 or 1 <= t["sssp_pull_alpha"] <= 12)
+    # BFS alpha: a coarse pass, then floor(0.7 x) and floor(1.4 x) around the winner (double arithmetic,
+    # as the tuner computes them); SSSP pull alpha: 2-16, then -1 / +1 / x1.5 around the winner.
+    coarse = (4, 8, 15, 30, 45, 60, 90, 120, 240)
+    alphas = set(coarse) | {max(1, math.floor(b * f)) for b in coarse for f in (0.7, 1.4)}
+    assert t["bfs_alpha"] in alphas and t["bfs_beta"] in (6, 12, 18, 36, 72)
+    assert t["sssp_delta"] > 0 and (t["sssp_pull_alpha"] == -1 or 1 <= t["sssp_pull_alpha"] <= 24)
     assert t["mbfs_group"] in (64, 128, 256, 512) and t["mbfs_switch_alpha"] in (5, 10, 20, 40, -1)
     assert t["mssp_group"] in (64, 128, 256, 512) and t["mssp_switch_alpha"] in (1, 2, 4, -1)
     assert 0 <= t["bfs_bu_split_levels"] <= 8 and len(t["bfs_bu_split"]) == t["bfs_bu_split_levels"]
