@@ -402,3 +402,51 @@ def test_host_outputs_pinned_and_mixed():
     assert np.array_equal(pinned_s, sd.cpu().numpy())
     for i, s in enumerate(src):
         assert oracle.verify_sp_tree(host.index, host.neighbors, host.weights, pinned_s[i], pinned_sp[i], s) == 0
+
+
+def test_bfs_frontier_summary_with_a_shift():
+    """Above 2^22 vertices a summary bit covers several frontier words (2^23 here: two); bottom-up levels
+    probe global memory only where it is set.  Depths against the serial BFS, parents as BFS trees."""
+    host = hc.gen_uniform(23, 2, 17)
+    assert host.num_nodes == 1 << 23
+    g = hc.Graph.from_host(host)
+    src = hc.pick_sources(host, 2)
+    for direction in (2, 0):  # every level bottom-up; Beamer's switching
+        depth, parent, _ = g.bfs(src, direction=direction)
+        for i, s in enumerate(src):
+            d = oracle.bfs_depth(host.index, host.neighbors, s)
+            assert np.array_equal(depth[i], d), (direction, i)
+            assert oracle.verify_bfs_parents(host.index, host.neighbors, d, parent[i], s)[0] == 0
+    g.close()
+
+
+def test_sssp_weight_ordered_pulls_on_hub_chunks():
+    """A hub row longer than the chunk size (its later chunks test their first window before reading it),
+    with skewed weights, every epoch a pull: exact against Dijkstra."""
+    rng = np.random.default_rng(5)
+    n, hub_deg = 30000, 20000
+    edges = {(0, int(v)) for v in rng.choice(np.arange(1, n), hub_deg, replace=False)}
+    while len(edges) < hub_deg + 4 * n:
+        a, b = (int(x) for x in rng.integers(1, n, 2))
+        if a != b:
+            edges.add((min(a, b), max(a, b)))
+    src_l, dst_l = zip(*edges)
+    src_a, dst_a = np.array(src_l + dst_l), np.array(dst_l + src_l)
+    order = np.lexsort((dst_a, src_a))
+    src_a, dst_a = src_a[order], dst_a[order]
+    index = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(index, src_a + 1, 1)
+    index = np.cumsum(index)
+    nbr = dst_a.astype(np.int32)
+    lo, hi = np.minimum(src_a, dst_a).astype(np.int64), np.maximum(src_a, dst_a).astype(np.int64)
+    h = (lo * 1000003 + hi * 7919) % 2147483629
+    w = np.where(h % 40 == 0, 1 + h % 3, 200 + h % 50).astype(np.int32)  # a few light edges, most heavy
+    g = hc.Graph(index, nbr, w)
+    srcs = np.array([0, 1, 12345], dtype=np.int32)
+    for pull_alpha in (1000000, 0):
+        dist, parent, _ = g.sssp(srcs, pull_alpha=pull_alpha, want_parent=True)
+        for i, s in enumerate(srcs):
+            d = oracle.sssp_dijkstra(index, nbr, w, int(s))
+            assert np.array_equal(dist[i], d), (pull_alpha, i)
+            assert oracle.verify_sp_tree(index, nbr, w, d, parent[i], int(s)) == 0
+    g.close()
