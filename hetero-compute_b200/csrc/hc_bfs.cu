@@ -19,6 +19,7 @@
 #include <cstring>
 #include <cstdlib>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "hc_expand.cuh"
@@ -419,6 +420,39 @@ __global__ void count_reached(const int32_t *depth, int32_t n, unsigned long lon
     if (threadIdx.x == 0 && c) atomicAdd(out, c);
 }
 
+// Host outputs on a degree-sorted graph: the vertices [n_copy, n) have no
+// edges, so every run leaves their depth and parent at -1 (a source among
+// them aside: depth 0, parent itself).  A few host threads write those
+// suffixes while the GPU runs, and only the first n_copy entries of each
+// source's rows cross PCIe.  The threads are joined by the destructor, on
+// every return path.
+struct SuffixFill {
+    std::vector<std::thread> th;
+    void start(int32_t *depth, int32_t *parent, const std::vector<int32_t> &src, int64_t n, int64_t n_copy) {
+        const int k = (int)src.size();
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const int nt = std::max(1, std::min({(int)(hw / 2), 8, k}));
+        for (int t = 0; t < nt; t++)
+            th.emplace_back([=, &src]() {
+                for (int i = t; i < k; i += nt) {
+                    for (int32_t *out : {depth, parent}) {
+                        if (!out) continue;
+                        int32_t *row = out + (size_t)i * n;
+                        std::fill(row + n_copy, row + n, -1);
+                    }
+                    const int32_t s = src[i];
+                    if (s >= n_copy) {
+                        if (depth) depth[(size_t)i * n + s] = 0;
+                        if (parent) parent[(size_t)i * n + s] = s;
+                    }
+                }
+            });
+    }
+    ~SuffixFill() {
+        for (auto &t : th) t.join();
+    }
+};
+
 template <bool kStats>
 hc_status launch_bfs(hc_graph *g, const BfsArgs &args) {
     static int blocks_per_sm[2] = {0, 0};
@@ -517,7 +551,15 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
     // Host outputs: staged on the device and copied while the next source runs.
     const bool host_depth = depth_out && !dev_depth, host_parent = parent_out && !dev_parent;
     OutPipe pipe;
-    if (host_depth || host_parent) HC_TRY(pipe.init(g, 2, 4 * n));
+    SuffixFill fill;  // declared after the pipe: its threads are joined first on any return
+    if (host_depth || host_parent) {
+        HC_TRY(pipe.init(g, 2, 4 * n));
+        const int64_t n_copy = g->degree_sorted ? (int64_t)g->n_active : n;
+        if (n_copy < n) {
+            pipe.copy_bytes = sizeof(int32_t) * (size_t)n_copy;
+            fill.start(host_depth ? depth_out : nullptr, host_parent ? parent_out : nullptr, src, n, n_copy);
+        }
+    }
 
     double total_ms = 0;
     for (int32_t i = 0; i < num_sources; i++) {

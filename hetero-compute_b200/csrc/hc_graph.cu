@@ -124,6 +124,7 @@ hc_status OutPipe::init(hc_graph *graph, int arrays, size_t each) {
     g = graph;
     narr = arrays;
     bytes = each;
+    copy_bytes = each;
     pending = false;
     if (!g->copy_stream) HC_CUDA_TRY(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
     for (int s = 0; s < 2; s++) {
@@ -161,7 +162,8 @@ hc_status OutPipe::flush() {
     HC_CUDA_TRY(cudaStreamWaitEvent(g->copy_stream, g->ev_ready[s], 0));
     for (int j = 0; j < narr; j++)
         if (pend_dst[j])
-            HC_CUDA_TRY(cudaMemcpyAsync(pend_dst[j], g->ws_stage[s][j].ptr, bytes, cudaMemcpyDefault, g->copy_stream));
+            HC_CUDA_TRY(cudaMemcpyAsync(pend_dst[j], g->ws_stage[s][j].ptr, copy_bytes, cudaMemcpyDefault,
+                                        g->copy_stream));
     HC_CUDA_TRY(cudaEventRecord(g->ev_done[s], g->copy_stream));
     return HC_OK;
 }

@@ -128,6 +128,7 @@ struct OutPipe {
     hc_graph *g = nullptr;
     int narr = 0;
     size_t bytes = 0;
+    size_t copy_bytes = 0;  // bytes of each array copied out (init: all; a caller may shorten it)
     bool pending = false;
     int pend_slot = 0;
     void *pend_dst[2] = {nullptr, nullptr};
