@@ -38,7 +38,7 @@ namespace {
 constexpr int kSsspThreads = 512;
 constexpr int kPullThreads = 256;
 constexpr int kTraceEpochs = 96;
-constexpr int kDefaultPullAlpha = 8;
+constexpr int kDefaultPullAlpha = 10;
 // After a pull epoch, far piles of at most this many entries end the near/far
 // phases (one last phase takes every remaining vertex).
 #ifndef HC_SSSP_TAIL_PILE

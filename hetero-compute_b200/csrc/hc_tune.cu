@@ -184,7 +184,7 @@ hc_status tune_sssp(Tuner &tu, hc_tuning &out) {
     const int32_t base = (int32_t)std::max(1.0, std::min(1e9, g->w_mean * 32.0 / std::max(davg, 1.0)));
     hc_sssp_opts o{};
     o.delta = out.sssp_delta > 0 ? out.sssp_delta : base;
-    o.pull_alpha = out.sssp_pull_alpha != 0 ? out.sssp_pull_alpha : 8;
+    o.pull_alpha = out.sssp_pull_alpha != 0 ? out.sssp_pull_alpha : 10;
     auto run = [&](const hc_sssp_opts &x) { return tu.sssp(x, k); };
     tu.sssp(o, 1);
     double best = run(o);
@@ -192,7 +192,7 @@ hc_status tune_sssp(Tuner &tu, hc_tuning &out) {
     std::vector<int32_t> deltas;
     for (double f : {0.25, 0.5, 1.0, 2.0, 4.0}) deltas.push_back((int32_t)std::max(1.0, std::floor(base * f)));
     descend(o, &o.delta, deltas, best, run);
-    if (g->w_symmetric) descend(o, &o.pull_alpha, {2, 4, 8, 12, 16, -1}, best, run);
+    if (g->w_symmetric) descend(o, &o.pull_alpha, {2, 4, 6, 8, 10, 12, 16, -1}, best, run);
     // Second, finer pass around the winners.
     std::vector<int32_t> fine;
     for (double f : {0.7, 0.85, 1.2, 1.4}) fine.push_back((int32_t)std::max(1.0, std::floor(o.delta * f)));

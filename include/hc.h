@@ -216,7 +216,7 @@ typedef struct hc_sssp_opts {
     int32_t collect_stats;
     int32_t pull_alpha;   /* run an epoch as a pull sweep over every row (the reference's
                              Bellman-Ford epoch, src/kernels/gpu/sssp.cuh:120-281) when the
-                             frontier's edges * pull_alpha > M; 0 = auto (8), < 0 = never.
+                             frontier's edges * pull_alpha > M; 0 = auto (10), < 0 = never.
                              Needs symmetric weights (checked once per graph). */
 } hc_sssp_opts;
 
