@@ -432,21 +432,27 @@ struct SuffixFill {
         const int k = (int)src.size();
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
         const int nt = std::max(1, std::min({(int)(hw / 2), 8, k}));
-        for (int t = 0; t < nt; t++)
-            th.emplace_back([=, &src]() {
-                for (int i = t; i < k; i += nt) {
-                    for (int32_t *out : {depth, parent}) {
-                        if (!out) continue;
-                        int32_t *row = out + (size_t)i * n;
-                        std::fill(row + n_copy, row + n, -1);
-                    }
-                    const int32_t s = src[i];
-                    if (s >= n_copy) {
-                        if (depth) depth[(size_t)i * n + s] = 0;
-                        if (parent) parent[(size_t)i * n + s] = s;
-                    }
+        auto part = [=, &src](int t) {
+            for (int i = t; i < k; i += nt) {
+                for (int32_t *out : {depth, parent}) {
+                    if (!out) continue;
+                    int32_t *row = out + (size_t)i * n;
+                    std::fill(row + n_copy, row + n, -1);
                 }
-            });
+                const int32_t s = src[i];
+                if (s >= n_copy) {
+                    if (depth) depth[(size_t)i * n + s] = 0;
+                    if (parent) parent[(size_t)i * n + s] = s;
+                }
+            }
+        };
+        for (int t = 0; t < nt; t++) {
+            try {
+                th.emplace_back(part, t);
+            } catch (...) {  // no thread to be had: this share runs here (nothing throws past the C ABI)
+                part(t);
+            }
+        }
     }
     ~SuffixFill() {
         for (auto &t : th) t.join();
