@@ -459,6 +459,30 @@ struct SuffixFill {
     }
 };
 
+// Results of the runs of one call, folded on the device after each run so
+// that the host need not wait for each source: the first failure (status and
+// source), the deepest run, the top-down / bottom-up level counts.
+struct BfsFold {
+    int err, err_src, levels, td_levels, bu_levels, pad;
+};
+
+// Folds the run just finished into *f, then clears the control block for the
+// next run (one block).
+__global__ void bfs_fold_clear(BfsCtl *ctl, BfsFold *f, int32_t src) {
+    if (threadIdx.x == 0) {
+        if (ctl->gs.err && !f->err) {
+            f->err = ctl->gs.err;
+            f->err_src = src;
+        }
+        f->levels = max(f->levels, ctl->levels);
+        f->td_levels += ctl->td_levels;
+        f->bu_levels += ctl->bu_levels;
+    }
+    __syncthreads();
+    uint32_t *w = reinterpret_cast<uint32_t *>(ctl);
+    for (int i = threadIdx.x; i < (int)(sizeof(BfsCtl) / 4); i += blockDim.x) w[i] = 0u;
+}
+
 template <bool kStats>
 hc_status launch_bfs(hc_graph *g, const BfsArgs &args) {
     static int blocks_per_sm[2] = {0, 0};
@@ -568,12 +592,34 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
     }
 
     double total_ms = 0;
+    // Without per-run statistics or a trace the runs go back to back: each
+    // run's result is folded on the device and the host waits once, at the
+    // end (with them, it reads each run's control block after it).
+    const bool per_run = (o.collect_stats && stats) || std::getenv("HC_TRACE");
+    static_assert(sizeof(BfsCtl) + 64 <= 2048, "BfsCtl overlaps the fold record");
+    BfsFold *fold = reinterpret_cast<BfsFold *>(reinterpret_cast<char *>(a.ctl) + 2560);
+    if (!per_run) {
+        HC_TRY(ctl_zero(g, fold, sizeof(BfsFold)));
+        HC_TRY(ctl_zero(g, a.ctl, sizeof(BfsCtl)));
+        HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
+    }
     for (int32_t i = 0; i < num_sources; i++) {
         a.src = src[i];
         int32_t *stage[2] = {nullptr, nullptr};
         if (host_depth || host_parent) HC_TRY(pipe.acquire(i, stage));
         a.depth = dev_depth ? depth_out + (size_t)i * n : host_depth ? stage[0] : g->ws_out0.as<int32_t>();
         a.parent = dev_parent ? parent_out + (size_t)i * n : host_parent ? stage[1] : g->ws_out1.as<int32_t>();
+        if (!per_run) {
+            HC_TRY(launch_bfs<false>(g, a));
+            if (host_depth || host_parent) {
+                void *dst[2] = {host_depth ? (void *)(depth_out + (size_t)i * n) : nullptr,
+                                host_parent ? (void *)(parent_out + (size_t)i * n) : nullptr};
+                HC_TRY(pipe.release(i, dst));
+            }
+            { bfs_fold_clear<<<1, 256, 0, g->stream>>>(a.ctl, fold, a.src); ::hc::count_launch(); }
+            HC_CUDA_TRY(cudaGetLastError());
+            continue;
+        }
         HC_TRY(ctl_zero(g, a.ctl, sizeof(BfsCtl)));
         HC_CUDA_TRY(cudaEventRecord(g->ev_start, g->stream));
         HC_TRY(o.collect_stats ? launch_bfs<true>(g, a) : launch_bfs<false>(g, a));
@@ -618,6 +664,24 @@ extern "C" hc_status hc_bfs(hc_graph *g, const int32_t *sources, int32_t num_sou
             for (int l = 0; l < nl; l++)
                 std::fprintf(stderr, "[hc bfs]   L%-3d %s nf=%-9d %8.1f us\n", l, c.trace[l].mode == 1 ? "TD" : "BU",
                              c.trace[l].nf, (c.trace[l + 1].t_ns - c.trace[l].t_ns) * 1e-3);
+        }
+    }
+    if (!per_run) {
+        HC_CUDA_TRY(cudaEventRecord(g->ev_stop, g->stream));
+        const void *h_fold = nullptr;
+        HC_TRY(ctl_read(g, fold, sizeof(BfsFold), 0, &h_fold));
+        HC_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        BfsFold f;
+        std::memcpy(&f, h_fold, sizeof(f));
+        if (f.err) return fail((hc_status)f.err, "hc_bfs: device run from source %d ended with status %d",
+                               f.err_src, f.err);
+        float ms = 0;
+        HC_CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_start, g->ev_stop));
+        total_ms = ms;
+        if (stats) {
+            stats->levels = f.levels;
+            stats->td_levels = f.td_levels;
+            stats->bu_levels = f.bu_levels;
         }
     }
     if (host_depth || host_parent) HC_TRY(pipe.finish());
