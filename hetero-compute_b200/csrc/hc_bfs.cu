@@ -436,8 +436,9 @@ struct SuffixFill {
             for (int i = t; i < k; i += nt) {
                 for (int32_t *out : {depth, parent}) {
                     if (!out) continue;
-                    int32_t *row = out + (size_t)i * n;
-                    std::fill(row + n_copy, row + n, -1);
+                    // -1 in every byte is -1 in every int32; a large memset streams its
+                    // stores without reading the lines first.
+                    std::memset(out + (size_t)i * n + n_copy, 0xFF, sizeof(int32_t) * (size_t)(n - n_copy));
                 }
                 const int32_t s = src[i];
                 if (s >= n_copy) {
